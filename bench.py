@@ -1,0 +1,363 @@
+"""Benchmark of the dnsbox pseudospectral time step on B200.
+
+Workload (the forced-isotropic-turbulence configuration the metric is quoted
+on): N = 256^3 in a 2 pi box, seeded spectrum E(k) ~ k^4 exp(-2 k^2/k0^2) with
+k0 = 3 and E = 0.5, band forcing on |k| <= 2.5 with Pin = 0.1, nu = 2e-3,
+integrating-factor Heun step with CFL control at Courant 0.5, FP64 (the plain
+form; the FP32 form is reported beside it).  One "step" is one time step of
+the whole box.  Inputs (the spectral velocity) are synthetic and larger than
+L2 (3 x 135 MB in FP64).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (torchrun) every rank advances its own independent box (the step
+does not shard: replicas only), value = steps of all ranks / max-over-ranks
+time.  ``--impl reference`` times the CPU restatement of the reference step on
+the host cores (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "steps/s @256^3 forced turbulence (IF-Heun, CFL 0.5, band forcing), FP64 plain form"
+UNIT = "steps/s"
+WORKLOAD = dict(n=256, k0=3.0, nu=2e-3, kCutOff=2.5, Pin=0.1, courant=0.5, dt_max=1e-2, dt0=1e-3)
+
+# Algorithmic HBM traffic per launch of each pass, in spectral-field units
+# (one field = nz*ny*(nx/2+1) complex values): reads + writes, each field once.
+PASS_FIELDS_HEUN = {"z_inv": [8, 8], "y_inv": [11, 11], "x_nl": [9, 9], "y_fwd": [6, 6],
+                    "z_fin": [9, 12]}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clock and clocks-event reasons through NVML while running."""
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown", 0x2: "applications_clocks",
+               0x1: "gpu_idle", 0x10: "sync_boost", 0x100: "display_clock"}
+
+    def __init__(self, index):
+        self.samples = []
+        self.reasons = 0
+        self.ok = False
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception as e:  # noqa: BLE001
+            log("clock sampling unavailable:", e)
+            self.max_mhz = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                try:
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except AttributeError:
+                    r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                self.reasons |= int(r)
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok:
+            return None
+        rs = sorted(v for b, v in self.REASONS.items() if self.reasons & b and b != 0x1)
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": rs, "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------- reference arm
+def cpu_reference_rate(n, max_steps, budget_s, warmup=1):
+    """Times the CPU restatement of the reference Heun step (oracle, FP64,
+    scipy.fft on all host threads) on the benchmark workload."""
+    from dnsbox_b200 import ic
+    from oracle import dnsbox_oracle as O
+    w = WORKLOAD
+    p = O.Params(nx=n, ny=n, nz=n, nu=w["nu"], kCutOff=w["kCutOff"], Pin=w["Pin"], bandlim=True,
+                 courant_min=w["courant"], courant_max=w["courant"], dt_max=w["dt_max"])
+    g = O.Grid(p)
+    uh = ic.random_field(n, seed=0, k0=w["k0"])
+    dt = w["dt0"]
+    u = O.state_uhat2u(g, uh)
+    dt, _ = O.set_time_step(g, dt, O.io_courant(g, u, dt))
+    for _ in range(warmup):
+        uh = O.heun_step(g, uh, dt)
+    done, t0 = 0, time.perf_counter()
+    while done < max_steps:
+        uh = O.heun_step(g, uh, dt)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return done / el, done, el
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import dnsbox_oracle as O
+    n = args.n
+    rate, done, el = cpu_reference_rate(n, args.steps, budget_s=args.ref_budget, warmup=min(args.warmup, 1))
+    cores = O.WORKERS
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"forced isotropic turbulence {n}^3, IF-Heun, CFL 0.5, band forcing Pin 0.1",
+                   "n": n, "precision": "fp64"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{done} full Heun steps at {n}^3 ({el:.1f} s) of the NumPy/scipy.fft "
+                                   f"restatement of rhs.f90 + dnsboxheun.f90 (the Fortran/MPI/p3dfft "
+                                   f"reference cannot be built on this image)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- our arm
+def make_box(n, precision, rank):
+    from dnsbox_b200.ops import Box
+    w = WORKLOAD
+    return Box(n, precision=precision, nu=w["nu"], kCutOff=w["kCutOff"], Pin=w["Pin"], bandlim=True,
+               courant_min=w["courant"], courant_max=w["courant"], dt_max=w["dt_max"], dt=w["dt0"],
+               device=torch.cuda.current_device())
+
+
+def timed_steps(box, u, k, dist_on):
+    """K steps bracketed by barrier + synchronize; CUDA events on the launch stream."""
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    box.step(u, k, diag=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    ms = e0.elapsed_time(e1)
+    if dist_on:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def measure_e2e(box, uh_np, k):
+    """Per step: H2D of the state from pinned host memory (reference layout),
+    one step through the C ABI, D2H of the new state and the step record."""
+    host = torch.empty((3, box.nxh, box.ny, box.nz), dtype=torch.complex128, pin_memory=True)
+    host_np = host.numpy()
+    host_np[...] = np.transpose(uh_np, (0, 3, 2, 1))
+    out = torch.empty_like(host, pin_memory=True).numpy()
+    u = box.zeros()
+    box.upload_state(host_np, u)
+    box.step(u, 1)
+    box.download_state(u, out)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        box.upload_state(host_np, u)
+        box.step(u, 1, diag=True)
+        box.download_state(u, host_np)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    nbytes = 3 * box.nz * box.ny * box.nxh * 16
+    return k / (ms / 1e3), nbytes, nbytes + 96
+
+
+def profile_passes(box, u, k):
+    box.profile(True)
+    box.profile_read(reset=True)
+    box.step(u, k, diag=False)
+    pr = box.profile_read(reset=True)
+    box.profile(False)
+    return pr
+
+
+def read_traffic(prec, n):
+    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    out = {}
+    if not os.path.exists(path):
+        return out
+    for line in open(path):
+        parts = line.split()
+        if len(parts) == 4 and not line.startswith("#") and parts[1] == prec and int(parts[2]) == n:
+            out[parts[0]] = float(parts[3])
+    return out
+
+
+def run_ours(args, rank, world, dist_on):
+    from dnsbox_b200 import ic
+    n = args.n
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    uh_np = ic.random_field(n, seed=rank, k0=WORKLOAD["k0"])
+    results = {}
+    for prec in args.precisions:
+        box = make_box(n, prec, rank)
+        u = box.from_numpy(uh_np)
+        box.step(u, args.warmup, diag=False)
+        torch.cuda.synchronize()
+        box.profile_read(reset=True)
+        sampler = ClockSampler(torch.cuda.current_device())
+        with sampler:
+            ms = timed_steps(box, u, args.steps, dist_on)
+        launches = box.profile_read(reset=True)["total_launches"]
+        pr = profile_passes(box, u, args.steps)
+        res = {"ms": ms, "launches": launches, "profile": pr, "clocks": sampler.summary()}
+        if prec == args.precisions[0] and rank == 0:
+            res["e2e"] = measure_e2e(box, uh_np, max(3, min(args.steps, 20)))
+        fb = box.nz * box.ny * box.nxh * (16 if prec == "fp64" else 8)
+        res["field_bytes"] = fb
+        results[prec] = res
+        box.close()
+        del u
+        torch.cuda.empty_cache()
+    if rank != 0:
+        return
+    main = args.precisions[0]
+    r = results[main]
+    steps_s = world * args.steps / (r["ms"] / 1e3)
+    # dominant kernel roofline
+    pr = r["profile"]
+    per_pass = {}
+    for name, fields in PASS_FIELDS_HEUN.items():
+        ms = pr["ms"][name]
+        nl = pr["launches"][name]
+        if nl == 0 or ms <= 0:
+            continue
+        # launches alternate between the two RHS of each step
+        nbytes = sum(fields[i % len(fields)] for i in range(nl)) * r["field_bytes"]
+        per_pass[name] = {"ms_total": ms, "launches": nl, "avg_us": 1e3 * ms / nl,
+                          "gbs": nbytes / (ms / 1e3) / 1e9, "bytes_per_launch": nbytes / nl}
+    dom = max(per_pass, key=lambda k: per_pass[k]["ms_total"])
+    d = per_pass[dom]
+    traffic = read_traffic(main, n).get(dom)
+    gp = float(n) ** 3
+    model_bytes = 72 * (8 if main == "fp64" else 4) * gp
+    step_time = r["ms"] / args.steps / 1e3
+    e2e = r.get("e2e")
+    line = {
+        "metric": METRIC, "value": steps_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if main == "fp64" else "f32",
+        "data": "synthetic",
+        "config": {"workload": f"forced isotropic turbulence {n}^3, IF-Heun, CFL 0.5, band forcing Pin 0.1, "
+                               f"nu 2e-3, k0 3 (independent box per GPU)",
+                   "n": n, "precision": main, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (3 x %.0f MB state, 12-field workspace)" % (r["field_bytes"] / 1e6)},
+        "grid_point_steps_per_s": steps_s * gp,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": hbm_peak, "unit": "GB/s",
+                     "frac": d["gbs"] / hbm_peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": d["bytes_per_launch"], "avg_launch_us": d["avg_us"],
+                     "peak_source": peak_src},
+        "step_roofline": {"model_bytes_per_gp_step": 72 * (8 if main == "fp64" else 4),
+                          "achieved": model_bytes / step_time / 1e9, "peak": hbm_peak,
+                          "frac": model_bytes / step_time / 1e9 / hbm_peak},
+        "passes": {k: {kk: round(vv, 3) for kk, vv in v.items()} for k, v in per_pass.items()},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+    }
+    if e2e:
+        line["e2e"] = {"value": e2e[0] * world, "unit": UNIT, "h2d_bytes_per_step": e2e[1],
+                       "d2h_bytes_per_step": e2e[2]}
+    for prec in args.precisions[1:]:
+        rr = results[prec]
+        line.setdefault("variants", {})[prec] = {
+            "value": world * args.steps / (rr["ms"] / 1e3), "ms_per_step": rr["ms"] / args.steps,
+            "gpu_launches": rr["launches"], "clocks": rr["clocks"]}
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import dnsbox_oracle as O
+        rate, done, el = cpu_reference_rate(n, 3, budget_s=args.cpu_budget, warmup=0)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": O.WORKERS, "kind": "port",
+                                "sample": f"{done} Heun step(s) of the {n}^3 workload, {el:.1f} s, NumPy/"
+                                          f"scipy.fft restatement of rhs.f90 + dnsboxheun.f90"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--precisions", default="fp64,fp32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--ref-budget", type=float, default=90.0)
+    args = ap.parse_args()
+    args.precisions = args.precisions.split(",")
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    global torch
+    import torch
+    dist_on = world > 1
+    if args.impl == "reference":
+        # rank 0 alone times the CPU reference; the other ranks exit without work
+        run_reference(args, rank, world)
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if dist_on:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    try:
+        run_ours(args, rank, world, dist_on)
+    finally:
+        if dist_on:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

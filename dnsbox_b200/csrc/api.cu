@@ -1,0 +1,1300 @@
+// C ABI of libdnsbox_gpu.so: context, buffers, step orchestration and the
+// small reduction / layout kernels.  See include/dnsbox.h for the contract.
+//
+// One right-hand side (rhs_nonlinear, rhs.f90:18-135) is five passes over HBM:
+//   A  inverse z FFT of u, v, w, -dz v, dz u          (3 fields in, 5 out)
+//   B  inverse y FFT, forming omega_x, dz u, -dy u     (5 in, 6 out)
+//   C  inverse x C2R, (omega x u)*s, max|u_i|, forward x R2C  (6 in, 3 out)
+//   D  forward y FFT                                   (3 in, 3 out)
+//   E  forward z FFT + dealias + projection + forcing + stepper + E/D sums
+// instead of the reference's 15 p3dfft transforms plus pointwise loops.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dnsbox.h"
+#include "launch.cuh"
+
+using namespace dnsbox;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+static int set_err(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                           \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return set_err(e_ == cudaErrorMemoryAllocation ? DNSBOX_ERR_OOM : DNSBOX_ERR_CUDA,  \
+                     "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));   \
+  } while (0)
+
+#define RET(call)                     \
+  do {                                \
+    int r_ = (call);                  \
+    if (r_ != DNSBOX_OK) return r_;   \
+  } while (0)
+
+// ------------------------------------------------------------------ context
+struct dnsbox_ctx {
+  dnsbox_params p;
+  int fp64;                 // 1: complex double, 0: complex float
+  size_t cbytes;            // bytes per complex element
+  size_t nh, np;            // elements per spectral / physical field
+  int nxh;
+  cudaStream_t stream = 0;
+  char *W1 = nullptr, *W2 = nullptr;     // 6 spectral fields each
+  char *ustar = nullptr, *nold = nullptr;
+  char *tw[3] = {nullptr, nullptr, nullptr};
+  StepState *st = nullptr;               // device
+  double *partials = nullptr;            // device, 2 per finish CTA
+  int npartials = 0;
+  double *red = nullptr;                 // device scratch for diagnostics
+  size_t red_cap = 0;
+  int *band = nullptr;                   // band-mode index triples
+  int nband = 0;
+  dnsbox_diag *ddiag = nullptr;          // device per-step records
+  int ddiag_cap = 0;
+  double *hstage = nullptr;              // pinned host staging (8 doubles)
+  int nspec = 0;
+  int ab2_started = 0;
+  int cfl_first = 1;                     // reference calls set_time_step before the loop
+  // measurement
+  int prof_on = 0;
+  std::vector<cudaEvent_t> ev_pool;      // pairs
+  std::vector<int> ev_kind;
+  size_t ev_used = 0;
+  int64_t launches[DNSBOX_NPASS] = {0};
+  int64_t total_launches = 0;
+};
+
+// brackets a launch of pass `kind` with events when profiling is on
+struct Prof {
+  dnsbox_ctx *c;
+  int kind;
+  size_t slot;
+  int nl;
+  Prof(dnsbox_ctx *c_, int k, int nlaunch = 1) : c(c_), kind(k), slot((size_t)-1), nl(nlaunch) {
+    c->launches[kind] += nl;
+    c->total_launches += nl;
+    if (!c->prof_on) return;
+    if (2 * (c->ev_used + 1) > c->ev_pool.size()) {
+      for (int i = 0; i < 64; ++i) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        c->ev_pool.push_back(e);
+      }
+      c->ev_kind.resize(c->ev_pool.size() / 2);
+    }
+    slot = c->ev_used++;
+    c->ev_kind[slot] = kind;
+    cudaEventRecord(c->ev_pool[2 * slot], c->stream);
+  }
+  ~Prof() {
+    if (slot != (size_t)-1) cudaEventRecord(c->ev_pool[2 * slot + 1], c->stream);
+  }
+};
+
+static const int kSizes[] = {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 512, 1024};
+
+extern "C" int dnsbox_supported_size(int n) {
+  for (int s : kSizes)
+    if (s == n) return 1;
+  return 0;
+}
+
+extern "C" int dnsbox_abi_version(void) { return DNSBOX_ABI_VERSION; }
+extern "C" const char *dnsbox_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" void dnsbox_default_params(dnsbox_params *p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  // parameters.f90:11-50
+  p->nx = p->ny = p->nz = 128;
+  p->precision = DNSBOX_FP64;
+  p->stepper = DNSBOX_HEUN;
+  p->ab2_mode = DNSBOX_AB2_REFERENCE;
+  p->bandlim = 1;
+  p->spherical = 0;
+  p->tstep_fix = 0;
+  p->hminone = 1;
+  p->spectrum_mode = DNSBOX_SPECTRUM_MPI;
+  p->adj_phat = DNSBOX_ADJ_PHAT_INTENT;
+  p->alpha_x = p->alpha_y = p->alpha_z = 1.0;
+  p->nu = 0.005;
+  p->Q = 0.0;
+  p->kCutOff = 2.0;
+  p->Pin = 0.1;
+  p->Deltak = 1.0;
+  p->courant_min = 0.15;
+  p->courant_max = 0.2;
+  p->dt_max = 1.0e-2;
+  p->dt = 1.0e-3;   // variables.f90:9
+}
+
+// ------------------------------------------------------------- dispatch
+template <typename T> struct Ops {
+#define DNSBOX_CASE_STRIDED(NN) \
+  case NN: return Launcher<T, NN>::strided(a, inv, ntiles, st);
+  static cudaError_t strided(int n, const StridedArgs<T> &a, bool inv, int ntiles, cudaStream_t st) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_STRIDED) }
+    return cudaErrorInvalidValue;
+  }
+#define DNSBOX_CASE_NL(NN) \
+  case NN: return Launcher<T, NN>::xline_nl(a, st);
+  static cudaError_t xline_nl(int n, const XlineNLArgs<T> &a, cudaStream_t st) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_NL) }
+    return cudaErrorInvalidValue;
+  }
+#define DNSBOX_CASE_C2R(NN) \
+  case NN: return Launcher<T, NN>::xline_c2r(a, nf, st);
+  static cudaError_t xline_c2r(int n, const XlineArgs<T> &a, int nf, cudaStream_t st) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_C2R) }
+    return cudaErrorInvalidValue;
+  }
+#define DNSBOX_CASE_R2C(NN) \
+  case NN: return Launcher<T, NN>::xline_r2c(a, nf, st);
+  static cudaError_t xline_r2c(int n, const XlineArgs<T> &a, int nf, cudaStream_t st) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_R2C) }
+    return cudaErrorInvalidValue;
+  }
+#define DNSBOX_CASE_FIN(NN) \
+  case NN: return Launcher<T, NN>::zfinish(a, nb, st);
+  static cudaError_t zfinish(int n, const FinishArgs<T> &a, int nb, cudaStream_t st) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_FIN) }
+    return cudaErrorInvalidValue;
+  }
+};
+
+// ------------------------------------------------------------ small kernels
+template <typename C>
+__global__ void k_eband(const C *u, long long nh, const int *band, int nband, int nx, StepState *st,
+                        double s2, int reset_umax) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  // band[] holds (offset, kx) pairs flattened as ints: off_lo, off_hi, kx
+  for (int i = threadIdx.x; i < nband; i += blockDim.x) {
+    const long long off = (long long)(unsigned)band[3 * i] | ((long long)band[3 * i + 1] << 32);
+    const int kx = band[3 * i + 2];
+    const double w = (k_half(kx, nx, 1.0) == 0.0) ? 0.5 : 1.0;   // rhs.f90:151-155
+    double e = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      const C v = u[c * nh + off];
+      e += ((double)v.x * v.x + (double)v.y * v.y) * w;
+    }
+    acc += e;
+  }
+  double v[1] = {acc};
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) {
+    st->eband = v[0] * s2;
+    if (reset_umax) st->umax[0] = st->umax[1] = st->umax[2] = 0.0;
+  }
+}
+
+// io_Courant (io.f90:664-676) on the fused max|u_i| and, when control is on,
+// set_time_step (dnsboxheun.f90:153-157, 227-246).
+__global__ void k_cfl(StepState *st, double dx, double dy, double dz, int control, int force,
+                      double cmin, double cmax, double dtmax, dnsbox_diag *drec) {
+  if (threadIdx.x != 0) return;
+  double dt = st->dt;
+  double C = st->umax[0] * dt / dx + st->umax[1] * dt / dy + st->umax[2] * dt / dz;
+  if (control && (force || C > cmax || (C < cmin && dt < dtmax))) {
+    double nd = ((cmax + cmin) / (2.0 * C)) * dt;
+    if (nd > dtmax) nd = dtmax;
+    C = C * nd / dt;
+    st->dt = nd;
+    dt = nd;
+  }
+  st->courant = C;
+  st->eband1 = st->eband;
+  if (drec) {
+    drec->courant = C;
+    drec->umax[0] = st->umax[0];
+    drec->umax[1] = st->umax[1];
+    drec->umax[2] = st->umax[2];
+    drec->eband = st->eband;
+    drec->dt = dt;
+  }
+}
+
+// Sums the finish-kernel partials (fixed order), writes the step record and
+// advances the clock.
+__global__ void k_finalize(StepState *st, const double *partials, int np, double s2, double nu,
+                           double Q, double Pin, int bandlim, dnsbox_diag *drec) {
+  __shared__ double red[2 * 32];
+  double e = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    e += partials[2 * i];
+    d += partials[2 * i + 1];
+  }
+  double v[2] = {e, d};
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    const double E = v[0] * s2, D = nu * v[1] * s2;
+    const double dt = st->dt;
+    if (drec) {
+      drec->t = st->t + dt;
+      drec->dt = dt;
+      drec->ekin = E;
+      drec->dissipation = D;
+      drec->production_literal = 2.0 * Q * E;
+      drec->injected_power = (bandlim ? Pin : 0.0) + 2.0 * Q * E;
+      drec->nonfinite = !(isfinite(E) && isfinite(D));
+      drec->step = (int)st->step + 1;
+    }
+    st->t_prev = st->t;
+    st->t = st->t + dt;
+    st->step += 1.0;
+  }
+}
+
+// Spectral diagnostics over the half spectrum: shell spectrum (state.f90:350-411
+// or single/state.f90:191-230), EZero/EOne/Esqrt2, kinetic energy
+// (state.f90:429-454) and the Parseval dissipation sum.  Per-block partials
+// [gridDim][NV], NV = nspec + 5.
+template <typename C>
+__global__ void k_specdiag(const C *u, long long nh, int nx, int ny, int nz, double ax, double ay,
+                           double az, int nspec, double deltak, int single, double s2,
+                           double *partials) {
+  extern __shared__ double hist[];
+  const int NV = nspec + 5;
+  for (int i = threadIdx.x; i < NV; i += blockDim.x) hist[i] = 0.0;
+  __syncthreads();
+  const int nxh = nx / 2 + 1;
+  const double sq2 = sqrt(2.0);
+  double ez = 0, e1 = 0, es = 0, ek = 0, dk = 0;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(m % nxh);
+    const int ky = (int)((m / nxh) % ny);
+    const int kz = (int)(m / ((long long)nxh * ny));
+    const double kxr = k_half(kx, nx, ax), kyr = k_full(ky, ny, ay), kzr = k_full(kz, nz, az);
+    const double k2 = kxr * kxr + kyr * kyr + kzr * kzr;
+    const double absk = sqrt(k2);
+    double e2 = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      const C v = u[c * nh + m];
+      e2 += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    const double w = (kxr == 0.0) ? 0.5 : 1.0;
+    ek += w * e2;
+    dk += 2.0 * w * k2 * e2;
+    const double base = floor(absk / deltak);
+    const int nk = (absk < base + 0.5 * deltak) ? (int)base : (int)base + 1;
+    if (!single) {
+      if (absk == 0.0) ez += e2;
+      if (absk == 1.0) e1 += e2;
+      if (absk - sq2 < 1.0e-9) es += e2;
+      if (nk < nspec && nk != 0) atomicAdd(&hist[nk - 1], e2 * s2 / deltak);
+    } else {
+      if (absk == 0.0) ez += w * e2;
+      if (nk <= nspec && nk != 0) atomicAdd(&hist[nk - 1], w * e2 * s2 / deltak);
+    }
+  }
+  __shared__ double red[5 * 32];
+  double v[5] = {ez, e1, es, ek, dk};
+  block_sum<5>(v, red);
+  if (threadIdx.x == 0)
+    for (int i = 0; i < 5; ++i) hist[nspec + i] = v[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < NV; i += blockDim.x) partials[(long long)blockIdx.x * NV + i] = hist[i];
+}
+
+__global__ void k_sum_partials(const double *partials, int nblk, int nv, double *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += partials[(long long)b * nv + i];
+    out[i] = s;
+  }
+}
+
+// max (signed or |.|) of a real array: per-block partials
+template <typename T>
+__global__ void k_max(const T *f, long long n, int absval, double *partials) {
+  __shared__ double red[32];
+  double m = -INFINITY;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double x = (double)f[i];
+    m = fmax(m, absval ? fabs(x) : x);
+  }
+  m = warp_max(m);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = m;
+  __syncthreads();
+  if (wid == 0) {
+    double x = lane < (int)(blockDim.x >> 5) ? red[lane] : -INFINITY;
+    x = warp_max(x);
+    if (lane == 0) partials[blockIdx.x] = x;
+  }
+}
+
+__global__ void k_max_partials(const double *partials, int nblk, double *out) {
+  __shared__ double red[32];
+  double m = -INFINITY;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) m = fmax(m, partials[i]);
+  m = warp_max(m);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = m;
+  __syncthreads();
+  if (wid == 0) {
+    double x = lane < (int)(blockDim.x >> 5) ? red[lane] : -INFINITY;
+    x = warp_max(x);
+    if (lane == 0) *out = x;
+  }
+}
+
+// state_project (state.f90:120-179), in place
+template <typename C>
+__global__ void k_project(C *u, long long nh, int nx, int ny, int nz, double ax, double ay, double az) {
+  using T = decltype(C{}.x);
+  const int nxh = nx / 2 + 1;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(m % nxh), ky = (int)((m / nxh) % ny), kz = (int)(m / ((long long)nxh * ny));
+    const double kr[3] = {k_half(kx, nx, ax), k_full(ky, ny, ay), k_full(kz, nz, az)};
+    if (kr[0] == 0.0 && kr[1] == 0.0 && kr[2] == 0.0) continue;
+    const double k2 = kr[0] * kr[0] + kr[1] * kr[1] + kr[2] * kr[2];
+    const C v[3] = {u[m], u[nh + m], u[2 * nh + m]};
+    for (int i = 0; i < 3; ++i) {
+      double re = v[i].x, im = v[i].y;
+      for (int j = 0; j < 3; ++j) {
+        re -= (kr[i] * kr[j] * (double)v[j].x) / k2;
+        im -= (kr[i] * kr[j] * (double)v[j].y) / k2;
+      }
+      u[i * nh + m] = mkc<C>(T(re), T(im));
+    }
+  }
+}
+
+// state_dealias (state.f90:181-209), in place
+template <typename C>
+__global__ void k_dealias(C *u, long long nh, int nx, int ny, int nz, double ax, double ay, double az,
+                          int spherical, double cx, double cy, double cz, double sph2) {
+  const int nxh = nx / 2 + 1;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(m % nxh), ky = (int)((m / nxh) % ny), kz = (int)(m / ((long long)nxh * ny));
+    const double kxr = k_half(kx, nx, ax), kyr = k_full(ky, ny, ay), kzr = k_full(kz, nz, az);
+    const double k2 = kxr * kxr + kyr * kyr + kzr * kzr;
+    const bool cut = (spherical && k2 >= sph2) || fabs(kxr) >= cx || fabs(kyr) >= cy ||
+                     fabs(kzr) >= cz || (kxr == 0.0 && kyr == 0.0 && kzr == 0.0);
+    if (cut)
+      for (int c = 0; c < 3; ++c) u[c * nh + m] = mkc<C>(0, 0);
+  }
+}
+
+// (i k . u) * s for one field (divergence)
+template <typename C>
+__global__ void k_divhat(const C *u, C *out, long long nh, int nx, int ny, int nz, double ax, double ay,
+                         double az, double s) {
+  using T = decltype(C{}.x);
+  const int nxh = nx / 2 + 1;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(m % nxh), ky = (int)((m / nxh) % ny), kz = (int)(m / ((long long)nxh * ny));
+    const double kr[3] = {k_half(kx, nx, ax), k_full(ky, ny, ay), k_full(kz, nz, az)};
+    double re = 0, im = 0;
+    for (int c = 0; c < 3; ++c) {
+      const C v = u[c * nh + m];
+      re += -kr[c] * s * (double)v.y;
+      im += kr[c] * s * (double)v.x;
+    }
+    out[m] = mkc<C>(T(re), T(im));
+  }
+}
+
+// p3dfft STRIDE1 host layout [c][kx][ky][kz] (complex double) <-> internal [c][kz][ky][kx]
+template <typename C>
+__global__ void k_from_p3dfft(const double2 *src, C *dst, int nxh, int ny, int nz) {
+  using T = decltype(C{}.x);
+  __shared__ double2 tile[32][33];
+  const int c = blockIdx.z / ny, ky = blockIdx.z % ny;
+  const int kz0 = blockIdx.x * 32, kx0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int kx = kx0 + i, kz = kz0 + threadIdx.x;
+    if (kx < nxh && kz < nz)
+      tile[i][threadIdx.x] = src[(((long long)c * nxh + kx) * ny + ky) * nz + kz];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int kz = kz0 + i, kx = kx0 + threadIdx.x;
+    if (kx < nxh && kz < nz) {
+      const double2 v = tile[threadIdx.x][i];
+      dst[(((long long)c * nz + kz) * ny + ky) * nxh + kx] = mkc<C>(T(v.x), T(v.y));
+    }
+  }
+}
+
+template <typename C>
+__global__ void k_to_p3dfft(const C *src, double2 *dst, int nxh, int ny, int nz) {
+  __shared__ double2 tile[32][33];
+  const int c = blockIdx.z / ny, ky = blockIdx.z % ny;
+  const int kz0 = blockIdx.x * 32, kx0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int kz = kz0 + i, kx = kx0 + threadIdx.x;
+    if (kx < nxh && kz < nz) {
+      const C v = src[(((long long)c * nz + kz) * ny + ky) * nxh + kx];
+      tile[i][threadIdx.x] = make_double2((double)v.x, (double)v.y);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int kx = kx0 + i, kz = kz0 + threadIdx.x;
+    if (kx < nxh && kz < nz) dst[(((long long)c * nxh + kx) * ny + ky) * nz + kz] = tile[threadIdx.x][i];
+  }
+}
+
+template <typename A, typename B>
+__global__ void k_convert(const A *src, B *dst, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (B)src[i];
+}
+
+// ---------------------------------------------------------------- helpers
+static inline int grid_for(long long n, int threads = 256, int cap = 148 * 16) {
+  long long b = (n + threads - 1) / threads;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+static char *field(char *base, const dnsbox_ctx *c, int slot) { return base + (size_t)slot * c->nh * c->cbytes; }
+static const char *cfield(const char *base, const dnsbox_ctx *c, int slot) {
+  return base + (size_t)slot * c->nh * c->cbytes;
+}
+
+static int ensure_red(dnsbox_ctx *c, size_t ndoubles) {
+  if (ndoubles <= c->red_cap) return DNSBOX_OK;
+  if (c->red) cudaFree(c->red);
+  c->red = nullptr;
+  CK(cudaMalloc(&c->red, ndoubles * sizeof(double)));
+  c->red_cap = ndoubles;
+  return DNSBOX_OK;
+}
+
+static int ensure_diag(dnsbox_ctx *c, int n) {
+  if (n <= c->ddiag_cap) return DNSBOX_OK;
+  if (c->ddiag) cudaFree(c->ddiag);
+  c->ddiag = nullptr;
+  CK(cudaMalloc(&c->ddiag, (size_t)n * sizeof(dnsbox_diag)));
+  c->ddiag_cap = n;
+  return DNSBOX_OK;
+}
+
+template <typename T> static StridedArgs<T> strided_base(const dnsbox_ctx *c, int axis) {
+  StridedArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  a.ncols = c->nxh;
+  a.nx = c->p.nx;
+  a.alpha_x = c->p.alpha_x;
+  if (axis == 2) {  // z: rows kz/z, tiles over y
+    a.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[2]);
+    a.rowstride = (long long)c->p.ny * c->nxh;
+    a.otherstride = c->nxh;
+    a.alpha_row = c->p.alpha_z;
+  } else {          // y: rows ky/y, tiles over z
+    a.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[1]);
+    a.rowstride = c->nxh;
+    a.otherstride = (long long)c->p.ny * c->nxh;
+    a.alpha_row = c->p.alpha_y;
+  }
+  return a;
+}
+
+template <typename T>
+static void set_job(StridedArgs<T> &a, int j, const void *in1, void *out, double a1 = 1, double b1 = 0,
+                    int ks1 = 0, const void *in2 = nullptr, double a2 = 1, double b2 = 0, int ks2 = 0) {
+  using C = typename CT<T>::type;
+  a.job[j].in1 = reinterpret_cast<const C *>(in1);
+  a.job[j].in2 = reinterpret_cast<const C *>(in2);
+  a.job[j].out = reinterpret_cast<C *>(out);
+  a.job[j].a1 = a1;
+  a.job[j].b1 = b1;
+  a.job[j].ks1 = ks1;
+  a.job[j].a2 = a2;
+  a.job[j].b2 = b2;
+  a.job[j].ks2 = ks2;
+}
+
+template <typename T>
+static int run_strided(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<T> &a,
+                       int kind = DNSBOX_PASS_OTHER) {
+  const int ntx = (c->nxh + TileCols<T>::v - 1) / TileCols<T>::v;
+  const int nother = axis == 2 ? c->p.ny : c->p.nz;
+  const int n = axis == 2 ? c->p.nz : c->p.ny;
+  Prof pr(c, kind);
+  CK(Ops<T>::strided(n, a, inv, ntx * nother, c->stream));
+  return DNSBOX_OK;
+}
+
+// 3D C2R of nf spectral fields (in[] -> out[] physical), through W1/W2.
+// Inputs must not live in W1 slots [0, nf) or W2 slots [0, nf).
+template <typename T>
+static int c2r_fields(dnsbox_ctx *c, int nf, const void *const *in, void *const *out, double scale) {
+  StridedArgs<T> a = strided_base<T>(c, 2);
+  a.njobs = nf;
+  for (int f = 0; f < nf; ++f) set_job<T>(a, f, in[f], field(c->W1, c, f));
+  RET(run_strided<T>(c, 2, true, a));
+  StridedArgs<T> b = strided_base<T>(c, 1);
+  b.njobs = nf;
+  for (int f = 0; f < nf; ++f) set_job<T>(b, f, field(c->W1, c, f), field(c->W2, c, f));
+  RET(run_strided<T>(c, 1, true, b));
+  XlineArgs<T> x;
+  memset(&x, 0, sizeof(x));
+  for (int f = 0; f < nf; ++f) {
+    x.in[f] = field(c->W2, c, f);
+    x.out[f] = out[f];
+  }
+  x.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[0]);
+  x.nlines = c->p.ny * c->p.nz;
+  x.nxh = c->nxh;
+  x.scale = scale;
+  Prof pr(c, DNSBOX_PASS_OTHER);
+  CK(Ops<T>::xline_c2r(c->p.nx, x, nf, c->stream));
+  return DNSBOX_OK;
+}
+
+// 3D R2C of nf physical fields.  Inputs must not live in W1 slots [0, nf).
+template <typename T>
+static int r2c_fields(dnsbox_ctx *c, int nf, const void *const *in, void *const *out) {
+  XlineArgs<T> x;
+  memset(&x, 0, sizeof(x));
+  for (int f = 0; f < nf; ++f) {
+    x.in[f] = in[f];
+    x.out[f] = field(c->W1, c, f);
+  }
+  x.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[0]);
+  x.nlines = c->p.ny * c->p.nz;
+  x.nxh = c->nxh;
+  x.scale = 1.0;
+  {
+    Prof pr(c, DNSBOX_PASS_OTHER);
+    CK(Ops<T>::xline_r2c(c->p.nx, x, nf, c->stream));
+  }
+  StridedArgs<T> b = strided_base<T>(c, 1);
+  b.njobs = nf;
+  for (int f = 0; f < nf; ++f) set_job<T>(b, f, field(c->W1, c, f), field(c->W2, c, f));
+  RET(run_strided<T>(c, 1, false, b));
+  StridedArgs<T> a = strided_base<T>(c, 2);
+  a.njobs = nf;
+  for (int f = 0; f < nf; ++f) set_job<T>(a, f, field(c->W2, c, f), out[f]);
+  RET(run_strided<T>(c, 2, false, a));
+  return DNSBOX_OK;
+}
+
+template <typename T> static FinishArgs<T> finish_base(const dnsbox_ctx *c) {
+  FinishArgs<T> f;
+  memset(&f, 0, sizeof(f));
+  const dnsbox_params &p = c->p;
+  f.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[2]);
+  f.nh = (long long)c->nh;
+  f.nx = p.nx;
+  f.ny = p.ny;
+  f.nz = p.nz;
+  f.nxh = c->nxh;
+  f.ax = p.alpha_x;
+  f.ay = p.alpha_y;
+  f.az = p.alpha_z;
+  f.nu = p.nu;
+  f.Q = p.Q;
+  f.Pin = p.Pin;
+  f.kcut = p.kCutOff;
+  // rhs.f90:74-88
+  f.cutx = (p.nx / 2.0) * (2.0 * p.alpha_x / 3.0);
+  f.cuty = (p.ny / 2.0) * (2.0 * p.alpha_y / 3.0);
+  f.cutz = (p.nz / 2.0) * (2.0 * p.alpha_z / 3.0);
+  f.sph2 = pow((p.nx / 2.0) * 0.5 * p.alpha_x, 2);
+  f.bandlim = p.bandlim;
+  f.spherical = p.spherical;
+  f.ab2_standard = p.ab2_mode == DNSBOX_AB2_STANDARD;
+  f.s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  f.st = c->st;
+  return f;
+}
+
+// One right-hand side: passes A-E.  cfl: 0 none, 1 record (+control).
+template <typename T>
+static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *state, void *nold,
+                   bool partials, int cfl, dnsbox_diag *drec) {
+  using C = typename CT<T>::type;
+  const dnsbox_params &p = c->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  // rhs_Eband (rhs.f90:22-24) and reset of the CFL maxima
+  if (p.bandlim) {
+    Prof pr(c, DNSBOX_PASS_SMALL);
+    k_eband<C><<<1, 256, 0, c->stream>>>(reinterpret_cast<const C *>(uin), (long long)c->nh, c->band,
+                                         c->nband, p.nx, c->st, s * s, 1);
+  } else {
+    CK(cudaMemsetAsync(&c->st->umax[0], 0, 3 * sizeof(double), c->stream));
+  }
+  CK(cudaGetLastError());
+  const char *u = reinterpret_cast<const char *>(uin);
+  // pass A: inverse z
+  StridedArgs<T> a = strided_base<T>(c, 2);
+  a.njobs = 5;
+  set_job<T>(a, 0, cfield(u, c, 0), field(c->W1, c, 0));
+  set_job<T>(a, 1, cfield(u, c, 1), field(c->W1, c, 1));
+  set_job<T>(a, 2, cfield(u, c, 2), field(c->W1, c, 2));
+  set_job<T>(a, 3, cfield(u, c, 1), field(c->W1, c, 3), 0.0, -s, 1);   // -dz v
+  set_job<T>(a, 4, cfield(u, c, 0), field(c->W1, c, 4), 0.0, s, 1);    //  dz u
+  RET(run_strided<T>(c, 2, true, a, DNSBOX_PASS_Z_INV));
+  // pass B: inverse y
+  StridedArgs<T> b = strided_base<T>(c, 1);
+  b.njobs = 6;
+  set_job<T>(b, 0, field(c->W1, c, 0), field(c->W2, c, 0));
+  set_job<T>(b, 1, field(c->W1, c, 1), field(c->W2, c, 1));
+  set_job<T>(b, 2, field(c->W1, c, 2), field(c->W2, c, 2));
+  set_job<T>(b, 3, field(c->W1, c, 2), field(c->W2, c, 3), 0.0, s, 1, field(c->W1, c, 3));  // omega_x
+  set_job<T>(b, 4, field(c->W1, c, 4), field(c->W2, c, 4));
+  set_job<T>(b, 5, field(c->W1, c, 0), field(c->W2, c, 5), 0.0, -s, 1);                     // -dy u
+  RET(run_strided<T>(c, 1, true, b, DNSBOX_PASS_Y_INV));
+  // pass C: fused x pass
+  XlineNLArgs<T> x;
+  memset(&x, 0, sizeof(x));
+  x.U = reinterpret_cast<const C *>(field(c->W2, c, 0));
+  x.V = reinterpret_cast<const C *>(field(c->W2, c, 1));
+  x.W = reinterpret_cast<const C *>(field(c->W2, c, 2));
+  x.OX = reinterpret_cast<const C *>(field(c->W2, c, 3));
+  x.B1 = reinterpret_cast<const C *>(field(c->W2, c, 4));
+  x.C1 = reinterpret_cast<const C *>(field(c->W2, c, 5));
+  x.NX = reinterpret_cast<C *>(field(c->W1, c, 0));
+  x.NY = reinterpret_cast<C *>(field(c->W1, c, 1));
+  x.NZ = reinterpret_cast<C *>(field(c->W1, c, 2));
+  x.tw = reinterpret_cast<const C *>(c->tw[0]);
+  x.umax = &c->st->umax[0];
+  x.nlines = p.ny * p.nz;
+  x.nxh = c->nxh;
+  x.alpha_x = p.alpha_x;
+  x.s = s;
+  {
+    Prof pr(c, DNSBOX_PASS_X_NL);
+    CK(Ops<T>::xline_nl(p.nx, x, c->stream));
+  }
+  if (cfl) {
+    const double dx = (2 * M_PI / p.alpha_x) / p.nx, dy = (2 * M_PI / p.alpha_y) / p.ny,
+                 dz = (2 * M_PI / p.alpha_z) / p.nz;
+    Prof pr(c, DNSBOX_PASS_SMALL);
+    k_cfl<<<1, 32, 0, c->stream>>>(c->st, dx, dy, dz, !p.tstep_fix, c->cfl_first, p.courant_min,
+                                   p.courant_max, p.dt_max, drec);
+    CK(cudaGetLastError());
+    c->cfl_first = 0;
+  }
+  // pass D: forward y
+  StridedArgs<T> d = strided_base<T>(c, 1);
+  d.njobs = 3;
+  for (int f = 0; f < 3; ++f) set_job<T>(d, f, field(c->W1, c, f), field(c->W2, c, f));
+  RET(run_strided<T>(c, 1, false, d, DNSBOX_PASS_Y_FWD));
+  // pass E: forward z + spectral finish
+  FinishArgs<T> e = finish_base<T>(c);
+  e.n3 = reinterpret_cast<const C *>(c->W2);
+  e.uin = reinterpret_cast<const C *>(uin);
+  e.out = reinterpret_cast<C *>(out);
+  e.state = reinterpret_cast<C *>(state);
+  e.nold = reinterpret_cast<C *>(nold);
+  e.partials = partials ? c->partials : nullptr;
+  e.mode = mode;
+  const int ntx = (c->nxh + TileCols<T>::v - 1) / TileCols<T>::v;
+  Prof pr(c, DNSBOX_PASS_Z_FIN);
+  CK(Ops<T>::zfinish(p.nz, e, ntx * p.ny, c->stream));
+  return DNSBOX_OK;
+}
+
+template <typename T> static int step_impl(dnsbox_ctx *c, void *uh, int nsteps, dnsbox_diag *dh) {
+  const dnsbox_params &p = c->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  if (dh) RET(ensure_diag(c, nsteps));
+  for (int n = 0; n < nsteps; ++n) {
+    dnsbox_diag *drec = dh ? c->ddiag + n : nullptr;
+    const bool pc = (p.stepper == DNSBOX_HEUN) || !c->ab2_started;
+    if (pc) {
+      // dnsboxheun.f90:85-126 (and dnsbox.f90:87-141 for the AB2 first step)
+      RET(run_rhs<T>(c, uh, FIN_PRED, c->ustar, nullptr, p.stepper == DNSBOX_AB2 ? c->nold : nullptr,
+                     false, 1, drec));
+      RET(run_rhs<T>(c, c->ustar, FIN_CORR, nullptr, uh, nullptr, true, 0, nullptr));
+      if (p.stepper == DNSBOX_AB2) c->ab2_started = 1;
+    } else {
+      // dnsbox.f90:143-191
+      RET(run_rhs<T>(c, uh, FIN_AB2, nullptr, uh, c->nold, true, 1, drec));
+    }
+    const int ntx = (c->nxh + TileCols<T>::v - 1) / TileCols<T>::v;
+    Prof pr(c, DNSBOX_PASS_SMALL);
+    k_finalize<<<1, 1024, 0, c->stream>>>(c->st, c->partials, ntx * p.ny, s * s, p.nu, p.Q, p.Pin,
+                                          p.bandlim, drec);
+    CK(cudaGetLastError());
+  }
+  if (dh) {
+    CK(cudaMemcpyAsync(dh, c->ddiag, (size_t)nsteps * sizeof(dnsbox_diag), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int n = 0; n < nsteps; ++n)
+      if (dh[n].nonfinite) return set_err(DNSBOX_ERR_NONFINITE, "non-finite energy at step %d", dh[n].step);
+  }
+  return DNSBOX_OK;
+}
+
+// --------------------------------------------------------------- create
+static int alloc_twiddles(dnsbox_ctx *c, int axis, int n) {
+  std::vector<double> h(2 * (size_t)n);
+  for (int j = 0; j < n; ++j) {
+    const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)j / (long double)n;
+    h[2 * j] = (double)cosl(a);
+    h[2 * j + 1] = (double)sinl(a);
+  }
+  CK(cudaMalloc(&c->tw[axis], (size_t)n * c->cbytes));
+  if (c->fp64) {
+    CK(cudaMemcpy(c->tw[axis], h.data(), (size_t)n * 16, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(2 * (size_t)n);
+    for (size_t i = 0; i < f.size(); ++i) f[i] = (float)h[i];
+    CK(cudaMemcpy(c->tw[axis], f.data(), (size_t)n * 8, cudaMemcpyHostToDevice));
+  }
+  return DNSBOX_OK;
+}
+
+static void free_ctx(dnsbox_ctx *c) {
+  if (!c) return;
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  cudaFree(c->W1);
+  cudaFree(c->W2);
+  cudaFree(c->ustar);
+  cudaFree(c->nold);
+  for (int i = 0; i < 3; ++i) cudaFree(c->tw[i]);
+  cudaFree(c->st);
+  cudaFree(c->partials);
+  cudaFree(c->red);
+  cudaFree(c->band);
+  cudaFree(c->ddiag);
+  if (c->hstage) cudaFreeHost(c->hstage);
+  delete c;
+}
+
+extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
+  if (!p || !out) return set_err(DNSBOX_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (!dnsbox_supported_size(p->nx) || !dnsbox_supported_size(p->ny) || !dnsbox_supported_size(p->nz))
+    return set_err(DNSBOX_ERR_SIZE, "unsupported grid %dx%dx%d", p->nx, p->ny, p->nz);
+  if (p->precision != DNSBOX_FP64 && p->precision != DNSBOX_FP32)
+    return set_err(DNSBOX_ERR_UNSUPPORTED, "precision %d not available", p->precision);
+  if (!(p->nu >= 0.0) || !(p->Deltak > 0.0) || !(p->dt > 0.0) || !(p->alpha_x > 0) || !(p->alpha_y > 0) ||
+      !(p->alpha_z > 0))
+    return set_err(DNSBOX_ERR_ARG, "invalid physical parameter");
+  if (p->stepper != DNSBOX_HEUN && p->stepper != DNSBOX_AB2)
+    return set_err(DNSBOX_ERR_ARG, "invalid stepper %d", p->stepper);
+  CK(cudaSetDevice(p->device));
+  dnsbox_ctx *c = new dnsbox_ctx();
+  c->p = *p;
+  c->fp64 = p->precision == DNSBOX_FP64;
+  c->cbytes = c->fp64 ? 16 : 8;
+  c->nxh = p->nx / 2 + 1;
+  c->nh = (size_t)p->nz * p->ny * c->nxh;
+  c->np = (size_t)p->nz * p->ny * p->nx;
+  int rc = DNSBOX_OK;
+  auto fail = [&](int r) {
+    free_ctx(c);
+    return r;
+  };
+  const size_t fb = c->nh * c->cbytes;
+  cudaError_t e;
+  if ((e = cudaMalloc(&c->W1, 6 * fb)) != cudaSuccess ||
+      (e = cudaMalloc(&c->W2, 6 * fb)) != cudaSuccess ||
+      (e = cudaMalloc(&c->ustar, 3 * fb)) != cudaSuccess ||
+      (p->stepper == DNSBOX_AB2 && (e = cudaMalloc(&c->nold, 3 * fb)) != cudaSuccess) ||
+      (e = cudaMalloc(&c->st, sizeof(StepState))) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed: %s", cudaGetErrorString(e)));
+  }
+  if ((rc = alloc_twiddles(c, 0, p->nx)) || (rc = alloc_twiddles(c, 1, p->ny)) ||
+      (rc = alloc_twiddles(c, 2, p->nz)))
+    return fail(rc);
+  const int ntx64 = (c->nxh + 7) / 8, ntx32 = (c->nxh + 15) / 16;
+  c->npartials = (c->fp64 ? ntx64 : ntx32) * p->ny;
+  if ((e = cudaMalloc(&c->partials, 2 * (size_t)c->npartials * sizeof(double))) != cudaSuccess)
+    return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed"));
+  // band modes |k| <= kCutOff (rhs.f90:145-149), stored as (offset lo, offset hi, kx)
+  std::vector<int> band;
+  auto cand = [](int n, double a, double kc, bool half) {
+    std::vector<int> v;
+    const int m = half ? n / 2 + 1 : n;
+    for (int i = 0; i < m; ++i) {
+      const double k = half ? k_half(i, n, a) : k_full(i, n, a);
+      if (fabs(k) <= kc) v.push_back(i);
+    }
+    return v;
+  };
+  if (p->bandlim) {
+    for (int kz : cand(p->nz, p->alpha_z, p->kCutOff, false))
+      for (int ky : cand(p->ny, p->alpha_y, p->kCutOff, false))
+        for (int kx : cand(p->nx, p->alpha_x, p->kCutOff, true)) {
+          const double a = k_half(kx, p->nx, p->alpha_x), b = k_full(ky, p->ny, p->alpha_y),
+                       cc = k_full(kz, p->nz, p->alpha_z);
+          if (sqrt(a * a + b * b + cc * cc) > p->kCutOff) continue;
+          const long long off = ((long long)kz * p->ny + ky) * c->nxh + kx;
+          band.push_back((int)(off & 0xffffffffLL));
+          band.push_back((int)(off >> 32));
+          band.push_back(kx);
+        }
+    c->nband = (int)band.size() / 3;
+    if (c->nband) {
+      if ((e = cudaMalloc(&c->band, band.size() * sizeof(int))) != cudaSuccess)
+        return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed"));
+      if ((e = cudaMemcpy(c->band, band.data(), band.size() * sizeof(int), cudaMemcpyHostToDevice)) !=
+          cudaSuccess)
+        return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
+    }
+  }
+  StepState hs;
+  memset(&hs, 0, sizeof(hs));
+  hs.dt = p->dt;
+  if ((e = cudaMemcpy(c->st, &hs, sizeof(hs), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
+  if ((e = cudaMallocHost(&c->hstage, 64 * sizeof(double))) != cudaSuccess)
+    return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
+  // variables.f90:112-123
+  if (p->spherical)
+    c->nspec = (int)(((p->nx / 2.0) * (2.0 * p->alpha_x / 3.0)) / p->Deltak) - 1;
+  else
+    c->nspec = (int)(sqrt(pow((p->nx / 2.0) * (2.0 * p->alpha_x / 3.0), 2) +
+                          pow((p->ny / 2.0) * (2.0 * p->alpha_y / 3.0), 2) +
+                          pow((p->nz / 2.0) * (2.0 * p->alpha_z / 3.0), 2)) /
+                     p->Deltak) -
+               1;
+  *out = c;
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_destroy(dnsbox_ctx *ctx) {
+  if (!ctx) return DNSBOX_OK;
+  cudaSetDevice(ctx->p.device);
+  cudaStreamSynchronize(ctx->stream);
+  free_ctx(ctx);
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_set_stream(dnsbox_ctx *ctx, void *stream) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  ctx->stream = reinterpret_cast<cudaStream_t>(stream);
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_field_bytes(const dnsbox_ctx *ctx, size_t *sb, size_t *pb) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  if (sb) *sb = ctx->nh * ctx->cbytes;
+  if (pb) *pb = ctx->np * ctx->cbytes / 2;
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_nspec(const dnsbox_ctx *ctx) { return ctx ? ctx->nspec : -1; }
+
+#define BEGIN(ctx)                                              \
+  if (!(ctx)) return set_err(DNSBOX_ERR_ARG, "null context");   \
+  CK(cudaSetDevice((ctx)->p.device));
+
+extern "C" int dnsbox_set_dt(dnsbox_ctx *ctx, double dt) {
+  BEGIN(ctx);
+  if (!(dt > 0.0) || !isfinite(dt)) return set_err(DNSBOX_ERR_ARG, "dt must be positive and finite");
+  ctx->hstage[0] = dt;
+  CK(cudaMemcpyAsync(&ctx->st->dt, ctx->hstage, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_get_dt(dnsbox_ctx *ctx, double *dt) {
+  BEGIN(ctx);
+  if (!dt) return set_err(DNSBOX_ERR_ARG, "null output");
+  CK(cudaMemcpyAsync(ctx->hstage, &ctx->st->dt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *dt = ctx->hstage[0];
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_set_time(dnsbox_ctx *ctx, double t) {
+  BEGIN(ctx);
+  ctx->hstage[0] = t;
+  ctx->hstage[1] = t;
+  CK(cudaMemcpyAsync(&ctx->st->t, ctx->hstage, 2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_get_time(dnsbox_ctx *ctx, double *t) {
+  BEGIN(ctx);
+  if (!t) return set_err(DNSBOX_ERR_ARG, "null output");
+  CK(cudaMemcpyAsync(ctx->hstage, &ctx->st->t, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *t = ctx->hstage[0];
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_reset_history(dnsbox_ctx *ctx) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  ctx->ab2_started = 0;
+  ctx->cfl_first = 1;
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_rhs_nonlinear(dnsbox_ctx *ctx, const void *uh, void *out, double *eband) {
+  BEGIN(ctx);
+  if (!uh || !out) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  if (uh == out) return set_err(DNSBOX_ERR_ARG, "input and output may not alias");
+  int rc = ctx->fp64 ? run_rhs<double>(ctx, uh, FIN_RHS, out, nullptr, nullptr, false, 0, nullptr)
+                     : run_rhs<float>(ctx, uh, FIN_RHS, out, nullptr, nullptr, false, 0, nullptr);
+  RET(rc);
+  if (eband) {
+    CK(cudaMemcpyAsync(ctx->hstage, &ctx->st->eband, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *eband = ctx->p.bandlim ? ctx->hstage[0] : 0.0;
+  }
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_step(dnsbox_ctx *ctx, void *uh, int nsteps, dnsbox_diag *diag) {
+  BEGIN(ctx);
+  if (!uh || nsteps < 0) return set_err(DNSBOX_ERR_ARG, "invalid argument");
+  if (nsteps == 0) return DNSBOX_OK;
+  return ctx->fp64 ? step_impl<double>(ctx, uh, nsteps, diag) : step_impl<float>(ctx, uh, nsteps, diag);
+}
+
+extern "C" int dnsbox_project(dnsbox_ctx *ctx, void *uh) {
+  BEGIN(ctx);
+  if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  const int g = grid_for((long long)ctx->nh);
+  if (ctx->fp64)
+    k_project<double2><<<g, 256, 0, ctx->stream>>>((double2 *)uh, (long long)ctx->nh, p.nx, p.ny, p.nz,
+                                                   p.alpha_x, p.alpha_y, p.alpha_z);
+  else
+    k_project<float2><<<g, 256, 0, ctx->stream>>>((float2 *)uh, (long long)ctx->nh, p.nx, p.ny, p.nz,
+                                                  p.alpha_x, p.alpha_y, p.alpha_z);
+  CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_dealias(dnsbox_ctx *ctx, void *uh) {
+  BEGIN(ctx);
+  if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  const int g = grid_for((long long)ctx->nh);
+  const double cx = (p.nx / 2.0) * (2.0 * p.alpha_x / 3.0), cy = (p.ny / 2.0) * (2.0 * p.alpha_y / 3.0),
+               cz = (p.nz / 2.0) * (2.0 * p.alpha_z / 3.0);
+  const double sph2 = pow((p.nx / 2.0) * (2.0 * p.alpha_x / 3.0), 2);   // state.f90:189-190
+  if (ctx->fp64)
+    k_dealias<double2><<<g, 256, 0, ctx->stream>>>((double2 *)uh, (long long)ctx->nh, p.nx, p.ny, p.nz,
+                                                   p.alpha_x, p.alpha_y, p.alpha_z, p.spherical, cx, cy,
+                                                   cz, sph2);
+  else
+    k_dealias<float2><<<g, 256, 0, ctx->stream>>>((float2 *)uh, (long long)ctx->nh, p.nx, p.ny, p.nz,
+                                                  p.alpha_x, p.alpha_y, p.alpha_z, p.spherical, cx, cy, cz,
+                                                  sph2);
+  CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+// shared spectral diagnostics: out[0..nspec) spectrum, then ezero, eone, esqrt2, E-sum, D-sum
+static int specdiag(dnsbox_ctx *ctx, const void *uh, int single, std::vector<double> &out) {
+  const dnsbox_params &p = ctx->p;
+  const int nv = ctx->nspec + 5;
+  const int nblk = 148 * 2;
+  RET(ensure_red(ctx, (size_t)nblk * nv + nv));
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  const size_t smem = (size_t)nv * sizeof(double);
+  if (ctx->fp64)
+    k_specdiag<double2><<<nblk, 256, smem, ctx->stream>>>((const double2 *)uh, (long long)ctx->nh, p.nx, p.ny,
+                                                          p.nz, p.alpha_x, p.alpha_y, p.alpha_z, ctx->nspec,
+                                                          p.Deltak, single, s * s, ctx->red);
+  else
+    k_specdiag<float2><<<nblk, 256, smem, ctx->stream>>>((const float2 *)uh, (long long)ctx->nh, p.nx, p.ny,
+                                                         p.nz, p.alpha_x, p.alpha_y, p.alpha_z, ctx->nspec,
+                                                         p.Deltak, single, s * s, ctx->red);
+  CK(cudaGetLastError());
+  k_sum_partials<<<(nv + 255) / 256, 256, 0, ctx->stream>>>(ctx->red, nblk, nv, ctx->red + (size_t)nblk * nv);
+  CK(cudaGetLastError());
+  out.resize(nv);
+  CK(cudaMemcpyAsync(out.data(), ctx->red + (size_t)nblk * nv, nv * sizeof(double), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_spectrum(dnsbox_ctx *ctx, const void *uh, double *espec, double *ezero, double *eone,
+                               double *esqrt2) {
+  BEGIN(ctx);
+  if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  std::vector<double> v;
+  RET(specdiag(ctx, uh, ctx->p.spectrum_mode == DNSBOX_SPECTRUM_SINGLE, v));
+  const int ns = ctx->nspec;
+  if (espec) memcpy(espec, v.data(), ns * sizeof(double));
+  if (ezero) *ezero = v[ns];
+  if (eone) *eone = v[ns + 1];
+  if (esqrt2) *esqrt2 = v[ns + 2];
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_kinetic(dnsbox_ctx *ctx, const void *uh, double *ekin) {
+  BEGIN(ctx);
+  if (!uh || !ekin) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  std::vector<double> v;
+  RET(specdiag(ctx, uh, 0, v));
+  const dnsbox_params &p = ctx->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  *ekin = v[ctx->nspec + 3] * s * s;
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_dissipation(dnsbox_ctx *ctx, const void *uh, double *disp) {
+  BEGIN(ctx);
+  if (!uh || !disp) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  std::vector<double> v;
+  RET(specdiag(ctx, uh, 0, v));
+  const dnsbox_params &p = ctx->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  *disp = p.nu * v[ctx->nspec + 4] * s * s;
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_eband(dnsbox_ctx *ctx, const void *uh, double *eband) {
+  BEGIN(ctx);
+  if (!uh || !eband) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  if (!ctx->nband) {
+    *eband = 0.0;
+    return DNSBOX_OK;
+  }
+  if (ctx->fp64)
+    k_eband<double2><<<1, 256, 0, ctx->stream>>>((const double2 *)uh, (long long)ctx->nh, ctx->band,
+                                                 ctx->nband, p.nx, ctx->st, s * s, 0);
+  else
+    k_eband<float2><<<1, 256, 0, ctx->stream>>>((const float2 *)uh, (long long)ctx->nh, ctx->band, ctx->nband,
+                                                p.nx, ctx->st, s * s, 0);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->hstage, &ctx->st->eband, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *eband = ctx->hstage[0];
+  return DNSBOX_OK;
+}
+
+// physical fields of the spectral state go to W1 (as 3 real fields after the
+// z/y passes freed it); returns pointers to them.
+template <typename T> static int state_to_phys(dnsbox_ctx *ctx, const void *uh, double scale, void **phys) {
+  const void *in[3];
+  void *out[3];
+  // the c2r passes use W1 slots 0-2 and W2 slots 0-2; the physical output goes
+  // to W1 slots 3-5 (each real field needs half a complex field's bytes)
+  for (int f = 0; f < 3; ++f) {
+    in[f] = cfield(reinterpret_cast<const char *>(uh), ctx, f);
+    out[f] = field(ctx->W1, ctx, 3 + f);
+    phys[f] = out[f];
+  }
+  return c2r_fields<T>(ctx, 3, in, out, scale);
+}
+
+static int reduce_max(dnsbox_ctx *ctx, const void *f, bool fp64, long long n, int absval, double *host) {
+  const int nblk = 148 * 4;
+  RET(ensure_red(ctx, nblk + 1));
+  if (fp64)
+    k_max<double><<<nblk, 256, 0, ctx->stream>>>((const double *)f, n, absval, ctx->red);
+  else
+    k_max<float><<<nblk, 256, 0, ctx->stream>>>((const float *)f, n, absval, ctx->red);
+  CK(cudaGetLastError());
+  k_max_partials<<<1, 1024, 0, ctx->stream>>>(ctx->red, nblk, ctx->red + nblk);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->hstage, ctx->red + nblk, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *host = ctx->hstage[0];
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_courant(dnsbox_ctx *ctx, const void *uh, double dt, double *courant, double *umax3) {
+  BEGIN(ctx);
+  if (!uh || !courant) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  void *phys[3];
+  RET(ctx->fp64 ? state_to_phys<double>(ctx, uh, s, phys) : state_to_phys<float>(ctx, uh, s, phys));
+  double m[3];
+  for (int c = 0; c < 3; ++c) RET(reduce_max(ctx, phys[c], ctx->fp64, (long long)ctx->np, 1, &m[c]));
+  // io.f90:669-671
+  *courant = m[0] * dt / ((2 * M_PI / p.alpha_x) / p.nx) + m[1] * dt / ((2 * M_PI / p.alpha_y) / p.ny) +
+             m[2] * dt / ((2 * M_PI / p.alpha_z) / p.nz);
+  if (umax3)
+    for (int c = 0; c < 3; ++c) umax3[c] = m[c];
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_divergence(dnsbox_ctx *ctx, const void *uh, double *divmax) {
+  BEGIN(ctx);
+  if (!uh || !divmax) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  // (i k . u) s into W2 slot 5, C2R into W1 slot 4
+  void *dh = field(ctx->W2, ctx, 5);
+  const int g = grid_for((long long)ctx->nh);
+  if (ctx->fp64)
+    k_divhat<double2><<<g, 256, 0, ctx->stream>>>((const double2 *)uh, (double2 *)dh, (long long)ctx->nh, p.nx,
+                                                  p.ny, p.nz, p.alpha_x, p.alpha_y, p.alpha_z, s);
+  else
+    k_divhat<float2><<<g, 256, 0, ctx->stream>>>((const float2 *)uh, (float2 *)dh, (long long)ctx->nh, p.nx,
+                                                 p.ny, p.nz, p.alpha_x, p.alpha_y, p.alpha_z, s);
+  CK(cudaGetLastError());
+  const void *in[1] = {dh};
+  void *out[1] = {field(ctx->W1, ctx, 4)};
+  RET(ctx->fp64 ? c2r_fields<double>(ctx, 1, in, out, 1.0) : c2r_fields<float>(ctx, 1, in, out, 1.0));
+  return reduce_max(ctx, out[0], ctx->fp64, (long long)ctx->np, 0, divmax);
+}
+
+extern "C" int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec, void *phys) {
+  BEGIN(ctx);
+  if (!spec || !phys) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const void *in[1] = {spec};
+  void *out[1] = {phys};
+  return ctx->fp64 ? c2r_fields<double>(ctx, 1, in, out, 1.0) : c2r_fields<float>(ctx, 1, in, out, 1.0);
+}
+
+extern "C" int dnsbox_r2c(dnsbox_ctx *ctx, const void *phys, void *spec) {
+  BEGIN(ctx);
+  if (!spec || !phys) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const void *in[1] = {phys};
+  void *out[1] = {spec};
+  return ctx->fp64 ? r2c_fields<double>(ctx, 1, in, out) : r2c_fields<float>(ctx, 1, in, out);
+}
+
+extern "C" int dnsbox_upload_state(dnsbox_ctx *ctx, const double *host, void *uh) {
+  BEGIN(ctx);
+  if (!host || !uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  // 3 complex-double fields fit in W1 (6 fields of the context precision >= 3 x 16 B)
+  const size_t bytes = 3 * ctx->nh * 16;
+  CK(cudaMemcpyAsync(ctx->W1, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  dim3 grid((p.nz + 31) / 32, (ctx->nxh + 31) / 32, 3 * p.ny), blk(32, 8);
+  if (ctx->fp64)
+    k_from_p3dfft<double2><<<grid, blk, 0, ctx->stream>>>((const double2 *)ctx->W1, (double2 *)uh, ctx->nxh,
+                                                          p.ny, p.nz);
+  else
+    k_from_p3dfft<float2><<<grid, blk, 0, ctx->stream>>>((const double2 *)ctx->W1, (float2 *)uh, ctx->nxh, p.ny,
+                                                         p.nz);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_download_state(dnsbox_ctx *ctx, const void *uh, double *host) {
+  BEGIN(ctx);
+  if (!host || !uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  dim3 grid((p.nz + 31) / 32, (ctx->nxh + 31) / 32, 3 * p.ny), blk(32, 8);
+  if (ctx->fp64)
+    k_to_p3dfft<double2><<<grid, blk, 0, ctx->stream>>>((const double2 *)uh, (double2 *)ctx->W1, ctx->nxh, p.ny,
+                                                        p.nz);
+  else
+    k_to_p3dfft<float2><<<grid, blk, 0, ctx->stream>>>((const float2 *)uh, (double2 *)ctx->W1, ctx->nxh, p.ny,
+                                                       p.nz);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, ctx->W1, 3 * ctx->nh * 16, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_upload_physical(dnsbox_ctx *ctx, const double *host, void *uh) {
+  BEGIN(ctx);
+  if (!host || !uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  // host doubles -> W2 (3 physical double fields fit: 6 nh cbytes >= 3 np 8 for both precisions)
+  const size_t pbytes = ctx->np * sizeof(double);
+  CK(cudaMemcpyAsync(ctx->W2, host, 3 * pbytes, cudaMemcpyHostToDevice, ctx->stream));
+  const void *in[3];
+  void *out[3];
+  char *src = ctx->W2;
+  if (!ctx->fp64) {
+    // convert to float into W1 slots 3-5 (each holds nh*8 B >= np*4 B)
+    for (int c = 0; c < 3; ++c) {
+      float *dst = reinterpret_cast<float *>(field(ctx->W1, ctx, 3 + c));
+      k_convert<double, float><<<grid_for((long long)ctx->np), 256, 0, ctx->stream>>>(
+          reinterpret_cast<const double *>(src + c * pbytes), dst, (long long)ctx->np);
+      in[c] = dst;
+    }
+    CK(cudaGetLastError());
+  } else {
+    for (int c = 0; c < 3; ++c) in[c] = src + c * pbytes;
+  }
+  for (int c = 0; c < 3; ++c) out[c] = field(reinterpret_cast<char *>(uh), ctx, c);
+  RET(ctx->fp64 ? r2c_fields<double>(ctx, 3, in, out) : r2c_fields<float>(ctx, 3, in, out));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_download_physical(dnsbox_ctx *ctx, const void *uh, double *host) {
+  BEGIN(ctx);
+  if (!host || !uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  void *phys[3];
+  RET(ctx->fp64 ? state_to_phys<double>(ctx, uh, s, phys) : state_to_phys<float>(ctx, uh, s, phys));
+  const size_t pbytes = ctx->np * sizeof(double);
+  for (int c = 0; c < 3; ++c) {
+    if (ctx->fp64) {
+      CK(cudaMemcpyAsync(reinterpret_cast<char *>(host) + c * pbytes, phys[c], pbytes, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    } else {
+      double *stage = reinterpret_cast<double *>(ctx->W2);   // free after the c2r passes
+      k_convert<float, double><<<grid_for((long long)ctx->np), 256, 0, ctx->stream>>>(
+          reinterpret_cast<const float *>(phys[c]), stage, (long long)ctx->np);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(reinterpret_cast<char *>(host) + c * pbytes, stage, pbytes, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_rhs_adj(dnsbox_ctx *ctx, const void *, void *, void *) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  return set_err(DNSBOX_ERR_UNSUPPORTED, "rhs_adj not built yet");
+}
+
+extern "C" int dnsbox_rhs_nonlinear_vjp(dnsbox_ctx *ctx, const void *, const void *, void *) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  return set_err(DNSBOX_ERR_UNSUPPORTED, "rhs_nonlinear_vjp not built yet");
+}
+
+extern "C" int dnsbox_profile_enable(dnsbox_ctx *ctx, int on) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  ctx->prof_on = on ? 1 : 0;
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_profile_read(dnsbox_ctx *ctx, dnsbox_profile *out, int reset) {
+  BEGIN(ctx);
+  if (!out) return set_err(DNSBOX_ERR_ARG, "null output");
+  CK(cudaStreamSynchronize(ctx->stream));
+  memset(out, 0, sizeof(*out));
+  for (size_t i = 0; i < ctx->ev_used; ++i) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev_pool[2 * i], ctx->ev_pool[2 * i + 1]));
+    out->ms[ctx->ev_kind[i]] += ms;
+  }
+  for (int k = 0; k < DNSBOX_NPASS; ++k) out->launches[k] = ctx->launches[k];
+  out->total_launches = ctx->total_launches;
+  if (reset) {
+    ctx->ev_used = 0;
+    for (int k = 0; k < DNSBOX_NPASS; ++k) ctx->launches[k] = 0;
+    ctx->total_launches = 0;
+  }
+  return DNSBOX_OK;
+}

@@ -1,0 +1,106 @@
+// Launchers of the size-templated pass kernels.  Each (precision, N) pair is
+// explicitly instantiated in its own translation unit (inst.cu built once per
+// pair), so the library compiles in parallel; api.cu sees declarations only.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace dnsbox {
+
+template <typename T, int N> struct Launcher {
+  static cudaError_t strided(const StridedArgs<T> &a, bool inv, int ntiles, cudaStream_t st);
+  static cudaError_t xline_nl(const XlineNLArgs<T> &a, cudaStream_t st);
+  static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);
+  static cudaError_t xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_t st);
+  static cudaError_t zfinish(const FinishArgs<T> &a, int nblocks, cudaStream_t st);
+  static int strided_threads();
+  static int zfinish_threads();
+};
+
+#define DNSBOX_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512) X(1024)
+
+#ifdef DNSBOX_LAUNCH_IMPL
+template <typename K>
+static cudaError_t set_smem(K kernel, size_t bytes) {
+  if (bytes > 227 * 1024) return cudaErrorInvalidConfiguration;   // over the per-CTA limit
+  if (bytes > 48 * 1024)
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return cudaSuccess;
+}
+
+template <typename T, int N> int Launcher<T, N>::strided_threads() {
+  return round32(TileCols<T>::v * (N / FftPlan<N>::E));
+}
+template <typename T, int N> int Launcher<T, N>::zfinish_threads() {
+  return round32(TileCols<T>::v * (N / FftPlan<N>::E));
+}
+
+template <typename T, int N>
+cudaError_t Launcher<T, N>::strided(const StridedArgs<T> &a, bool inv, int ntiles, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  const size_t smem = (size_t)N * TileCols<T>::v * sizeof(C);
+  const int nt = strided_threads();
+  const unsigned nb = (unsigned)ntiles * a.njobs;
+  cudaError_t e;
+  if (inv) {
+    if ((e = set_smem(k_strided<T, N, true>, smem)) != cudaSuccess) return e;
+    k_strided<T, N, true><<<nb, nt, smem, st>>>(a);
+  } else {
+    if ((e = set_smem(k_strided<T, N, false>, smem)) != cudaSuccess) return e;
+    k_strided<T, N, false><<<nb, nt, smem, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T, int N>
+cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  constexpr int B = XlineB<T, N>::v;
+  const size_t smem = (size_t)N * 3 * B * sizeof(C);
+  const int nt = round32(3 * B * (N / FftPlan<N>::E));
+  cudaError_t e;
+  if ((e = set_smem(k_xline_nl<T, N>, smem)) != cudaSuccess) return e;
+  const unsigned nb = (unsigned)((a.nlines + B - 1) / B);
+  k_xline_nl<T, N><<<nb, nt, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int N>
+cudaError_t Launcher<T, N>::xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  constexpr int B = XlinePlainB<T, N>::v;
+  const size_t smem = (size_t)N * (B / 2) * sizeof(C);
+  const int nt = round32((B / 2) * (N / FftPlan<N>::E));
+  cudaError_t e;
+  if ((e = set_smem(k_xline_c2r<T, N>, smem)) != cudaSuccess) return e;
+  dim3 grid((unsigned)((a.nlines + B - 1) / B), (unsigned)nf);
+  k_xline_c2r<T, N><<<grid, nt, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int N>
+cudaError_t Launcher<T, N>::xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  constexpr int B = XlinePlainB<T, N>::v;
+  const size_t smem = (size_t)N * (B / 2) * sizeof(C);
+  const int nt = round32((B / 2) * (N / FftPlan<N>::E));
+  cudaError_t e;
+  if ((e = set_smem(k_xline_r2c<T, N>, smem)) != cudaSuccess) return e;
+  dim3 grid((unsigned)((a.nlines + B - 1) / B), (unsigned)nf);
+  k_xline_r2c<T, N><<<grid, nt, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int N>
+cudaError_t Launcher<T, N>::zfinish(const FinishArgs<T> &a, int nblocks, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  const size_t smem = (size_t)3 * N * TileCols<T>::v * sizeof(C);
+  const int nt = zfinish_threads();
+  cudaError_t e;
+  if ((e = set_smem(k_zfinish<T, N>, smem)) != cudaSuccess) return e;
+  k_zfinish<T, N><<<(unsigned)nblocks, nt, smem, st>>>(a);
+  return cudaGetLastError();
+}
+#endif
+
+}  // namespace dnsbox

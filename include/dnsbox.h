@@ -1,0 +1,204 @@
+/* dnsbox.h -- C ABI of libdnsbox_gpu.so, the B200 (sm_100a) pseudospectral
+ * Navier-Stokes time step of dnsbox.
+ *
+ * The reference (DavetheSlayer/dnsbox) exposes its hot path as Fortran module
+ * subroutines without arguments acting on module globals.  Each entry point
+ * below replaces one of them; the reference routine is cited beside it
+ * (file:line in the reference tree).  All pointers named ``*_dev`` are device
+ * pointers; ``*_host`` are host pointers.  Every call returns an int status
+ * (DNSBOX_OK = 0, negative = DNSBOX_ERR_*); nothing throws across the ABI.
+ *
+ * Layouts in device memory (the library's own):
+ *   spectral field : [nz][ny][nx/2+1] complex, kx fastest; complex double for
+ *                    DNSBOX_FP64, complex float for DNSBOX_FP32.
+ *   vector field   : three spectral fields back to back (u, v, w).
+ *   physical field : [nz][ny][nx] real, x fastest (the reference's (x, y, z)).
+ * Transforms are unnormalised both ways, as p3dfft's ftran_r2c / btran_c2r.
+ * Host layouts of the upload/download calls are the reference's: complex(8)
+ * (kz, ky, kx) with kz fastest (p3dfft STRIDE1) and real(8) (x, y, z).
+ *
+ * Threading: one context per host thread; calls are asynchronous on the
+ * context's stream unless they return host values.
+ */
+#ifndef DNSBOX_H
+#define DNSBOX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DNSBOX_ABI_VERSION 1
+
+enum {
+  DNSBOX_OK = 0,
+  DNSBOX_ERR_ARG = -1,          /* null pointer or invalid parameter        */
+  DNSBOX_ERR_SIZE = -2,         /* grid size not supported                  */
+  DNSBOX_ERR_CUDA = -3,         /* CUDA runtime error (see dnsbox_last_error) */
+  DNSBOX_ERR_OOM = -4,          /* device allocation failed                 */
+  DNSBOX_ERR_NONFINITE = -5,    /* NaN/Inf found by a fused reduction       */
+  DNSBOX_ERR_TIMEOUT = -6,      /* a bounded device wait gave up            */
+  DNSBOX_ERR_STATE = -7,        /* call order (e.g. no time step set)       */
+  DNSBOX_ERR_UNSUPPORTED = -8   /* option not available in this build       */
+};
+
+enum dnsbox_precision { DNSBOX_FP64 = 0, DNSBOX_FP32 = 1, DNSBOX_TC_SPLIT = 2 };
+enum dnsbox_stepper { DNSBOX_HEUN = 0, DNSBOX_AB2 = 1 };
+/* dnsbox.f90:150-161 literal coefficients (quirk Q2) or standard IF-AB2 */
+enum dnsbox_ab2_mode { DNSBOX_AB2_REFERENCE = 0, DNSBOX_AB2_STANDARD = 1 };
+/* state.f90:350-411 (MPI build) or single/state.f90:191-230 (quirk Q4) */
+enum dnsbox_spectrum_mode { DNSBOX_SPECTRUM_MPI = 0, DNSBOX_SPECTRUM_SINGLE = 1 };
+/* rhsAdj.f90:343-348: phatadj := phat (intent) or 0 (literal, quirk Q6) */
+enum dnsbox_adj_phat { DNSBOX_ADJ_PHAT_INTENT = 0, DNSBOX_ADJ_PHAT_LITERAL = 1 };
+
+/* Runtime form of the compile-time parameters of parameters.f90:11-50. */
+typedef struct dnsbox_params {
+  int32_t nx, ny, nz;            /* parameters.f90:12-14                     */
+  int32_t precision;             /* enum dnsbox_precision                    */
+  int32_t stepper;               /* enum dnsbox_stepper (parameters.f90:44)  */
+  int32_t ab2_mode;              /* enum dnsbox_ab2_mode                     */
+  int32_t bandlim;               /* parameters.f90:50                        */
+  int32_t spherical;             /* parameters.f90:48                        */
+  int32_t tstep_fix;             /* parameters.f90:38                        */
+  int32_t hminone;               /* parameters.f90:43                        */
+  int32_t spectrum_mode;         /* enum dnsbox_spectrum_mode                */
+  int32_t adj_phat;              /* enum dnsbox_adj_phat                     */
+  int32_t device;                /* CUDA device ordinal                      */
+  int32_t reserved_i[3];
+  double alpha_x, alpha_y, alpha_z; /* parameters.f90:18-20                  */
+  double nu;                     /* parameters.f90:21                        */
+  double Q;                      /* parameters.f90:22                        */
+  double kCutOff;                /* parameters.f90:23                        */
+  double Pin;                    /* parameters.f90:24                        */
+  double Deltak;                 /* parameters.f90:27                        */
+  double courant_min, courant_max; /* parameters.f90:33-34                   */
+  double dt_max;                 /* parameters.f90:35 (tStepMax)             */
+  double dt;                     /* initial time step (variables.f90:9)      */
+  double reserved_d[4];
+} dnsbox_params;
+
+/* Per-step diagnostics (the quantities io_save_stats writes to Ekin.dat,
+ * io.f90:628-661, computed on the device every step). */
+typedef struct dnsbox_diag {
+  double t;                      /* time after the step                      */
+  double dt;                     /* step size used                           */
+  double ekin;                   /* state_kinetic of the new state           */
+  double dissipation;            /* nu <|grad u|^2> of the new state (Parseval) */
+  double production_literal;     /* 2 Q Ekin, as io.f90:644                  */
+  double injected_power;         /* Pin (band forcing) + 2 Q Ekin            */
+  double courant;                /* io_Courant of the step's initial state   */
+  double umax[3];                /* max |u_i| of the step's initial state    */
+  double eband;                  /* rhs_Eband of the step's initial state    */
+  int32_t nonfinite;             /* 1 if a NaN/Inf was seen                  */
+  int32_t step;                  /* step counter after the step              */
+} dnsbox_diag;
+
+typedef struct dnsbox_ctx dnsbox_ctx;
+
+/* ---- context (replaces var_init, variables.f90:99-280) ------------------ */
+void dnsbox_default_params(dnsbox_params *p);
+int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out);
+int dnsbox_destroy(dnsbox_ctx *ctx);
+int dnsbox_set_stream(dnsbox_ctx *ctx, void *cuda_stream);
+const char *dnsbox_last_error(void);
+int dnsbox_supported_size(int n);
+int dnsbox_abi_version(void);
+int dnsbox_field_bytes(const dnsbox_ctx *ctx, size_t *spectral_bytes, size_t *physical_bytes);
+int dnsbox_nspec(const dnsbox_ctx *ctx);
+
+/* ---- time step (rhs_int_fact, rhs.f90:8-16; set_time_step,
+ *      dnsboxheun.f90:227-246).  The integrating factor is evaluated on the
+ *      fly, so setting dt stores it only. -------------------------------- */
+int dnsbox_set_dt(dnsbox_ctx *ctx, double dt);
+int dnsbox_get_dt(dnsbox_ctx *ctx, double *dt);
+int dnsbox_set_time(dnsbox_ctx *ctx, double t);
+int dnsbox_get_time(dnsbox_ctx *ctx, double *t);
+/* AB2: the next dnsbox_step starts with a predictor-corrector step
+ * (dnsbox.f90:87-141). */
+int dnsbox_reset_history(dnsbox_ctx *ctx);
+
+/* ---- operators ----------------------------------------------------------- */
+/* rhs_nonlinear, rhs.f90:18-135 (+ rhs_Eband, rhs.f90:137-168).
+ * uhat3_dev -> nonlin3_dev (may not alias); eband_host may be NULL. */
+int dnsbox_rhs_nonlinear(dnsbox_ctx *ctx, const void *uhat3_dev, void *nonlin3_dev,
+                         double *eband_host);
+/* Integrating-factor Heun (dnsboxheun.f90:85-126) or IF-AB2 with a
+ * predictor-corrector first step (dnsbox.f90:87-218), nsteps in place, with
+ * CFL control (dnsboxheun.f90:153-157 + io_Courant, io.f90:664-676) unless
+ * tstep_fix.  diag_host (nsteps records) may be NULL; when given, the call
+ * synchronises the stream before returning. */
+int dnsbox_step(dnsbox_ctx *ctx, void *uhat3_dev, int nsteps, dnsbox_diag *diag_host);
+/* state_project, state.f90:120-179 (in place) */
+int dnsbox_project(dnsbox_ctx *ctx, void *uhat3_dev);
+/* state_dealias, state.f90:181-209 (in place) */
+int dnsbox_dealias(dnsbox_ctx *ctx, void *uhat3_dev);
+/* state_spectrum, state.f90:350-411: espec_host has dnsbox_nspec() entries */
+int dnsbox_spectrum(dnsbox_ctx *ctx, const void *uhat3_dev, double *espec_host,
+                    double *ezero, double *eone, double *esqrt2);
+/* state_kinetic, state.f90:429-454 */
+int dnsbox_kinetic(dnsbox_ctx *ctx, const void *uhat3_dev, double *ekin);
+/* state_dissipation, state.f90:517-544, in its Parseval form */
+int dnsbox_dissipation(dnsbox_ctx *ctx, const void *uhat3_dev, double *disp);
+/* io_Courant, io.f90:664-676, from the current velocity; umax3 may be NULL */
+int dnsbox_courant(dnsbox_ctx *ctx, const void *uhat3_dev, double dt, double *courant,
+                   double *umax3);
+/* state_divergence, state.f90:413-427 (signed maximum on the grid) */
+int dnsbox_divergence(dnsbox_ctx *ctx, const void *uhat3_dev, double *divmax);
+/* rhs_Eband, rhs.f90:137-168 */
+int dnsbox_eband(dnsbox_ctx *ctx, const void *uhat3_dev, double *eband);
+
+/* ---- transforms: p3dfft_ftran_r2c / p3dfft_btran_c2r (state.f90:58-72),
+ *      unnormalised, input not destroyed ------------------------------------ */
+int dnsbox_r2c(dnsbox_ctx *ctx, const void *phys_dev, void *spec_dev);
+int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec_dev, void *phys_dev);
+
+/* ---- host <-> device state (replaces the module arrays uhat/vhat/what and
+ *      u/v/w; io.f90:100-278 / 455-626 read and write the physical form) --- */
+/* complex(8) (kz, ky, kx), kz fastest, 3 components -> device state */
+int dnsbox_upload_state(dnsbox_ctx *ctx, const double *uhat3_host, void *uhat3_dev);
+int dnsbox_download_state(dnsbox_ctx *ctx, const void *uhat3_dev, double *uhat3_host);
+/* real(8) (x, y, z), 3 components: R2C on upload (state_u2uhat,
+ * state.f90:74-80), C2R * scalemodes on download (state_uhat2u, state.f90:82-96) */
+int dnsbox_upload_physical(dnsbox_ctx *ctx, const double *u3_host, void *uhat3_dev);
+int dnsbox_download_physical(dnsbox_ctx *ctx, const void *uhat3_dev, double *u3_host);
+
+/* ---- adjoint (rhsAdj.f90) --------------------------------------------------- */
+/* rhsAdj, rhsAdj.f90:356-381: r~ (rhsupptilde, :177-213) and rhsadj. */
+int dnsbox_rhs_adj(dnsbox_ctx *ctx, const void *uhat3_dev, void *rtilde3_dev,
+                   void *rhsadj3_dev);
+/* Exact transpose of the linearised rhs_nonlinear at uhat, applied to g
+ * (Euclidean inner product on the Re/Im parts of the half spectrum).  No
+ * reference counterpart: the reference's rhsNonlinearAdj (rhsAdj.f90:261-354)
+ * is its continuous-adjoint analogue. */
+int dnsbox_rhs_nonlinear_vjp(dnsbox_ctx *ctx, const void *uhat3_dev, const void *g3_dev,
+                             void *out3_dev);
+
+/* ---- measurement ------------------------------------------------------------
+ * No reference counterpart (the reference times nothing; Makefile:3 passes
+ * -DMEASURE to p3dfft only).  When enabled, CUDA events are recorded on the
+ * context's stream around every kernel launch of the library and summed per
+ * pass; the launch counter always runs. */
+enum dnsbox_pass {
+  DNSBOX_PASS_Z_INV = 0,     /* pass A: inverse z FFT + curl terms           */
+  DNSBOX_PASS_Y_INV = 1,     /* pass B: inverse y FFT, vorticity assembly    */
+  DNSBOX_PASS_X_NL = 2,      /* pass C: C2R x, u x omega, CFL max, R2C x     */
+  DNSBOX_PASS_Y_FWD = 3,     /* pass D: forward y FFT                        */
+  DNSBOX_PASS_Z_FIN = 4,     /* pass E: forward z FFT + projection + stepper */
+  DNSBOX_PASS_SMALL = 5,     /* band energy, CFL, step bookkeeping           */
+  DNSBOX_PASS_OTHER = 6,     /* standalone transforms and diagnostics        */
+  DNSBOX_NPASS = 8
+};
+typedef struct dnsbox_profile {
+  double ms[DNSBOX_NPASS];          /* summed event time per pass (ms)       */
+  int64_t launches[DNSBOX_NPASS];   /* kernel launches per pass              */
+  int64_t total_launches;           /* all kernel launches since reset       */
+} dnsbox_profile;
+int dnsbox_profile_enable(dnsbox_ctx *ctx, int on);
+int dnsbox_profile_read(dnsbox_ctx *ctx, dnsbox_profile *out, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DNSBOX_H */

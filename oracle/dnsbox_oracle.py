@@ -508,3 +508,26 @@ def rhs_nonlinear_vjp(g: Grid, uh, gout):
     curl_t = np.stack([k[1] * psi[2] - k[2] * psi[1], k[2] * psi[0] - k[0] * psi[2],
                        k[0] * psi[1] - k[1] * psi[0]])
     return curl_t + grad_u
+
+
+# ================================================================ drivers
+def drive(g: Grid, uh, nsteps, dt, stepper="heun", cfl=False):
+    """Time loop of dnsboxheun.f90:81-191 / dnsbox.f90:81-218 without I/O.
+
+    With ``cfl`` the Courant number is taken from the current velocity every
+    step (quirk Q5: the reference uses a copy refreshed every iSaveRate1
+    steps) and set_time_step is applied before the first step (as
+    dnsboxheun.f90:69-73) and whenever it leaves [Cmin, Cmax]."""
+    recs = []
+    ab2 = AB2Stepper(g) if stepper == "ab2" else None
+    first = True
+    for _ in range(nsteps):
+        umax = np.abs(state_uhat2u(g, uh)).reshape(3, -1).max(axis=1)
+        C = io_courant(g, state_uhat2u(g, uh), dt)
+        if cfl and (first or needs_time_step(g, dt, C)):
+            dt, C = set_time_step(g, dt, C)
+        first = False
+        uh = heun_step(g, uh, dt) if ab2 is None else ab2.step(uh, dt)
+        recs.append(dict(dt=dt, courant=C, umax=umax, ekin=state_kinetic(g, uh),
+                         dissipation=dissipation_spectral(g, uh)))
+    return uh, recs
