@@ -148,28 +148,55 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
   __shared__ double red[3 * 32];
   const int line0 = blockIdx.x * B;
   const T sc = T(a.s);
-  // build Z = X1 + i X2 for the pairs (u,v), (w,ox), (oy,oz) of every line
-  for (int it = threadIdx.x; it < B * 3 * H; it += NT) {
+  // Build Z = X1 + i X2.  Each pair holds two quantities of the same kind and
+  // scale (velocity is unscaled, vorticity carries the 1/N^3 of the
+  // reference's derivative transforms), so neither loses bits to the other.
+  // Per line pair (a = 2j, b = 2j+1) the six columns are
+  //   (u_a, v_a) (u_b, v_b) (w_a, w_b) (ox_a, oy_a) (ox_b, oy_b) (oz_a, oz_b).
+  for (int it = threadIdx.x; it < (B / 2) * 6 * H; it += NT) {
     const int k = it % H;
-    const int q = (it / H) % 3;
-    const int l = it / (3 * H);
-    const int line = line0 + l;
-    const int col = 3 * l + q;
+    const int q = (it / H) % 6;
+    const int j = it / (6 * H);
+    const int la = line0 + 2 * j, lb = la + 1;
+    const int col = 6 * j + q;
+    const T kx = T(k_half(k, N, a.alpha_x)) * sc;
+    const long long oa = (long long)la * a.nxh + k, ob = (long long)lb * a.nxh + k;
+    const bool va = la < a.nlines, vb = lb < a.nlines;
     C X1 = mkc<C>(0, 0), X2 = mkc<C>(0, 0);
-    if (line < a.nlines) {
-      const long long off = (long long)line * a.nxh + k;
-      if (q == 0) {
-        X1 = a.U[off];
-        X2 = a.V[off];
-      } else if (q == 1) {
-        X1 = a.W[off];
-        X2 = a.OX[off];
-      } else {
-        // omega_y = dz u - dx w ; omega_z = dx v - dy u (kx still spectral here)
-        const T kx = T(k_half(k, N, a.alpha_x)) * sc;
-        const C w = a.W[off], v = a.V[off], b1 = a.B1[off], c1 = a.C1[off];
-        X1 = mkc<C>(b1.x + kx * w.y, b1.y - kx * w.x);   // b1 - i kx s w
-        X2 = mkc<C>(c1.x - kx * v.y, c1.y + kx * v.x);   // c1 + i kx s v
+    switch (q) {
+      case 0:
+        if (va) { X1 = a.U[oa]; X2 = a.V[oa]; }
+        break;
+      case 1:
+        if (vb) { X1 = a.U[ob]; X2 = a.V[ob]; }
+        break;
+      case 2:
+        if (va) X1 = a.W[oa];
+        if (vb) X2 = a.W[ob];
+        break;
+      case 3:
+      case 4: {
+        // omega_x, and omega_y = dz u - dx w (kx still spectral here)
+        const bool v = q == 3 ? va : vb;
+        const long long o = q == 3 ? oa : ob;
+        if (v) {
+          const C w = a.W[o], b1 = a.B1[o];
+          X1 = a.OX[o];
+          X2 = mkc<C>(b1.x + kx * w.y, b1.y - kx * w.x);   // b1 - i kx s w
+        }
+        break;
+      }
+      default: {
+        // omega_z = dx v - dy u for both lines
+        if (va) {
+          const C v = a.V[oa], c1 = a.C1[oa];
+          X1 = mkc<C>(c1.x - kx * v.y, c1.y + kx * v.x);   // c1 + i kx s v
+        }
+        if (vb) {
+          const C v = a.V[ob], c1 = a.C1[ob];
+          X2 = mkc<C>(c1.x - kx * v.y, c1.y + kx * v.x);
+        }
+        break;
       }
     }
     if (k == 0 || k == N / 2) {
@@ -191,13 +218,15 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
     const int j = it % (B / 2), n = it / (B / 2);
     C *r = s + n * LD + 6 * j;
     T px[2], py[2], pz[2];
+    const C c0 = r[0], c1 = r[1], c2 = r[2], c3 = r[3], c4 = r[4], c5 = r[5];
+    const T uu[2] = {c0.x, c1.x}, vv[2] = {c0.y, c1.y}, ww[2] = {c2.x, c2.y};
+    const T ox[2] = {c3.x, c4.x}, oy[2] = {c3.y, c4.y}, oz[2] = {c5.x, c5.y};
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const C z0 = r[3 * h], z1 = r[3 * h + 1], z2 = r[3 * h + 2];
-      const T u = z0.x, v = z0.y, w = z1.x, ox = z1.y, oy = z2.x, oz = z2.y;
-      px[h] = (oy * w - oz * v) * sc;
-      py[h] = (oz * u - ox * w) * sc;
-      pz[h] = (ox * v - oy * u) * sc;
+      const T u = uu[h], v = vv[h], w = ww[h];
+      px[h] = (oy[h] * w - oz[h] * v) * sc;
+      py[h] = (oz[h] * u - ox[h] * w) * sc;
+      pz[h] = (ox[h] * v - oy[h] * u) * sc;
       m0 = fmax(m0, fabs((double)u));
       m1 = fmax(m1, fabs((double)v));
       m2 = fmax(m2, fabs((double)w));

@@ -20,12 +20,13 @@ template <typename T, int N> struct Launcher {
 #define DNSBOX_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512) X(1024)
 
 #ifdef DNSBOX_LAUNCH_IMPL
+// Opts the kernel in to `bytes` of dynamic shared memory (the 48 KB default
+// covers static + dynamic, so it is set for every size); refuses sizes over
+// the 227 KB per-CTA limit.
 template <typename K>
 static cudaError_t set_smem(K kernel, size_t bytes) {
-  if (bytes > 227 * 1024) return cudaErrorInvalidConfiguration;   // over the per-CTA limit
-  if (bytes > 48 * 1024)
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  return cudaSuccess;
+  if (bytes > 227 * 1024) return cudaErrorInvalidConfiguration;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 template <typename T, int N> int Launcher<T, N>::strided_threads() {
