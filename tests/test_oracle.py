@@ -217,3 +217,39 @@ def test_vjp_oracle_finite_difference():
     lhs = np.sum(gout.real * jp.real + gout.imag * jp.imag)
     rhs = np.sum(vjp.real * d.real + vjp.imag * d.imag)
     assert abs(lhs - rhs) < 1e-6 * abs(lhs)
+
+
+def _nyquist_planes(n):
+    m = np.zeros((n, n, n // 2 + 1), bool)
+    m[:, :, n // 2] = True
+    m[:, n // 2, :] = True
+    m[n // 2] = True
+    return m
+
+
+def test_exact_adjoint_matches_reference_rhsadj():
+    """rhsAdj.f90:261-354 computes -P_d[(grad r)^T u + (u.grad) r], the
+    continuous adjoint of the linearised nonlinear term.  The exact discrete
+    transpose (Euclidean on the half spectrum) relates to it through the
+    half-spectrum weight W: P W^-1 vjp(W r) = -rhsNonlinearAdj(r) on the
+    retained modes off the Nyquist planes (where quirk Q1 breaks the identity)."""
+    n = 16
+    p = O.Params(nx=n, ny=n, nz=n, nu=0.01, bandlim=False)
+    g = O.Grid(p)
+    uh = ic.random_field(n, seed=1, k0=3.0)
+    rt = ic.random_field(n, seed=2, k0=3.0)
+    keep = ~g.dealias_mask(0.5) & ~_nyquist_planes(n)
+    W = O.half_weight(g)
+    pv = O.state_project(g, O.rhs_nonlinear_vjp(g, uh, W * rt) / W)
+    ref = O.adj_nonlinear_part(g, uh, rt)
+    assert rel(pv[:, keep], -ref[:, keep]) < 1e-13
+
+
+def test_convective_equals_rotational_off_nyquist():
+    """rhsAdj.f90's convective N equals rhs.f90's rotational N on dealiased
+    solenoidal fields, except on the Nyquist planes (quirk Q1)."""
+    n = 16
+    g = O.Grid(O.Params(nx=n, ny=n, nz=n, nu=0.01, bandlim=False))
+    uh = ic.random_field(n, seed=1, k0=3.0)
+    keep = ~g.dealias_mask(0.5) & ~_nyquist_planes(n)
+    assert rel(O.adj_rhs_nonlinear(g, uh)[:, keep], O.rhs_nonlinear(g, uh)[:, keep]) < 1e-13
