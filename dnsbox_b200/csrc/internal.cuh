@@ -136,12 +136,12 @@ static inline int grid_for(long long n, int threads = 256, int cap = 148 * 16) {
   return (int)b;
 }
 
-static char *field(char *base, const dnsbox_ctx *c, int slot) { return base + (size_t)slot * c->nh * c->cbytes; }
-static const char *cfield(const char *base, const dnsbox_ctx *c, int slot) {
+static inline char *field(char *base, const dnsbox_ctx *c, int slot) { return base + (size_t)slot * c->nh * c->cbytes; }
+static inline const char *cfield(const char *base, const dnsbox_ctx *c, int slot) {
   return base + (size_t)slot * c->nh * c->cbytes;
 }
 
-static int ensure_red(dnsbox_ctx *c, size_t ndoubles) {
+static inline int ensure_red(dnsbox_ctx *c, size_t ndoubles) {
   if (ndoubles <= c->red_cap) return DNSBOX_OK;
   if (c->red) cudaFree(c->red);
   c->red = nullptr;
@@ -150,7 +150,7 @@ static int ensure_red(dnsbox_ctx *c, size_t ndoubles) {
   return DNSBOX_OK;
 }
 
-static int ensure_diag(dnsbox_ctx *c, int n) {
+static inline int ensure_diag(dnsbox_ctx *c, int n) {
   if (n <= c->ddiag_cap) return DNSBOX_OK;
   if (c->ddiag) cudaFree(c->ddiag);
   c->ddiag = nullptr;

@@ -153,6 +153,18 @@ int dnsbox_eband(dnsbox_ctx *ctx, const void *uhat3_dev, double *eband);
  *      unnormalised, input not destroyed ------------------------------------ */
 int dnsbox_r2c(dnsbox_ctx *ctx, const void *phys_dev, void *spec_dev);
 int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec_dev, void *phys_dev);
+/* No counterpart in the reference.  dnsbox_c2r for callers that cannot
+ * allocate device memory (their memory belongs to a pool they must not bypass,
+ * or they run where allocating is not allowed) and so cannot create a context.
+ * No context; allocates nothing: the two intermediate fields live in a static
+ * 8 MiB device array, so 2 * nz*ny*(nx/2+1) * (16 for DNSBOX_FP64, 8 for
+ * DNSBOX_FP32) bytes must fit in 8 MiB (64^3 FP64, 96^3 FP32), else
+ * DNSBOX_ERR_SIZE.  Runs on the current device and the given stream.  The first
+ * call on a device sets that device up (resolves the arrays' addresses, fills
+ * the twiddle tables): make it before any stream capture.  All calls share the
+ * scratch array, so calls that overlap on the GPU race. */
+int dnsbox_c2r_noalloc(int nx, int ny, int nz, int precision, const void *spec_dev, void *phys_dev,
+                       void *cuda_stream);
 
 /* ---- host <-> device state (replaces the module arrays uhat/vhat/what and
  *      u/v/w; io.f90:100-278 / 455-626 read and write the physical form) --- */
