@@ -407,9 +407,10 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   set_job<T>(b, 0, field(c->W1, c, 0), field(c->W2, c, 0));
   set_job<T>(b, 1, field(c->W1, c, 1), field(c->W2, c, 1));
   set_job<T>(b, 2, field(c->W1, c, 2), field(c->W2, c, 2));
-  set_job<T>(b, 3, field(c->W1, c, 2), field(c->W2, c, 3), 0.0, s, 1, field(c->W1, c, 3));  // omega_x
-  set_job<T>(b, 4, field(c->W1, c, 4), field(c->W2, c, 4));
-  set_job<T>(b, 5, field(c->W1, c, 0), field(c->W2, c, 5), 0.0, -s, 1);                     // -dy u
+  // omega_x = dy w - dz v ; omega_y = dz u - dx w ; omega_z = dx v - dy u (ks: 0 kx, 1 ky here)
+  set_job<T>(b, 3, field(c->W1, c, 2), field(c->W2, c, 3), 0.0, s, 1, field(c->W1, c, 3));
+  set_job<T>(b, 4, field(c->W1, c, 4), field(c->W2, c, 4), 1.0, 0.0, 0, field(c->W1, c, 2), 0.0, -s, 0);
+  set_job<T>(b, 5, field(c->W1, c, 0), field(c->W2, c, 5), 0.0, -s, 1, field(c->W1, c, 1), 0.0, s, 0);
   RET(run_strided<T>(c, 1, true, b, DNSBOX_PASS_Y_INV));
   // pass C: fused x pass
   XlineNLArgs<T> x;
@@ -418,8 +419,8 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   x.V = reinterpret_cast<const C *>(field(c->W2, c, 1));
   x.W = reinterpret_cast<const C *>(field(c->W2, c, 2));
   x.OX = reinterpret_cast<const C *>(field(c->W2, c, 3));
-  x.B1 = reinterpret_cast<const C *>(field(c->W2, c, 4));
-  x.C1 = reinterpret_cast<const C *>(field(c->W2, c, 5));
+  x.OY = reinterpret_cast<const C *>(field(c->W2, c, 4));
+  x.OZ = reinterpret_cast<const C *>(field(c->W2, c, 5));
   x.NX = reinterpret_cast<C *>(field(c->W1, c, 0));
   x.NY = reinterpret_cast<C *>(field(c->W1, c, 1));
   x.NZ = reinterpret_cast<C *>(field(c->W1, c, 2));
@@ -456,7 +457,8 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   e.nold = reinterpret_cast<C *>(nold);
   e.partials = partials ? c->partials : nullptr;
   e.mode = mode;
-  const int ntx = (c->nxh + TileCols<T>::v - 1) / TileCols<T>::v;
+  const int ztc = Ops<T>::zfinish_cols(p.nz);
+  const int ntx = (c->nxh + ztc - 1) / ztc;
   Prof pr(c, DNSBOX_PASS_Z_FIN);
   CK(Ops<T>::zfinish(p.nz, e, ntx * p.ny, c->stream));
   return DNSBOX_OK;
@@ -479,7 +481,8 @@ template <typename T> static int step_impl(dnsbox_ctx *c, void *uh, int nsteps, 
       // dnsbox.f90:143-191
       RET(run_rhs<T>(c, uh, FIN_AB2, nullptr, uh, c->nold, true, 1, drec));
     }
-    const int ntx = (c->nxh + TileCols<T>::v - 1) / TileCols<T>::v;
+    const int ztc = Ops<T>::zfinish_cols(p.nz);
+    const int ntx = (c->nxh + ztc - 1) / ztc;
     Prof pr(c, DNSBOX_PASS_SMALL);
     k_finalize<<<1, 1024, 0, c->stream>>>(c->st, c->partials, ntx * p.ny, s * s, p.nu, p.Q, p.Pin,
                                           p.bandlim, drec);
@@ -569,8 +572,10 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
   if ((rc = alloc_twiddles(c, 0, p->nx)) || (rc = alloc_twiddles(c, 1, p->ny)) ||
       (rc = alloc_twiddles(c, 2, p->nz)))
     return fail(rc);
-  const int ntx64 = (c->nxh + 7) / 8, ntx32 = (c->nxh + 15) / 16;
-  c->npartials = (c->fp64 ? ntx64 : ntx32) * p->ny;
+  {
+    const int ztc = c->fp64 ? Ops<double>::zfinish_cols(p->nz) : Ops<float>::zfinish_cols(p->nz);
+    c->npartials = ((c->nxh + ztc - 1) / ztc) * p->ny;
+  }
   if ((e = cudaMalloc(&c->partials, 2 * (size_t)c->npartials * sizeof(double))) != cudaSuccess)
     return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed"));
   // band modes |k| <= kCutOff (rhs.f90:145-149), stored as (offset lo, offset hi, kx)

@@ -199,4 +199,101 @@ __device__ __forceinline__ void fft_columns(C *s, int LD, int col, int p, bool a
   }
 }
 
+// ------------------------------------------------- register-resident ends
+// A thread's E values are v[m * R + r] for butterfly b = p + m P (P = N/E)
+// and leg r.  The first stage reads rows b + r N/R0 and the last stage writes
+// rows b + r N/RL: for consecutive p these are consecutive rows, so a caller
+// can load the first stage's inputs straight from global memory and store the
+// last stage's outputs straight back, with only the middle exchanges in
+// shared memory.
+template <int N> struct FftEnds {
+  using PL = FftPlan<N>;
+  static constexpr int E = PL::E;
+  static constexpr int P = N / E;
+  static constexpr int R0 = PL::R[0];
+  static constexpr int RL = PL::R[PL::NST - 1];
+  static constexpr int NB0 = N / R0;
+  static constexpr int NBL = N / RL;
+  __device__ static __forceinline__ int in_row(int p, int i) { return p + (i / R0) * P + (i % R0) * NB0; }
+  __device__ static __forceinline__ int out_row(int p, int i) { return p + (i / RL) * P + (i % RL) * NBL; }
+};
+
+// Stage 0 on registers (no twiddles since Ns = 1), result stored to shared
+// memory in Stockham order, then barrier.  For a single-stage plan the result
+// stays in v (in out_row order) and nothing touches shared memory.
+template <typename C, int N, bool INV>
+__device__ __forceinline__ void fft_first_regs(C *v, C *s, int LD, int col, int p, bool active) {
+  using PL = FftPlan<N>;
+  constexpr int R = PL::R[0];
+  constexpr int M = PL::E / R;
+  constexpr int P = N / PL::E;
+  if (active) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) dft<R, C, INV>(v + m * R);
+  }
+  if constexpr (PL::NST > 1) {
+    if (active) {
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int b = p + m * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) s[(b * R + r) * LD + col] = v[m * R + r];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Last stage from shared memory into registers (v in out_row order).  The
+// caller owns the barrier that must follow before shared memory is reused.
+template <typename C, int N, bool INV>
+__device__ __forceinline__ void fft_last_regs(C *v, const C *s, int LD, int col, int p, bool active,
+                                              const C *__restrict__ tw) {
+  using PL = FftPlan<N>;
+  constexpr int S = PL::NST - 1;
+  constexpr int R = PL::R[S];
+  constexpr int NS = PL::ns(S);
+  constexpr int NB = N / R;
+  constexpr int P = N / PL::E;
+  constexpr int M = PL::E / R;
+  if (!active) return;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int b = p + m * P;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[m * R + r] = s[(b + r * NB) * LD + col];
+    const int j = b % NS;
+    constexpr int TS = N / (NS * R);
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      const C w = __ldg(&tw[r * j * TS]);
+      v[m * R + r] = INV ? cmulc(v[m * R + r], w) : cmul(v[m * R + r], w);
+    }
+    dft<R, C, INV>(v + m * R);
+  }
+}
+
+// Stages 1 .. NST-2 in shared memory.
+template <typename C, int N, bool INV, int S = 1>
+__device__ __forceinline__ void fft_middle(C *s, int LD, int col, int p, bool active, const C *__restrict__ tw) {
+  if constexpr (S + 1 < FftPlan<N>::NST) {
+    fft_stage<C, N, S, INV>(s, LD, col, p, active, tw);
+    fft_middle<C, N, INV, S + 1>(s, LD, col, p, active, tw);
+  }
+}
+
+// Whole transform with v holding the first stage's inputs on entry and the
+// last stage's outputs on exit.  Shared memory (N x LD tile) is scratch;
+// ends with a barrier so the tile may be reused.
+template <typename C, int N, bool INV>
+__device__ __forceinline__ void fft_regs(C *v, C *s, int LD, int col, int p, bool active,
+                                         const C *__restrict__ tw) {
+  fft_first_regs<C, N, INV>(v, s, LD, col, p, active);
+  if constexpr (FftPlan<N>::NST > 1) {
+    fft_middle<C, N, INV>(s, LD, col, p, active, tw);
+    fft_last_regs<C, N, INV>(v, s, LD, col, p, active, tw);
+    __syncthreads();
+  }
+}
+
 }  // namespace dnsbox

@@ -120,6 +120,12 @@ template <typename T> struct Ops {
     switch (n) { DNSBOX_SIZES(DNSBOX_CASE_R2C) }
     return cudaErrorInvalidValue;
   }
+#define DNSBOX_CASE_FINC(NN) \
+  case NN: return Launcher<T, NN>::zfinish_cols();
+  static int zfinish_cols(int n) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_FINC) }
+    return 1;
+  }
 #define DNSBOX_CASE_FIN(NN) \
   case NN: return Launcher<T, NN>::zfinish(a, nb, st);
   static cudaError_t zfinish(int n, const FinishArgs<T> &a, int nb, cudaStream_t st) {

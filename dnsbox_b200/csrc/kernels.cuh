@@ -42,6 +42,11 @@ struct StepState {
 template <typename T> struct TileCols;
 template <> struct TileCols<double> { static constexpr int v = 8; };
 template <> struct TileCols<float> { static constexpr int v = 16; };
+// Tile width of the fused z finish, which holds three N-row tiles in shared
+// memory (halved at N = 1024 to stay within 227 KB per CTA).
+template <typename T, int N> struct FinishCols {
+  static constexpr int v = N >= 1024 ? TileCols<T>::v / 2 : TileCols<T>::v;
+};
 
 template <typename T> struct StridedJob {
   using C = typename CT<T>::type;
@@ -76,9 +81,10 @@ template <typename T, int N, bool INV>
 __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
     k_strided(const __grid_constant__ StridedArgs<T> a) {
   using C = typename CT<T>::type;
+  using EN = FftEnds<N>;
   constexpr int TC = TileCols<T>::v;
-  constexpr int NF = TC * (N / FftPlan<N>::E);   // FFT threads
-  const int NT = blockDim.x;
+  constexpr int E = EN::E;
+  constexpr int NF = TC * (N / E);   // FFT threads: column fastest, 128 B per row
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s = reinterpret_cast<C *>(smem_raw);
   const int job = blockIdx.x % a.njobs;
@@ -87,39 +93,48 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
   const int other = tile / ntx;
   const int kx0 = (tile - other * ntx) * TC;
   const StridedJob<T> &J = a.job[job];
-  const long long base = (long long)other * a.otherstride + kx0;
-  const bool plain1 = (J.a1 == 1.0 && J.b1 == 0.0);
-  for (int e = threadIdx.x; e < N * TC; e += NT) {
-    const int row = e / TC, col = e - (e / TC) * TC;
-    const int kx = kx0 + col;
-    C v = mkc<C>(0, 0);
-    if (kx < a.ncols) {
-      const long long off = base + (long long)row * a.rowstride + col;
-      v = J.in1[off];
-      if (!plain1) {
-        const double k = J.ks1 ? k_full(row, N, a.alpha_row) : k_half(kx, a.nx, a.alpha_x);
-        v = apply_mult<T>(v, J.a1, J.b1, k);
-      }
-      if (J.in2) {
-        const double k = J.ks2 ? k_full(row, N, a.alpha_row) : k_half(kx, a.nx, a.alpha_x);
-        v = cadd(v, apply_mult<T>(J.in2[off], J.a2, J.b2, k));
+  const bool act = threadIdx.x < NF;
+  const int col = threadIdx.x % TC, p = threadIdx.x / TC;
+  const int kx = kx0 + col;
+  const bool valid = act && kx < a.ncols;
+  const long long base = (long long)other * a.otherstride + kx;
+  C v[E];
+  if (valid) {
+    // all E loads of the first stage are independent and issued together
+    const C *in1 = J.in1 + base;
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = in1[(long long)EN::in_row(p, i) * a.rowstride];
+    if (!(J.a1 == 1.0 && J.b1 == 0.0)) {
+      const double kc = k_half(kx, a.nx, a.alpha_x);
+#pragma unroll
+      for (int i = 0; i < E; ++i)
+        v[i] = apply_mult<T>(v[i], J.a1, J.b1, J.ks1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc);
+    }
+    if (J.in2) {
+      const C *in2 = J.in2 + base;
+      const double kc = k_half(kx, a.nx, a.alpha_x);
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const C w = in2[(long long)EN::in_row(p, i) * a.rowstride];
+        v[i] = cadd(v[i], apply_mult<T>(w, J.a2, J.b2, J.ks2 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc));
       }
     }
-    s[e] = v;
+  } else {
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = mkc<C>(0, 0);
   }
-  __syncthreads();
-  const int col = threadIdx.x % TC, p = threadIdx.x / TC;
-  fft_columns<C, N, INV>(s, TC, col, p, threadIdx.x < NF, a.tw);
-  for (int e = threadIdx.x; e < N * TC; e += NT) {
-    const int row = e / TC, col2 = e - (e / TC) * TC;
-    if (kx0 + col2 < a.ncols) J.out[base + (long long)row * a.rowstride + col2] = s[e];
+  fft_regs<C, N, INV>(v, s, TC, col, p, act, a.tw);
+  if (valid) {
+    C *out = J.out + base;
+#pragma unroll
+    for (int i = 0; i < E; ++i) out[(long long)EN::out_row(p, i) * a.rowstride] = v[i];
   }
 }
 
 // ------------------------------------------------------------------ x lines
 template <typename T> struct XlineNLArgs {
   using C = typename CT<T>::type;
-  const C *U, *V, *W, *OX, *B1, *C1;  // (kx, y, z) space, rows of nxh
+  const C *U, *V, *W, *OX, *OY, *OZ;  // (kx, y, z) space, rows of nxh; omega scaled by 1/N^3
   C *NX, *NY, *NZ;                     // forward x transforms of (omega x u) * s
   const C *tw;
   double *umax;                        // 3 values, max |u_i| (true scale)
@@ -133,118 +148,116 @@ template <typename T, int N> struct XlineB {
   static constexpr int v = (N >= 512) ? 2 : (sizeof(T) == 8 ? (N >= 256 ? 4 : 8) : (N >= 256 ? 8 : 16));
 };
 
+// Full-length sequence value at row n of Z = X1 + i X2, where X1, X2 are the
+// half spectra (nxh values) of two real lines: rows above N/2 are the
+// Hermitian mirror; the imaginary parts of the kx = 0 and Nyquist bins are
+// dropped, as a C2R does.
+template <typename C, int N>
+__device__ __forceinline__ C pack_pair(int n, C X1, C X2) {
+  if (n == 0 || n == N / 2) return mkc<C>(X1.x, X2.x);
+  if (n < N / 2) return mkc<C>(X1.x - X2.y, X1.y + X2.x);
+  return mkc<C>(X1.x + X2.y, X2.x - X1.y);   // conj(X1) + i conj(X2) at N - n
+}
+
 template <typename T, int N>
 __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::E)))
     k_xline_nl(const __grid_constant__ XlineNLArgs<T> a) {
   using C = typename CT<T>::type;
+  using EN = FftEnds<N>;
   constexpr int B = XlineB<T, N>::v;
   constexpr int H = N / 2 + 1;
-  constexpr int LD = 3 * B;
-  constexpr int P = N / FftPlan<N>::E;
-  constexpr int NF = 3 * B * P;        // FFT threads of the inverse transforms
-  const int NT = blockDim.x;
+  constexpr int NCOL = 3 * B;
+  constexpr int LD = NCOL + 1;         // odd stride: rows fall in distinct bank groups
+  constexpr int E = EN::E;
+  constexpr int P = N / E;
+  constexpr int NF = NCOL * P;         // FFT threads, position index fastest
+  constexpr int NQ = NCOL / 2;         // forward sequences
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s = reinterpret_cast<C *>(smem_raw);
   __shared__ double red[3 * 32];
+  const int NT = blockDim.x;
   const int line0 = blockIdx.x * B;
   const T sc = T(a.s);
-  // Build Z = X1 + i X2.  Each pair holds two quantities of the same kind and
-  // scale (velocity is unscaled, vorticity carries the 1/N^3 of the
-  // reference's derivative transforms), so neither loses bits to the other.
-  // Per line pair (a = 2j, b = 2j+1) the six columns are
-  //   (u_a, v_a) (u_b, v_b) (w_a, w_b) (ox_a, oy_a) (ox_b, oy_b) (oz_a, oz_b).
-  for (int it = threadIdx.x; it < (B / 2) * 6 * H; it += NT) {
-    const int k = it % H;
-    const int q = (it / H) % 6;
-    const int j = it / (6 * H);
+  // Inverse transforms.  Column 6j+q of line pair (a = 2j, b = 2j+1) holds
+  // (u_a,v_a) (u_b,v_b) (w_a,w_b) (ox_a,oy_a) (ox_b,oy_b) (oz_a,oz_b): each
+  // pair is two quantities of the same kind and scale.
+  {
+    const bool act = threadIdx.x < NF;
+    const int p = threadIdx.x % P, col = threadIdx.x / P;
+    const int j = col / 6, q = col % 6;
     const int la = line0 + 2 * j, lb = la + 1;
-    const int col = 6 * j + q;
-    const T kx = T(k_half(k, N, a.alpha_x)) * sc;
-    const long long oa = (long long)la * a.nxh + k, ob = (long long)lb * a.nxh + k;
-    const bool va = la < a.nlines, vb = lb < a.nlines;
-    C X1 = mkc<C>(0, 0), X2 = mkc<C>(0, 0);
+    const C *f1, *f2;
+    int l1, l2;
     switch (q) {
-      case 0:
-        if (va) { X1 = a.U[oa]; X2 = a.V[oa]; }
-        break;
-      case 1:
-        if (vb) { X1 = a.U[ob]; X2 = a.V[ob]; }
-        break;
-      case 2:
-        if (va) X1 = a.W[oa];
-        if (vb) X2 = a.W[ob];
-        break;
-      case 3:
-      case 4: {
-        // omega_x, and omega_y = dz u - dx w (kx still spectral here)
-        const bool v = q == 3 ? va : vb;
-        const long long o = q == 3 ? oa : ob;
-        if (v) {
-          const C w = a.W[o], b1 = a.B1[o];
-          X1 = a.OX[o];
-          X2 = mkc<C>(b1.x + kx * w.y, b1.y - kx * w.x);   // b1 - i kx s w
-        }
-        break;
-      }
-      default: {
-        // omega_z = dx v - dy u for both lines
-        if (va) {
-          const C v = a.V[oa], c1 = a.C1[oa];
-          X1 = mkc<C>(c1.x - kx * v.y, c1.y + kx * v.x);   // c1 + i kx s v
-        }
-        if (vb) {
-          const C v = a.V[ob], c1 = a.C1[ob];
-          X2 = mkc<C>(c1.x - kx * v.y, c1.y + kx * v.x);
-        }
-        break;
-      }
+      case 0: f1 = a.U; l1 = la; f2 = a.V; l2 = la; break;
+      case 1: f1 = a.U; l1 = lb; f2 = a.V; l2 = lb; break;
+      case 2: f1 = a.W; l1 = la; f2 = a.W; l2 = lb; break;
+      case 3: f1 = a.OX; l1 = la; f2 = a.OY; l2 = la; break;
+      case 4: f1 = a.OX; l1 = lb; f2 = a.OY; l2 = lb; break;
+      default: f1 = a.OZ; l1 = la; f2 = a.OZ; l2 = lb; break;
     }
-    if (k == 0 || k == N / 2) {
-      s[k * LD + col] = mkc<C>(X1.x, X2.x);
-    } else {
-      s[k * LD + col] = mkc<C>(X1.x - X2.y, X1.y + X2.x);
-      s[(N - k) * LD + col] = mkc<C>(X1.x + X2.y, X2.x - X1.y);
+    const bool v1 = act && l1 < a.nlines, v2 = act && l2 < a.nlines;
+    const C *r1 = f1 + (long long)l1 * a.nxh, *r2 = f2 + (long long)l2 * a.nxh;
+    C v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int n = EN::in_row(p, i);
+      const int kk = n <= N / 2 ? n : N - n;
+      const C X1 = v1 ? r1[kk] : mkc<C>(0, 0);
+      const C X2 = v2 ? r2[kk] : mkc<C>(0, 0);
+      v[i] = pack_pair<C, N>(n, X1, X2);
+    }
+    fft_regs<C, N, true>(v, s, LD, col, p, act, a.tw);
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) s[EN::out_row(p, i) * LD + col] = v[i];
     }
   }
   __syncthreads();
-  {
-    const int col = threadIdx.x % (3 * B), p = threadIdx.x / (3 * B);
-    fft_columns<C, N, true>(s, LD, col, p, threadIdx.x < NF, a.tw);
-  }
-  // products (omega x u) * s, written back as three complex sequences per
-  // line pair: (px_a, py_a), (pz_a, pz_b), (px_b, py_b)
+  // (omega x u) * s at every point; written back as (px_a,py_a) (pz_a,pz_b)
+  // (px_b,py_b) in columns 6j, 6j+1, 6j+2
   double m0 = 0, m1 = 0, m2 = 0;
   for (int it = threadIdx.x; it < N * (B / 2); it += NT) {
-    const int j = it % (B / 2), n = it / (B / 2);
+    const int n = it % N, j = it / N;
     C *r = s + n * LD + 6 * j;
-    T px[2], py[2], pz[2];
     const C c0 = r[0], c1 = r[1], c2 = r[2], c3 = r[3], c4 = r[4], c5 = r[5];
     const T uu[2] = {c0.x, c1.x}, vv[2] = {c0.y, c1.y}, ww[2] = {c2.x, c2.y};
     const T ox[2] = {c3.x, c4.x}, oy[2] = {c3.y, c4.y}, oz[2] = {c5.x, c5.y};
+    T px[2], py[2], pz[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const T u = uu[h], v = vv[h], w = ww[h];
-      px[h] = (oy[h] * w - oz[h] * v) * sc;
-      py[h] = (oz[h] * u - ox[h] * w) * sc;
-      pz[h] = (ox[h] * v - oy[h] * u) * sc;
-      m0 = fmax(m0, fabs((double)u));
-      m1 = fmax(m1, fabs((double)v));
-      m2 = fmax(m2, fabs((double)w));
+      px[h] = (oy[h] * ww[h] - oz[h] * vv[h]) * sc;
+      py[h] = (oz[h] * uu[h] - ox[h] * ww[h]) * sc;
+      pz[h] = (ox[h] * vv[h] - oy[h] * uu[h]) * sc;
+      m0 = fmax(m0, fabs((double)uu[h]));
+      m1 = fmax(m1, fabs((double)vv[h]));
+      m2 = fmax(m2, fabs((double)ww[h]));
     }
     r[0] = mkc<C>(px[0], py[0]);
     r[1] = mkc<C>(pz[0], pz[1]);
     r[2] = mkc<C>(px[1], py[1]);
   }
   __syncthreads();
+  // forward transforms of the NQ product sequences
   {
-    constexpr int NQ = 3 * B / 2;
-    const bool active = threadIdx.x < NQ * P;
-    const int q = threadIdx.x % NQ, p = threadIdx.x / NQ;
+    const bool act = threadIdx.x < NQ * P;
+    const int p = threadIdx.x % P, q = threadIdx.x / P;
     const int col = 6 * (q / 3) + q % 3;
-    fft_columns<C, N, false>(s, LD, col, p, active, a.tw);
+    C v[E];
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = s[EN::in_row(p, i) * LD + col];
+    }
+    __syncthreads();
+    fft_regs<C, N, false>(v, s, LD, col, p, act, a.tw);
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) s[EN::out_row(p, i) * LD + col] = v[i];
+    }
   }
+  __syncthreads();
   // unpack two real transforms per sequence and store
-  for (int it = threadIdx.x; it < (3 * B / 2) * H; it += NT) {
+  for (int it = threadIdx.x; it < NQ * H; it += NT) {
     const int k = it % H, q = it / H;
     const int j = q / 3, c = q % 3;
     const int col = 6 * j + c;
@@ -296,8 +309,8 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
 // Plain x-line transforms of nf fields (blockIdx.y = field).
 template <typename T> struct XlineArgs {
   using C = typename CT<T>::type;
-  const void *in[3];
-  void *out[3];
+  const void *in[6];
+  void *out[6];
   const C *tw;
   int nlines, nxh;
   double scale;            // multiplies the output
@@ -312,37 +325,37 @@ template <typename T, int N>
 __global__ void __launch_bounds__(round32((XlinePlainB<T, N>::v / 2) * (N / FftPlan<N>::E)))
     k_xline_c2r(const __grid_constant__ XlineArgs<T> a) {
   using C = typename CT<T>::type;
+  using EN = FftEnds<N>;
   constexpr int B = XlinePlainB<T, N>::v;
   constexpr int NC = B / 2;
-  constexpr int H = N / 2 + 1;
-  constexpr int NF = NC * (N / FftPlan<N>::E);
-  const int NT = blockDim.x;
+  constexpr int LD = NC + 1;
+  constexpr int E = EN::E;
+  constexpr int P = N / E;
+  constexpr int NF = NC * P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s = reinterpret_cast<C *>(smem_raw);
   const C *in = reinterpret_cast<const C *>(a.in[blockIdx.y]);
   T *out = reinterpret_cast<T *>(a.out[blockIdx.y]);
-  const int line0 = blockIdx.x * B;
-  for (int it = threadIdx.x; it < NC * H; it += NT) {
-    const int k = it % H, j = it / H;
-    const int la = line0 + 2 * j, lb = la + 1;
-    const C X1 = la < a.nlines ? in[(long long)la * a.nxh + k] : mkc<C>(0, 0);
-    const C X2 = lb < a.nlines ? in[(long long)lb * a.nxh + k] : mkc<C>(0, 0);
-    if (k == 0 || k == N / 2) {
-      s[k * NC + j] = mkc<C>(X1.x, X2.x);
-    } else {
-      s[k * NC + j] = mkc<C>(X1.x - X2.y, X1.y + X2.x);
-      s[(N - k) * NC + j] = mkc<C>(X1.x + X2.y, X2.x - X1.y);
-    }
+  const bool act = threadIdx.x < NF;
+  const int p = threadIdx.x % P, j = threadIdx.x / P;
+  const int la = blockIdx.x * B + 2 * j, lb = la + 1;
+  const bool va = act && la < a.nlines, vb = act && lb < a.nlines;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int n = EN::in_row(p, i);
+    const int kk = n <= N / 2 ? n : N - n;
+    const C X1 = va ? in[(long long)la * a.nxh + kk] : mkc<C>(0, 0);
+    const C X2 = vb ? in[(long long)lb * a.nxh + kk] : mkc<C>(0, 0);
+    v[i] = pack_pair<C, N>(n, X1, X2);
   }
-  __syncthreads();
-  fft_columns<C, N, true>(s, NC, threadIdx.x % NC, threadIdx.x / NC, threadIdx.x < NF, a.tw);
+  fft_regs<C, N, true>(v, s, LD, j, p, act, a.tw);
   const T sc = T(a.scale);
-  for (int it = threadIdx.x; it < NC * N; it += NT) {
-    const int n = it % N, j = it / N;
-    const int la = line0 + 2 * j, lb = la + 1;
-    const C z = s[n * NC + j];
-    if (la < a.nlines) out[(long long)la * N + n] = z.x * sc;
-    if (lb < a.nlines) out[(long long)lb * N + n] = z.y * sc;
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int n = EN::out_row(p, i);
+    if (va) out[(long long)la * N + n] = v[i].x * sc;
+    if (vb) out[(long long)lb * N + n] = v[i].y * sc;
   }
 }
 
@@ -351,30 +364,43 @@ template <typename T, int N>
 __global__ void __launch_bounds__(round32((XlinePlainB<T, N>::v / 2) * (N / FftPlan<N>::E)))
     k_xline_r2c(const __grid_constant__ XlineArgs<T> a) {
   using C = typename CT<T>::type;
+  using EN = FftEnds<N>;
   constexpr int B = XlinePlainB<T, N>::v;
   constexpr int NC = B / 2;
+  constexpr int LD = NC + 1;
   constexpr int H = N / 2 + 1;
-  constexpr int NF = NC * (N / FftPlan<N>::E);
-  const int NT = blockDim.x;
+  constexpr int E = EN::E;
+  constexpr int P = N / E;
+  constexpr int NF = NC * P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s = reinterpret_cast<C *>(smem_raw);
   const T *in = reinterpret_cast<const T *>(a.in[blockIdx.y]);
   C *out = reinterpret_cast<C *>(a.out[blockIdx.y]);
+  const int NT = blockDim.x;
+  const bool act = threadIdx.x < NF;
+  const int p = threadIdx.x % P, j = threadIdx.x / P;
   const int line0 = blockIdx.x * B;
-  for (int it = threadIdx.x; it < NC * N; it += NT) {
-    const int n = it % N, j = it / N;
+  {
     const int la = line0 + 2 * j, lb = la + 1;
-    const T x1 = la < a.nlines ? in[(long long)la * N + n] : T(0);
-    const T x2 = lb < a.nlines ? in[(long long)lb * N + n] : T(0);
-    s[n * NC + j] = mkc<C>(x1, x2);
+    const bool va = act && la < a.nlines, vb = act && lb < a.nlines;
+    C v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int n = EN::in_row(p, i);
+      v[i] = mkc<C>(va ? in[(long long)la * N + n] : T(0), vb ? in[(long long)lb * N + n] : T(0));
+    }
+    fft_regs<C, N, false>(v, s, LD, j, p, act, a.tw);
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) s[EN::out_row(p, i) * LD + j] = v[i];
+    }
   }
   __syncthreads();
-  fft_columns<C, N, false>(s, NC, threadIdx.x % NC, threadIdx.x / NC, threadIdx.x < NF, a.tw);
   const T sc = T(a.scale);
   for (int it = threadIdx.x; it < NC * H; it += NT) {
-    const int k = it % H, j = it / H;
-    const int la = line0 + 2 * j, lb = la + 1;
-    const C zk = s[k * NC + j], zn = s[((N - k) % N) * NC + j];
+    const int k = it % H, jj = it / H;
+    const int la = line0 + 2 * jj, lb = la + 1;
+    const C zk = s[k * LD + jj], zn = s[((N - k) % N) * LD + jj];
     const C X1 = mkc<C>(T(0.5) * (zk.x + zn.x) * sc, T(0.5) * (zk.y - zn.y) * sc);
     const C X2 = mkc<C>(T(0.5) * (zk.y + zn.y) * sc, T(-0.5) * (zk.x - zn.x) * sc);
     if (la < a.nlines) out[(long long)la * a.nxh + k] = X1;
@@ -410,34 +436,45 @@ template <typename T> struct FinishArgs {
 };
 
 template <typename T, int N>
-__global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
+__global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::E)))
     k_zfinish(const __grid_constant__ FinishArgs<T> a) {
   using C = typename CT<T>::type;
-  constexpr int TC = TileCols<T>::v;
-  constexpr int NF = TC * (N / FftPlan<N>::E);
-  const int NT = blockDim.x;
+  using EN = FftEnds<N>;
+  constexpr int TC = FinishCols<T, N>::v;
+  constexpr int E = EN::E;
+  constexpr int NF = TC * (N / E);
+  constexpr int CH = 2;                 // modes per batch of global loads (E is even)
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *s = reinterpret_cast<C *>(smem_raw);
+  C *s = reinterpret_cast<C *>(smem_raw);   // three N x TC tiles, one per component
   __shared__ double red[2 * 32];
   const int ntx = (a.nxh + TC - 1) / TC;
   const int ky = blockIdx.x / ntx;
   const int kx0 = (blockIdx.x - ky * ntx) * TC;
   const long long rowstride = (long long)a.ny * a.nxh;
-  const long long base = (long long)ky * a.nxh + kx0;
+  const bool act = threadIdx.x < NF;
+  const int col = threadIdx.x % TC, p = threadIdx.x / TC;
+  const int kx = kx0 + col;
+  const bool valid = act && kx < a.nxh;
+  const long long base = (long long)ky * a.nxh + kx;
+  // forward z transforms of the three components, each using its own tile as
+  // scratch; fields 0 and 1 park their outputs in this thread's own slots of
+  // tiles 0 and 1, field 2 stays in v
+  C v[E];
   for (int f = 0; f < 3; ++f) {
-    const C *src = a.n3 + f * a.nh;
-    for (int e = threadIdx.x; e < N * TC; e += NT) {
-      const int row = e / TC, col = e - (e / TC) * TC;
-      s[f * N * TC + e] = (kx0 + col < a.nxh) ? src[base + row * rowstride + col] : mkc<C>(0, 0);
+    const C *src = a.n3 + f * a.nh + base;
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = valid ? src[(long long)EN::in_row(p, i) * rowstride] : mkc<C>(0, 0);
+    C *tile = s + f * N * TC;
+    fft_regs<C, N, false>(v, tile, TC, col, p, act, a.tw);
+    if (f < 2 && act) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) tile[EN::out_row(p, i) * TC + col] = v[i];
     }
   }
-  __syncthreads();
-  const int col = threadIdx.x % TC, p = threadIdx.x / TC;
-  for (int f = 0; f < 3; ++f) fft_columns<C, N, false>(s + f * N * TC, TC, col, p, threadIdx.x < NF, a.tw);
 
   const StepState *st = a.st;
-  const double dt = st ? st->dt : 0.0;
-  const double fc = (a.bandlim && st) ? a.Pin / (2.0 * st->eband) : 0.0;
+  const double dt = st->dt;
+  const double fc = a.bandlim ? a.Pin / (2.0 * st->eband) : 0.0;
   double c1 = 0, c2 = 0, tau2 = 0;
   if (a.mode == FIN_AB2) {
     const double tn = st->t, tm = st->t_prev;
@@ -452,92 +489,107 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
     tau2 = dt + tn - tm;
   }
   const double kyr = k_full(ky, a.ny, a.ay);
+  const double kxr = k_half(kx, a.nx, a.ax);
+  const double wk = (kxr == 0.0) ? 0.5 : 1.0;   // state.f90:436-440
   double esum = 0.0, dsum = 0.0;
-  for (int e = threadIdx.x; e < N * TC; e += NT) {
-    const int kz = e / TC, cl = e - (e / TC) * TC;
-    const int kx = kx0 + cl;
-    if (kx >= a.nxh) continue;
-    const long long idx = (long long)kz * rowstride + base + cl;
-    const double kxr = k_half(kx, a.nx, a.ax), kzr = k_full(kz, N, a.az);
-    const double k2 = kxr * kxr + kyr * kyr + kzr * kzr;
-    const bool zero = (kxr == 0.0) && (kyr == 0.0) && (kzr == 0.0);
-    const bool cut = (a.spherical && k2 >= a.sph2) || fabs(kxr) >= a.cutx || fabs(kyr) >= a.cuty ||
-                     fabs(kzr) >= a.cutz || zero;
-    C Nc[3];
-    if (cut) {
-      Nc[0] = Nc[1] = Nc[2] = mkc<C>(0, 0);
-    } else {
-      const C n0 = s[e], n1 = s[N * TC + e], n2 = s[2 * N * TC + e];
-      // phat = -(i k . n) / (-(k.k))  (rhs.f90:101-106)
-      const double knre = kxr * (double)n0.x + kyr * (double)n1.x + kzr * (double)n2.x;
-      const double knim = kxr * (double)n0.y + kyr * (double)n1.y + kzr * (double)n2.y;
-      const double pre = -knim / k2, pim = knre / k2;
-      const double kr[3] = {kxr, kyr, kzr};
-      const C nn[3] = {n0, n1, n2};
-      const bool forced = a.bandlim && sqrt(k2) <= a.kcut;
+  if (valid) {
+    const bool need_u = a.bandlim || a.mode != FIN_RHS;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        double re = -(double)nn[c].x + kr[c] * pim;
-        double im = -(double)nn[c].y - kr[c] * pre;
-        if (forced) {
-          const C u = a.uin[c * a.nh + idx];
-          re += fc * (double)u.x;
-          im += fc * (double)u.y;
+    for (int i0 = 0; i0 < E; i0 += CH) {
+      // batch the global operands of CH modes before any store
+      C uu[CH][3], ss[CH][3], no[CH][3];
+#pragma unroll
+      for (int h = 0; h < CH; ++h) {
+        const long long idx = (long long)EN::out_row(p, i0 + h) * rowstride + base;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          uu[h][c] = need_u ? a.uin[c * a.nh + idx] : mkc<C>(0, 0);
+          ss[h][c] = a.mode == FIN_CORR ? a.state[c * a.nh + idx] : mkc<C>(0, 0);
+          no[h][c] = a.mode == FIN_AB2 ? a.nold[c * a.nh + idx] : mkc<C>(0, 0);
         }
-        Nc[c] = mkc<C>(T(re), T(im));
       }
-    }
-    if (a.mode == FIN_RHS) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) a.out[c * a.nh + idx] = Nc[c];
-      continue;
-    }
-    const T IF = T(exp((a.Q - a.nu * k2) * dt));
-    const T tdt = T(dt);
-    if (a.mode == FIN_PRED) {
+      for (int h = 0; h < CH; ++h) {
+        const int i = i0 + h;
+        const int kz = EN::out_row(p, i);
+        const long long idx = (long long)kz * rowstride + base;
+        const double kzr = k_full(kz, N, a.az);
+        const double k2 = kxr * kxr + kyr * kyr + kzr * kzr;
+        const bool zero = (kxr == 0.0) && (kyr == 0.0) && (kzr == 0.0);
+        const bool cut = (a.spherical && k2 >= a.sph2) || fabs(kxr) >= a.cutx || fabs(kyr) >= a.cuty ||
+                         fabs(kzr) >= a.cutz || zero;
+        C Nc[3];
+        if (cut) {
+          Nc[0] = Nc[1] = Nc[2] = mkc<C>(0, 0);
+        } else {
+          const C nn[3] = {s[kz * TC + col], s[N * TC + kz * TC + col], v[i]};
+          // phat = -(i k . n) / (-(k.k))  (rhs.f90:101-106)
+          const double knre = kxr * (double)nn[0].x + kyr * (double)nn[1].x + kzr * (double)nn[2].x;
+          const double knim = kxr * (double)nn[0].y + kyr * (double)nn[1].y + kzr * (double)nn[2].y;
+          const double pre = -knim / k2, pim = knre / k2;
+          const double kr[3] = {kxr, kyr, kzr};
+          const bool forced = a.bandlim && sqrt(k2) <= a.kcut;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const C u = a.uin[c * a.nh + idx];
-        a.out[c * a.nh + idx] = mkc<C>((u.x + tdt * Nc[c].x) * IF, (u.y + tdt * Nc[c].y) * IF);
-        if (a.nold) a.nold[c * a.nh + idx] = Nc[c];
+          for (int c = 0; c < 3; ++c) {
+            double re = -(double)nn[c].x + kr[c] * pim;
+            double im = -(double)nn[c].y - kr[c] * pre;
+            if (forced) {
+              re += fc * (double)uu[h][c].x;
+              im += fc * (double)uu[h][c].y;
+            }
+            Nc[c] = mkc<C>(T(re), T(im));
+          }
+        }
+        if (a.mode == FIN_RHS) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) a.out[c * a.nh + idx] = Nc[c];
+          continue;
+        }
+        const T IF = T(exp((a.Q - a.nu * k2) * dt));
+        const T tdt = T(dt);
+        if (a.mode == FIN_PRED) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const C u = uu[h][c];
+            a.out[c * a.nh + idx] = mkc<C>((u.x + tdt * Nc[c].x) * IF, (u.y + tdt * Nc[c].y) * IF);
+            if (a.nold) a.nold[c * a.nh + idx] = Nc[c];
+          }
+          continue;
+        }
+        C un[3];
+        if (a.mode == FIN_CORR) {
+          const T hf = T(0.5), hdt = T(0.5 * dt);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const C u = ss[h][c], us = uu[h][c];
+            un[c] = mkc<C>(hf * (IF * u.x + us.x) + hdt * Nc[c].x, hf * (IF * u.y + us.y) + hdt * Nc[c].y);
+            a.state[c * a.nh + idx] = un[c];
+          }
+        } else {  // FIN_AB2
+          const T e1c1 = T(c1) * IF;
+          const T e2c2 = T(c2 * exp((a.Q - a.nu * k2) * tau2));
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const C u = uu[h][c], o = no[h][c];
+            un[c] = mkc<C>(IF * u.x + e1c1 * Nc[c].x + e2c2 * o.x, IF * u.y + e1c1 * Nc[c].y + e2c2 * o.y);
+            a.state[c * a.nh + idx] = un[c];
+            a.nold[c * a.nh + idx] = Nc[c];
+          }
+        }
+        double e2 = 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) e2 += (double)un[c].x * un[c].x + (double)un[c].y * un[c].y;
+        esum += wk * e2;
+        dsum += 2.0 * wk * k2 * e2;
       }
-      continue;
-    }
-    C un[3];
-    if (a.mode == FIN_CORR) {
-      const T h = T(0.5), hdt = T(0.5 * dt);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const C u = a.state[c * a.nh + idx], us = a.uin[c * a.nh + idx];
-        un[c] = mkc<C>(h * (IF * u.x + us.x) + hdt * Nc[c].x, h * (IF * u.y + us.y) + hdt * Nc[c].y);
-        a.state[c * a.nh + idx] = un[c];
-      }
-    } else {  // FIN_AB2
-      const T e1c1 = T(c1) * IF;
-      const T e2c2 = T(c2 * exp((a.Q - a.nu * k2) * tau2));
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const C u = a.uin[c * a.nh + idx], no = a.nold[c * a.nh + idx];
-        un[c] = mkc<C>(IF * u.x + e1c1 * Nc[c].x + e2c2 * no.x, IF * u.y + e1c1 * Nc[c].y + e2c2 * no.y);
-        a.state[c * a.nh + idx] = un[c];
-        a.nold[c * a.nh + idx] = Nc[c];
-      }
-    }
-    if (a.partials) {
-      const double wk = (kxr == 0.0) ? 0.5 : 1.0;   // state.f90:436-440
-      double e2 = 0;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) e2 += (double)un[c].x * un[c].x + (double)un[c].y * un[c].y;
-      esum += wk * e2;
-      dsum += 2.0 * wk * k2 * e2;
     }
   }
   if (a.partials) {
-    double v[2] = {esum, dsum};
-    block_sum<2>(v, red);
+    double r2[2] = {esum, dsum};
+    block_sum<2>(r2, red);
     if (threadIdx.x == 0) {
-      a.partials[2 * blockIdx.x] = v[0];
-      a.partials[2 * blockIdx.x + 1] = v[1];
+      a.partials[2 * blockIdx.x] = r2[0];
+      a.partials[2 * blockIdx.x + 1] = r2[1];
     }
   }
 }

@@ -15,6 +15,7 @@ template <typename T, int N> struct Launcher {
   static cudaError_t zfinish(const FinishArgs<T> &a, int nblocks, cudaStream_t st);
   static int strided_threads();
   static int zfinish_threads();
+  static int zfinish_cols();
 };
 
 #define DNSBOX_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512) X(1024)
@@ -33,8 +34,9 @@ template <typename T, int N> int Launcher<T, N>::strided_threads() {
   return round32(TileCols<T>::v * (N / FftPlan<N>::E));
 }
 template <typename T, int N> int Launcher<T, N>::zfinish_threads() {
-  return round32(TileCols<T>::v * (N / FftPlan<N>::E));
+  return round32(FinishCols<T, N>::v * (N / FftPlan<N>::E));
 }
+template <typename T, int N> int Launcher<T, N>::zfinish_cols() { return FinishCols<T, N>::v; }
 
 template <typename T, int N>
 cudaError_t Launcher<T, N>::strided(const StridedArgs<T> &a, bool inv, int ntiles, cudaStream_t st) {
@@ -57,7 +59,7 @@ template <typename T, int N>
 cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, cudaStream_t st) {
   using C = typename CT<T>::type;
   constexpr int B = XlineB<T, N>::v;
-  const size_t smem = (size_t)N * 3 * B * sizeof(C);
+  const size_t smem = (size_t)N * (3 * B + 1) * sizeof(C);
   const int nt = round32(3 * B * (N / FftPlan<N>::E));
   cudaError_t e;
   if ((e = set_smem(k_xline_nl<T, N>, smem)) != cudaSuccess) return e;
@@ -70,7 +72,7 @@ template <typename T, int N>
 cudaError_t Launcher<T, N>::xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st) {
   using C = typename CT<T>::type;
   constexpr int B = XlinePlainB<T, N>::v;
-  const size_t smem = (size_t)N * (B / 2) * sizeof(C);
+  const size_t smem = (size_t)N * (B / 2 + 1) * sizeof(C);
   const int nt = round32((B / 2) * (N / FftPlan<N>::E));
   cudaError_t e;
   if ((e = set_smem(k_xline_c2r<T, N>, smem)) != cudaSuccess) return e;
@@ -83,7 +85,7 @@ template <typename T, int N>
 cudaError_t Launcher<T, N>::xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_t st) {
   using C = typename CT<T>::type;
   constexpr int B = XlinePlainB<T, N>::v;
-  const size_t smem = (size_t)N * (B / 2) * sizeof(C);
+  const size_t smem = (size_t)N * (B / 2 + 1) * sizeof(C);
   const int nt = round32((B / 2) * (N / FftPlan<N>::E));
   cudaError_t e;
   if ((e = set_smem(k_xline_r2c<T, N>, smem)) != cudaSuccess) return e;
@@ -95,7 +97,7 @@ cudaError_t Launcher<T, N>::xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_
 template <typename T, int N>
 cudaError_t Launcher<T, N>::zfinish(const FinishArgs<T> &a, int nblocks, cudaStream_t st) {
   using C = typename CT<T>::type;
-  const size_t smem = (size_t)3 * N * TileCols<T>::v * sizeof(C);
+  const size_t smem = (size_t)3 * N * FinishCols<T, N>::v * sizeof(C);
   const int nt = zfinish_threads();
   cudaError_t e;
   if ((e = set_smem(k_zfinish<T, N>, smem)) != cudaSuccess) return e;

@@ -75,7 +75,7 @@ def test_transform_round_trip_large(n):
 
 # ---------------------------------------------------------------- nonlinear term
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
-@pytest.mark.parametrize("n", [8, 12, 16, 24, 32, 48, 64, 96])
+@pytest.mark.parametrize("n", [8, 12, 16, 24, 32, 48, 64, 96, 128, 192])
 @pytest.mark.parametrize("bandlim", [False, True])
 def test_rhs_nonlinear(prec, n, bandlim):
     uh = field(n, seed=n, k0=3.0)
