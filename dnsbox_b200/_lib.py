@@ -99,6 +99,10 @@ SIGNATURES = {
     "dnsbox_download_physical": (ctypes.c_int, [_VP, _VP, _VP]),
     "dnsbox_rhs_adj": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "dnsbox_rhs_nonlinear_vjp": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "dnsbox_set_forcing": (ctypes.c_int, [_VP, _VP]),
+    "dnsbox_residual": (ctypes.c_int, [_VP, _VP, _DP]),
+    "dnsbox_residual_grad": (ctypes.c_int, [_VP, _VP, _VP, _DP]),
+    "dnsbox_adjoint_descent": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _DP, _DP]),
     "dnsbox_profile_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dnsbox_profile_read": (ctypes.c_int, [_VP, ctypes.POINTER(Profile), ctypes.c_int]),
 }

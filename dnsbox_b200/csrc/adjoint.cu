@@ -1,0 +1,574 @@
+// Adjoint operators and adjoint descent.
+//
+//  dnsbox_rhs_adj            rhsAdj (rhsAdj.f90:356-381), restated literally:
+//                            convective-form N (rhsAdj.f90:64-175, '.gt.' mask,
+//                            eps = 1e-13 at k = 0), r~ = H^-1 (L u + N)
+//                            (rhsupptilde, :177-213), the adjoint nonlinear term
+//                            -P_d[(grad r~)^T u + (u.grad) r~] (:261-354) and
+//                            rhsadj = L r~ + N_adj.
+//  dnsbox_rhs_nonlinear_vjp  the exact transpose of the linearised
+//                            rhs_nonlinear (Euclidean inner product on the Re/Im
+//                            parts of the half spectrum):
+//                              h = -P(D g),  phi = C2R(h / W),
+//                              u = C2R(uhat) s,  omega = C2R(ik x uhat) s,
+//                              out = s W (ik x R2C(u x phi) + R2C(phi x omega))
+//                            plus the band-forcing term when bandlim is on.
+//  dnsbox_residual(_grad)    J = 1/2 s^2 sum_half W h |r|^2 with r = L u + N(u) + f
+//                            (h = 1/(1+|k|^2) when hminone), and its gradient.
+//  dnsbox_adjoint_descent    steepest descent on J with an FP64 Armijo line search.
+//
+// W is the half-spectrum multiplicity (1 on the kx = 0 and Nyquist planes, 2
+// elsewhere); L = Q - nu |k|^2 (the reference's nu (k.k) + Q with imaginary k).
+#include "internal.cuh"
+
+namespace {
+
+struct Grid3 {
+  int nx, ny, nz, nxh;
+  double ax, ay, az;
+  double cutx, cuty, cutz, sph2;
+  int spherical;
+};
+
+__device__ __forceinline__ void mode_k(const Grid3 &g, long long m, double &kx, double &ky, double &kz) {
+  const int ix = (int)(m % g.nxh);
+  const int iy = (int)((m / g.nxh) % g.ny);
+  const int iz = (int)(m / ((long long)g.nxh * g.ny));
+  kx = k_half(ix, g.nx, g.ax);
+  ky = k_full(iy, g.ny, g.ay);
+  kz = k_full(iz, g.nz, g.az);
+}
+
+// rhs.f90:74-88 mask (dealias, .ge., spherical factor 0.5, or k = 0)
+__device__ __forceinline__ bool rhs_masked(const Grid3 &g, double kx, double ky, double kz) {
+  const double k2 = kx * kx + ky * ky + kz * kz;
+  return (g.spherical && k2 >= g.sph2) || fabs(kx) >= g.cutx || fabs(ky) >= g.cuty || fabs(kz) >= g.cutz ||
+         (kx == 0.0 && ky == 0.0 && kz == 0.0);
+}
+
+// rhsAdj.f90:131-136 mask (.gt., no k = 0 term)
+__device__ __forceinline__ bool adj_masked(const Grid3 &g, double kx, double ky, double kz) {
+  return fabs(kx) > g.cutx || fabs(ky) > g.cuty || fabs(kz) > g.cutz;
+}
+
+#define GRID_LOOP(m, n)                                                                   \
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < (n);           \
+       m += (long long)gridDim.x * blockDim.x)
+
+// h / W = -P(D g) / W
+template <typename C>
+__global__ void k_vjp_pre(const C *g, C *hw, long long nh, Grid3 gr) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    if (rhs_masked(gr, kx, ky, kz)) {
+      for (int c = 0; c < 3; ++c) hw[c * nh + m] = mkc<C>(0, 0);
+      continue;
+    }
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double kr[3] = {kx, ky, kz};
+    const C v[3] = {g[m], g[nh + m], g[2 * nh + m]};
+    const double dre = (kx * v[0].x + ky * v[1].x + kz * v[2].x) / k2;
+    const double dim = (kx * v[0].y + ky * v[1].y + kz * v[2].y) / k2;
+    const double w = (kx == 0.0) ? 1.0 : 0.5;   // 1 / W
+    for (int c = 0; c < 3; ++c)
+      hw[c * nh + m] = mkc<C>(T(-(v[c].x - kr[c] * dre) * w), T(-(v[c].y - kr[c] * dim) * w));
+  }
+}
+
+// physical: u <- u x phi, omega <- phi x omega (u: f[0..2], omega: f[3..5], phi: f[6..8])
+template <typename T>
+__global__ void k_vjp_cross(T *f, long long np) {
+  GRID_LOOP(i, np) {
+    const T u0 = f[i], u1 = f[np + i], u2 = f[2 * np + i];
+    const T o0 = f[3 * np + i], o1 = f[4 * np + i], o2 = f[5 * np + i];
+    const T p0 = f[6 * np + i], p1 = f[7 * np + i], p2 = f[8 * np + i];
+    f[i] = u1 * p2 - u2 * p1;
+    f[np + i] = u2 * p0 - u0 * p2;
+    f[2 * np + i] = u0 * p1 - u1 * p0;
+    f[3 * np + i] = p1 * o2 - p2 * o1;
+    f[4 * np + i] = p2 * o0 - p0 * o2;
+    f[5 * np + i] = p0 * o1 - p1 * o0;
+  }
+}
+
+// out = s W (ik x A + B)
+template <typename C>
+__global__ void k_vjp_combine(const C *A, const C *Bv, C *out, long long nh, Grid3 gr, double s) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    const double sw = s * ((kx == 0.0) ? 1.0 : 2.0);
+    const C a0 = A[m], a1 = A[nh + m], a2 = A[2 * nh + m];
+    // i (k x a): component = i (k_j a_k - k_k a_j)
+    const double cx_re = -(ky * a2.y - kz * a1.y), cx_im = ky * a2.x - kz * a1.x;
+    const double cy_re = -(kz * a0.y - kx * a2.y), cy_im = kz * a0.x - kx * a2.x;
+    const double cz_re = -(kx * a1.y - ky * a0.y), cz_im = kx * a1.x - ky * a0.x;
+    const C b0 = Bv[m], b1 = Bv[nh + m], b2 = Bv[2 * nh + m];
+    out[m] = mkc<C>(T(sw * (cx_re + b0.x)), T(sw * (cx_im + b0.y)));
+    out[nh + m] = mkc<C>(T(sw * (cy_re + b1.x)), T(sw * (cy_im + b1.y)));
+    out[2 * nh + m] = mkc<C>(T(sw * (cz_re + b2.x)), T(sw * (cz_im + b2.y)));
+  }
+}
+
+// Band forcing part of the VJP (one block): with c = Pin / (2 Eb),
+// out += c (Bm g) - (Pin / (2 Eb^2)) <Bm u, g> 2 s^2 (w Bb u), where Bb are the
+// band modes of rhs_Eband (weight w = 1/2 on kx = 0) and Bm those of them that
+// the rhs.f90 mask keeps.
+template <typename C>
+__global__ void k_vjp_band(const C *u, const C *g, C *out, long long nh, const int *band, int nband, Grid3 gr,
+                           const StepState *st, double Pin, double s2) {
+  using T = decltype(C{}.x);
+  __shared__ double red[32];
+  const double eb = st->eband;
+  double dot = 0.0;
+  for (int i = threadIdx.x; i < nband; i += blockDim.x) {
+    const long long off = (long long)(unsigned)band[3 * i] | ((long long)band[3 * i + 1] << 32);
+    double kx, ky, kz;
+    mode_k(gr, off, kx, ky, kz);
+    if (rhs_masked(gr, kx, ky, kz)) continue;
+    for (int c = 0; c < 3; ++c) {
+      const C a = u[c * nh + off], b = g[c * nh + off];
+      dot += (double)a.x * b.x + (double)a.y * b.y;
+    }
+  }
+  double v[1] = {dot};
+  block_sum<1>(v, red);
+  __shared__ double dsh;
+  if (threadIdx.x == 0) dsh = v[0];
+  __syncthreads();
+  dot = dsh;
+  const double cf = Pin / (2.0 * eb), cg = Pin / (2.0 * eb * eb) * dot * 2.0 * s2;
+  for (int i = threadIdx.x; i < nband; i += blockDim.x) {
+    const long long off = (long long)(unsigned)band[3 * i] | ((long long)band[3 * i + 1] << 32);
+    double kx, ky, kz;
+    mode_k(gr, off, kx, ky, kz);
+    const bool keep = !rhs_masked(gr, kx, ky, kz);
+    const double w = (kx == 0.0) ? 0.5 : 1.0;
+    for (int c = 0; c < 3; ++c) {
+      const C a = u[c * nh + off], b = g[c * nh + off];
+      C o = out[c * nh + off];
+      double re = o.x - cg * w * a.x, im = o.y - cg * w * a.y;
+      if (keep) {
+        re += cf * b.x;
+        im += cf * b.y;
+      }
+      out[c * nh + off] = mkc<C>(T(re), T(im));
+    }
+  }
+}
+
+// rhsAdj.f90:83-121: p_c = sum_j u_j d_j u_c * s  (u = f[0..2] unscaled, grad(c,j) = f[3+3c+j], out f[12..14])
+template <typename T>
+__global__ void k_conv_prod(T *f, long long np, double s) {
+  GRID_LOOP(i, np) {
+    const T u[3] = {f[i], f[np + i], f[2 * np + i]};
+    for (int c = 0; c < 3; ++c) {
+      T acc = 0;
+      for (int j = 0; j < 3; ++j) acc += u[j] * f[(3 + 3 * c + j) * np + i];
+      f[(12 + c) * np + i] = acc * T(s);
+    }
+  }
+}
+
+// rhsAdj.f90:271-309: q_c = (sum_j d_c r_j u_j + sum_j d_j r_c u_j) * s
+template <typename T>
+__global__ void k_adj_prod(T *f, long long np, double s) {
+  GRID_LOOP(i, np) {
+    const T u[3] = {f[i], f[np + i], f[2 * np + i]};
+    for (int c = 0; c < 3; ++c) {
+      T acc = 0;
+      for (int j = 0; j < 3; ++j) acc += f[(3 + 3 * j + c) * np + i] * u[j] + f[(3 + 3 * c + j) * np + i] * u[j];
+      f[(12 + c) * np + i] = acc * T(s);
+    }
+  }
+}
+
+// rhsAdj.f90 spectral loop (:128-169 / :311-352) on n -> N; stage 1 also forms
+// r~ = H^-1 (L u + N) (rhsupptilde, :177-213); stage 2 forms rhsadj = L r~ + N_adj.
+template <typename C>
+__global__ void k_adj_finish(const C *n, const C *uin, C *out, long long nh, Grid3 gr, double nu, double Q,
+                             int stage, int hminone, int phat_literal) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double kr[3] = {kx, ky, kz};
+    double N[3][2];
+    if (adj_masked(gr, kx, ky, kz)) {
+      for (int c = 0; c < 3; ++c) N[c][0] = N[c][1] = 0.0;
+    } else {
+      const double eps = (kx == 0.0 && ky == 0.0 && kz == 0.0) ? 1.0e-13 : 0.0;
+      const C v[3] = {n[m], n[nh + m], n[2 * nh + m]};
+      const double knre = kx * v[0].x + ky * v[1].x + kz * v[2].x;
+      const double knim = kx * v[0].y + ky * v[1].y + kz * v[2].y;
+      // phat = -(i k.n) / (-(k.k) + eps)
+      double pre = knim / (-k2 + eps), pim = -knre / (-k2 + eps);
+      if (stage == 2 && phat_literal) pre = pim = 0.0;   // phatadj never assigned (Q6)
+      for (int c = 0; c < 3; ++c) {
+        N[c][0] = -(double)v[c].x + kr[c] * pim;
+        N[c][1] = -(double)v[c].y - kr[c] * pre;
+      }
+    }
+    const double L = Q - nu * k2;
+    if (stage == 1) {
+      const double h = hminone ? 1.0 / (1.0 + k2) : 1.0;
+      for (int c = 0; c < 3; ++c) {
+        const C u = uin[c * nh + m];
+        out[c * nh + m] = mkc<C>(T(h * (L * u.x + N[c][0])), T(h * (L * u.y + N[c][1])));
+      }
+    } else {
+      for (int c = 0; c < 3; ++c) {
+        const C r = uin[c * nh + m];
+        out[c * nh + m] = mkc<C>(T(L * r.x + N[c][0]), T(L * r.y + N[c][1]));
+      }
+    }
+  }
+}
+
+// r = L u + N (N already carries any fixed forcing); per-block partials of
+// J = 1/2 s^2 sum W h |r|^2; gE = s^2 W h r
+template <typename C>
+__global__ void k_residual(const C *u, const C *N, C *gE, long long nh, Grid3 gr, double nu, double Q, int hminone,
+                           double s2, double *partials) {
+  using T = decltype(C{}.x);
+  __shared__ double red[32];
+  double acc = 0.0;
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double L = Q - nu * k2;
+    const double h = hminone ? 1.0 / (1.0 + k2) : 1.0;
+    const double W = (kx == 0.0) ? 1.0 : 2.0;
+    for (int c = 0; c < 3; ++c) {
+      const C a = u[c * nh + m], b = N[c * nh + m];
+      const double re = L * a.x + b.x, im = L * a.y + b.y;
+      acc += 0.5 * s2 * W * h * (re * re + im * im);
+      if (gE) gE[c * nh + m] = mkc<C>(T(s2 * W * h * re), T(s2 * W * h * im));
+    }
+  }
+  double v[1] = {acc};
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
+// grad += L gE
+template <typename C>
+__global__ void k_add_linear(C *grad, const C *gE, long long nh, Grid3 gr, double nu, double Q) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    const double L = Q - nu * (kx * kx + ky * ky + kz * kz);
+    for (int c = 0; c < 3; ++c) {
+      const C a = grad[c * nh + m], b = gE[c * nh + m];
+      grad[c * nh + m] = mkc<C>(T(a.x + L * b.x), T(a.y + L * b.y));
+    }
+  }
+}
+
+// d = -P D (grad / (s^2 W)): the steepest-descent direction in the
+// mean-square metric <|u|^2> = s^2 sum_half W |uhat|^2 of J's own norm,
+// projected and dealiased so the state stays admissible; per-block partials
+// of <grad, d>
+template <typename C>
+__global__ void k_descent_dir(const C *grad, C *d, long long nh, Grid3 gr, double s2, double *partials) {
+  using T = decltype(C{}.x);
+  __shared__ double red[32];
+  double acc = 0.0;
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    if (rhs_masked(gr, kx, ky, kz)) {
+      for (int c = 0; c < 3; ++c) d[c * nh + m] = mkc<C>(0, 0);
+      continue;
+    }
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double kr[3] = {kx, ky, kz};
+    const double w = ((kx == 0.0) ? 1.0 : 0.5) / s2;
+    const C v[3] = {grad[m], grad[nh + m], grad[2 * nh + m]};
+    const double dre = (kx * v[0].x + ky * v[1].x + kz * v[2].x) / k2;
+    const double dim = (kx * v[0].y + ky * v[1].y + kz * v[2].y) / k2;
+    for (int c = 0; c < 3; ++c) {
+      const double re = -(v[c].x - kr[c] * dre) * w, im = -(v[c].y - kr[c] * dim) * w;
+      d[c * nh + m] = mkc<C>(T(re), T(im));
+      acc += re * v[c].x + im * v[c].y;
+    }
+  }
+  double v[1] = {acc};
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
+template <typename C>
+__global__ void k_axpy(const C *x, const C *d, C *y, long long n, double alpha) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(i, n) {
+    const C a = x[i], b = d[i];
+    y[i] = mkc<C>(T(a.x + alpha * b.x), T(a.y + alpha * b.y));
+  }
+}
+
+constexpr int kRedBlocks = 148 * 2;
+
+Grid3 grid3(const dnsbox_ctx *c) {
+  const dnsbox_params &p = c->p;
+  Grid3 g;
+  g.nx = p.nx;
+  g.ny = p.ny;
+  g.nz = p.nz;
+  g.nxh = c->nxh;
+  g.ax = p.alpha_x;
+  g.ay = p.alpha_y;
+  g.az = p.alpha_z;
+  g.cutx = (p.nx / 2.0) * (2.0 * p.alpha_x / 3.0);
+  g.cuty = (p.ny / 2.0) * (2.0 * p.alpha_y / 3.0);
+  g.cutz = (p.nz / 2.0) * (2.0 * p.alpha_z / 3.0);
+  g.sph2 = pow((p.nx / 2.0) * 0.5 * p.alpha_x, 2);
+  g.spherical = p.spherical;
+  return g;
+}
+
+// adjoint arena: nphys physical fields followed by nspec spectral fields
+int ensure_adj(dnsbox_ctx *c, int nphys, int nspec, char **phys, char **spec) {
+  const size_t pb = c->np * (c->cbytes / 2), sb = c->nh * c->cbytes;
+  const size_t need = nphys * pb + nspec * sb;
+  if (need > c->adj_bytes) {
+    if (c->adj) cudaFree(c->adj);
+    c->adj = nullptr;
+    c->adj_bytes = 0;
+    CK(cudaMalloc(&c->adj, need));
+    c->adj_bytes = need;
+  }
+  *phys = c->adj;
+  *spec = c->adj + nphys * pb;
+  return DNSBOX_OK;
+}
+
+int sum_to_host(dnsbox_ctx *c, int nblk, double *out) {
+  k_sum_scalar<256><<<1, 256, 0, c->stream>>>(c->red, nblk, c->red + nblk);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->hstage, c->red + nblk, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *out = c->hstage[0];
+  return DNSBOX_OK;
+}
+
+template <typename T>
+int vjp_impl(dnsbox_ctx *c, const void *uh, const void *g, void *out) {
+  using C = typename CT<T>::type;
+  const dnsbox_params &p = c->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  const size_t pb = c->np * sizeof(T), sb = c->nh * sizeof(C);
+  char *P = nullptr, *S = nullptr;
+  RET(ensure_adj(c, 9, 6, &P, &S));
+  const Grid3 gr = grid3(c);
+  const int gb = grid_for((long long)c->nh);
+  const long long nh = (long long)c->nh, np = (long long)c->np;
+  const char *u = reinterpret_cast<const char *>(uh);
+  k_vjp_pre<C><<<gb, 256, 0, c->stream>>>(reinterpret_cast<const C *>(g), reinterpret_cast<C *>(S), nh, gr);
+  CK(cudaGetLastError());
+  // u (scaled), omega = ik x u (scaled), phi = C2R(h / W)
+  const void *u0 = u, *u1 = u + sb, *u2 = u + 2 * sb;
+  SpecJob jobs[9] = {
+      {{{u0, s, 0, 0}, {nullptr, 0, 0, 0}}, 1},
+      {{{u1, s, 0, 0}, {nullptr, 0, 0, 0}}, 1},
+      {{{u2, s, 0, 0}, {nullptr, 0, 0, 0}}, 1},
+      {{{u2, 0, s, 2}, {u1, 0, -s, 1}}, 2},   // i (ky w - kz v)
+      {{{u0, 0, s, 1}, {u2, 0, -s, 0}}, 2},   // i (kz u - kx w)
+      {{{u1, 0, s, 0}, {u0, 0, -s, 2}}, 2},   // i (kx v - ky u)
+      {{{S, 1, 0, 0}, {nullptr, 0, 0, 0}}, 1},
+      {{{S + sb, 1, 0, 0}, {nullptr, 0, 0, 0}}, 1},
+      {{{S + 2 * sb, 1, 0, 0}, {nullptr, 0, 0, 0}}, 1},
+  };
+  void *outs[9];
+  for (int i = 0; i < 9; ++i) outs[i] = P + i * pb;
+  RET(c2r_jobs<T>(c, 9, jobs, outs, 1.0));
+  k_vjp_cross<T><<<grid_for(np), 256, 0, c->stream>>>(reinterpret_cast<T *>(P), np);
+  CK(cudaGetLastError());
+  const void *ins[6];
+  void *specs[6];
+  for (int i = 0; i < 6; ++i) {
+    ins[i] = P + i * pb;
+    specs[i] = S + i * sb;
+  }
+  RET(r2c_fields<T>(c, 6, ins, specs));
+  k_vjp_combine<C><<<gb, 256, 0, c->stream>>>(reinterpret_cast<const C *>(S), reinterpret_cast<const C *>(S + 3 * sb),
+                                              reinterpret_cast<C *>(out), nh, gr, s);
+  CK(cudaGetLastError());
+  if (p.bandlim && c->nband) {
+    k_eband<C><<<1, 256, 0, c->stream>>>(reinterpret_cast<const C *>(uh), nh, c->band, c->nband, p.nx, c->st,
+                                         s * s, 0);
+    k_vjp_band<C><<<1, 256, 0, c->stream>>>(reinterpret_cast<const C *>(uh), reinterpret_cast<const C *>(g),
+                                            reinterpret_cast<C *>(out), nh, c->band, c->nband, gr, c->st, p.Pin,
+                                            s * s);
+    CK(cudaGetLastError());
+  }
+  return DNSBOX_OK;
+}
+
+template <typename T>
+int rhs_adj_impl(dnsbox_ctx *c, const void *uh, void *rt, void *rhsadj) {
+  using C = typename CT<T>::type;
+  const dnsbox_params &p = c->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  const size_t pb = c->np * sizeof(T), sb = c->nh * sizeof(C);
+  char *P = nullptr, *S = nullptr;
+  RET(ensure_adj(c, 15, 3, &P, &S));
+  const Grid3 gr = grid3(c);
+  const int gb = grid_for((long long)c->nh);
+  const long long nh = (long long)c->nh, np = (long long)c->np;
+  const char *u = reinterpret_cast<const char *>(uh);
+  const int ks_of_dir[3] = {0, 2, 1};   // d/dx: kx, d/dy: ky (other axis of the z pass), d/dz: kz (row)
+  // stage 1: u (unscaled, x N^3) and grad u (rhsAdj.f90:8-52, 75-77)
+  SpecJob jobs[12];
+  for (int cc = 0; cc < 3; ++cc) jobs[cc] = SpecJob{{{u + cc * sb, 1.0, 0.0, 0}, {nullptr, 0, 0, 0}}, 1};
+  for (int cc = 0; cc < 3; ++cc)
+    for (int j = 0; j < 3; ++j)
+      jobs[3 + 3 * cc + j] = SpecJob{{{u + cc * sb, 0.0, s, ks_of_dir[j]}, {nullptr, 0, 0, 0}}, 1};
+  void *outs[12];
+  for (int i = 0; i < 12; ++i) outs[i] = P + i * pb;
+  RET(c2r_jobs<T>(c, 12, jobs, outs, 1.0));
+  k_conv_prod<T><<<grid_for(np), 256, 0, c->stream>>>(reinterpret_cast<T *>(P), np, s);
+  CK(cudaGetLastError());
+  const void *ins[3] = {P + 12 * pb, P + 13 * pb, P + 14 * pb};
+  void *specs[3] = {S, S + sb, S + 2 * sb};
+  RET(r2c_fields<T>(c, 3, ins, specs));
+  k_adj_finish<C><<<gb, 256, 0, c->stream>>>(reinterpret_cast<const C *>(S), reinterpret_cast<const C *>(uh),
+                                             reinterpret_cast<C *>(rt), nh, gr, p.nu, p.Q, 1, p.hminone, 0);
+  CK(cudaGetLastError());
+  // stage 2: grad r~ (rhsAdj.f90:215-259), products, adjoint term
+  const char *r = reinterpret_cast<const char *>(rt);
+  SpecJob jobs2[9];
+  for (int cc = 0; cc < 3; ++cc)
+    for (int j = 0; j < 3; ++j)
+      jobs2[3 * cc + j] = SpecJob{{{r + cc * sb, 0.0, s, ks_of_dir[j]}, {nullptr, 0, 0, 0}}, 1};
+  RET(c2r_jobs<T>(c, 9, jobs2, outs + 3, 1.0));
+  k_adj_prod<T><<<grid_for(np), 256, 0, c->stream>>>(reinterpret_cast<T *>(P), np, s);
+  CK(cudaGetLastError());
+  RET(r2c_fields<T>(c, 3, ins, specs));
+  k_adj_finish<C><<<gb, 256, 0, c->stream>>>(reinterpret_cast<const C *>(S), reinterpret_cast<const C *>(rt),
+                                             reinterpret_cast<C *>(rhsadj), nh, gr, p.nu, p.Q, 2, p.hminone,
+                                             p.adj_phat == DNSBOX_ADJ_PHAT_LITERAL);
+  CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+// J (and, when grad != null, its Euclidean gradient) at uh.  Uses arena
+// spectral slots 6-8 for N and 9-11 for gE (slots 0-5 belong to the VJP).
+template <typename T>
+int residual_impl(dnsbox_ctx *c, const void *uh, void *grad, double *J) {
+  using C = typename CT<T>::type;
+  const dnsbox_params &p = c->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  const size_t sb = c->nh * sizeof(C);
+  char *P = nullptr, *S = nullptr;
+  RET(ensure_adj(c, 9, 12, &P, &S));
+  char *Nb = S + 6 * sb, *gE = S + 9 * sb;
+  {
+    const int rc = dnsbox_rhs_nonlinear(c, uh, Nb, nullptr);
+    if (rc != DNSBOX_OK) return rc;
+  }
+  RET(ensure_red(c, kRedBlocks + 1));
+  const Grid3 gr = grid3(c);
+  k_residual<C><<<kRedBlocks, 256, 0, c->stream>>>(
+      reinterpret_cast<const C *>(uh), reinterpret_cast<const C *>(Nb), grad ? reinterpret_cast<C *>(gE) : nullptr,
+      (long long)c->nh, gr, p.nu, p.Q, p.hminone, s * s, c->red);
+  CK(cudaGetLastError());
+  RET(sum_to_host(c, kRedBlocks, J));
+  if (grad) {
+    RET(vjp_impl<T>(c, uh, gE, grad));
+    k_add_linear<C><<<grid_for((long long)c->nh), 256, 0, c->stream>>>(
+        reinterpret_cast<C *>(grad), reinterpret_cast<const C *>(gE), (long long)c->nh, gr, p.nu, p.Q);
+    CK(cudaGetLastError());
+  }
+  return DNSBOX_OK;
+}
+
+template <typename T>
+int descent_impl(dnsbox_ctx *c, void *uh, int niter, double *Jhist, double *alpha_io) {
+  using C = typename CT<T>::type;
+  const size_t sb = c->nh * sizeof(C);
+  char *P = nullptr, *S = nullptr;
+  RET(ensure_adj(c, 9, 21, &P, &S));
+  char *grad = S + 12 * sb, *dir = S + 15 * sb, *trial = S + 18 * sb;
+  const Grid3 gr = grid3(c);
+  const long long n3 = 3 * (long long)c->nh;
+  double alpha = (alpha_io && *alpha_io > 0) ? *alpha_io : 1.0;
+  double J = 0.0;
+  RET(residual_impl<T>(c, uh, grad, &J));
+  if (Jhist) Jhist[0] = J;
+  for (int it = 0; it < niter; ++it) {
+    RET(ensure_red(c, kRedBlocks + 1));
+    const double s = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz);
+    k_descent_dir<C><<<kRedBlocks, 256, 0, c->stream>>>(reinterpret_cast<const C *>(grad), reinterpret_cast<C *>(dir),
+                                                        (long long)c->nh, gr, s * s, c->red);
+    CK(cudaGetLastError());
+    double slope;
+    RET(sum_to_host(c, kRedBlocks, &slope));   // <grad, d> < 0
+    if (!(slope < 0.0)) break;                    // stationary (or non-finite)
+    // Armijo backtracking in FP64: J(u + a d) <= J + 1e-4 a <grad, d>
+    double Jt = 0.0;
+    int tries = 0;
+    for (;;) {
+      k_axpy<C><<<grid_for(n3), 256, 0, c->stream>>>(reinterpret_cast<const C *>(uh), reinterpret_cast<const C *>(dir),
+                                                     reinterpret_cast<C *>(trial), n3, alpha);
+      CK(cudaGetLastError());
+      RET(residual_impl<T>(c, trial, nullptr, &Jt));
+      if ((isfinite(Jt) && Jt <= J + 1e-4 * alpha * slope) || ++tries >= 30) break;
+      alpha *= 0.5;
+    }
+    if (!(isfinite(Jt) && Jt <= J)) break;
+    CK(cudaMemcpyAsync(uh, trial, 3 * sb, cudaMemcpyDeviceToDevice, c->stream));
+    RET(residual_impl<T>(c, uh, grad, &J));
+    if (Jhist) Jhist[it + 1] = J;
+    if (tries == 0) alpha *= 2.0;
+  }
+  if (alpha_io) *alpha_io = alpha;
+  return DNSBOX_OK;
+}
+
+}  // namespace
+
+extern "C" int dnsbox_rhs_nonlinear_vjp(dnsbox_ctx *ctx, const void *uh, const void *g, void *out) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!uh || !g || !out) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  if (out == uh || out == g) return set_err(DNSBOX_ERR_ARG, "output may not alias an input");
+  return ctx->fp64 ? vjp_impl<double>(ctx, uh, g, out) : vjp_impl<float>(ctx, uh, g, out);
+}
+
+extern "C" int dnsbox_rhs_adj(dnsbox_ctx *ctx, const void *uh, void *rt, void *rhsadj) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!uh || !rt || !rhsadj) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  if (rt == uh || rhsadj == uh || rt == rhsadj) return set_err(DNSBOX_ERR_ARG, "outputs may not alias");
+  return ctx->fp64 ? rhs_adj_impl<double>(ctx, uh, rt, rhsadj) : rhs_adj_impl<float>(ctx, uh, rt, rhsadj);
+}
+
+extern "C" int dnsbox_residual(dnsbox_ctx *ctx, const void *uh, double *J) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!uh || !J) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  return ctx->fp64 ? residual_impl<double>(ctx, uh, nullptr, J) : residual_impl<float>(ctx, uh, nullptr, J);
+}
+
+extern "C" int dnsbox_residual_grad(dnsbox_ctx *ctx, const void *uh, void *grad, double *J) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!uh || !grad || !J) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  if (grad == uh) return set_err(DNSBOX_ERR_ARG, "output may not alias the input");
+  return ctx->fp64 ? residual_impl<double>(ctx, uh, grad, J) : residual_impl<float>(ctx, uh, grad, J);
+}
+
+extern "C" int dnsbox_adjoint_descent(dnsbox_ctx *ctx, void *uh, int niter, double *Jhist, double *alpha) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!uh || niter < 0) return set_err(DNSBOX_ERR_ARG, "invalid argument");
+  return ctx->fp64 ? descent_impl<double>(ctx, uh, niter, Jhist, alpha)
+                   : descent_impl<float>(ctx, uh, niter, Jhist, alpha);
+}

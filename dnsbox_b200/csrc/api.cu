@@ -59,31 +59,6 @@ extern "C" void dnsbox_default_params(dnsbox_params *p) {
 }
 
 // ------------------------------------------------------------ small kernels
-template <typename C>
-__global__ void k_eband(const C *u, long long nh, const int *band, int nband, int nx, StepState *st,
-                        double s2, int reset_umax) {
-  __shared__ double red[32];
-  double acc = 0.0;
-  // band[] holds (offset, kx) pairs flattened as ints: off_lo, off_hi, kx
-  for (int i = threadIdx.x; i < nband; i += blockDim.x) {
-    const long long off = (long long)(unsigned)band[3 * i] | ((long long)band[3 * i + 1] << 32);
-    const int kx = band[3 * i + 2];
-    const double w = (k_half(kx, nx, 1.0) == 0.0) ? 0.5 : 1.0;   // rhs.f90:151-155
-    double e = 0.0;
-    for (int c = 0; c < 3; ++c) {
-      const C v = u[c * nh + off];
-      e += ((double)v.x * v.x + (double)v.y * v.y) * w;
-    }
-    acc += e;
-  }
-  double v[1] = {acc};
-  block_sum<1>(v, red);
-  if (threadIdx.x == 0) {
-    st->eband = v[0] * s2;
-    if (reset_umax) st->umax[0] = st->umax[1] = st->umax[2] = 0.0;
-  }
-}
-
 // io_Courant (io.f90:664-676) on the fused max|u_i| and, when control is on,
 // set_time_step (dnsboxheun.f90:153-157, 227-246).
 __global__ void k_cfl(StepState *st, double dx, double dy, double dz, int control, int force,
@@ -455,6 +430,7 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   e.out = reinterpret_cast<C *>(out);
   e.state = reinterpret_cast<C *>(state);
   e.nold = reinterpret_cast<C *>(nold);
+  e.force = reinterpret_cast<const C *>(c->force);
   e.partials = partials ? c->partials : nullptr;
   e.mode = mode;
   const int ztc = Ops<T>::zfinish_cols(p.nz);
@@ -530,6 +506,7 @@ static void free_ctx(dnsbox_ctx *c) {
   cudaFree(c->red);
   cudaFree(c->band);
   cudaFree(c->ddiag);
+  cudaFree(c->adj);
   if (c->hstage) cudaFreeHost(c->hstage);
   delete c;
 }
@@ -1014,15 +991,6 @@ extern "C" int dnsbox_download_physical(dnsbox_ctx *ctx, const void *uh, double 
   return DNSBOX_OK;
 }
 
-extern "C" int dnsbox_rhs_adj(dnsbox_ctx *ctx, const void *, void *, void *) {
-  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
-  return set_err(DNSBOX_ERR_UNSUPPORTED, "rhs_adj not built yet");
-}
-
-extern "C" int dnsbox_rhs_nonlinear_vjp(dnsbox_ctx *ctx, const void *, const void *, void *) {
-  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
-  return set_err(DNSBOX_ERR_UNSUPPORTED, "rhs_nonlinear_vjp not built yet");
-}
 
 extern "C" int dnsbox_profile_enable(dnsbox_ctx *ctx, int on) {
   if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
@@ -1047,5 +1015,11 @@ extern "C" int dnsbox_profile_read(dnsbox_ctx *ctx, dnsbox_profile *out, int res
     for (int k = 0; k < DNSBOX_NPASS; ++k) ctx->launches[k] = 0;
     ctx->total_launches = 0;
   }
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_set_forcing(dnsbox_ctx *ctx, const void *f3_dev) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  ctx->force = f3_dev;
   return DNSBOX_OK;
 }

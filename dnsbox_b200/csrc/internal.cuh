@@ -58,6 +58,9 @@ struct dnsbox_ctx {
   int nspec = 0;
   int ab2_started = 0;
   int cfl_first = 1;                     // reference calls set_time_step before the loop
+  const void *force = nullptr;           // fixed spectral forcing (3 fields) or null
+  char *adj = nullptr;                   // adjoint arena
+  size_t adj_bytes = 0;
   // measurement
   int prof_on = 0;
   std::vector<cudaEvent_t> ev_pool;      // pairs
@@ -93,6 +96,44 @@ struct Prof {
     if (slot != (size_t)-1) cudaEventRecord(c->ev_pool[2 * slot + 1], c->stream);
   }
 };
+
+// ------------------------------------------------------------ shared kernels
+// rhs_Eband (rhs.f90:137-168) over the precomputed band-mode list, stored as
+// (offset lo, offset hi, kx) triples; optionally resets the CFL maxima.
+template <typename C>
+__global__ void k_eband(const C *u, long long nh, const int *band, int nband, int nx, StepState *st, double s2,
+                        int reset_umax) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nband; i += blockDim.x) {
+    const long long off = (long long)(unsigned)band[3 * i] | ((long long)band[3 * i + 1] << 32);
+    const int kx = band[3 * i + 2];
+    const double w = (k_half(kx, nx, 1.0) == 0.0) ? 0.5 : 1.0;   // rhs.f90:151-155
+    double e = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      const C v = u[c * nh + off];
+      e += ((double)v.x * v.x + (double)v.y * v.y) * w;
+    }
+    acc += e;
+  }
+  double v[1] = {acc};
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) {
+    st->eband = v[0] * s2;
+    if (reset_umax) st->umax[0] = st->umax[1] = st->umax[2] = 0.0;
+  }
+}
+
+// Sum of n doubles in a fixed order (one block).
+template <int NTH>
+__global__ void k_sum_scalar(const double *x, int n, double *out) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += NTH) acc += x[i];
+  double v[1] = {acc};
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) *out = v[0];
+}
 
 // ------------------------------------------------------------- dispatch
 template <typename T> struct Ops {
@@ -171,11 +212,13 @@ template <typename T> static StridedArgs<T> strided_base(const dnsbox_ctx *c, in
   a.ncols = c->nxh;
   a.nx = c->p.nx;
   a.alpha_x = c->p.alpha_x;
-  if (axis == 2) {  // z: rows kz/z, tiles over y
+  if (axis == 2) {  // z: rows kz/z, tiles over y (ky while y is spectral)
     a.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[2]);
     a.rowstride = (long long)c->p.ny * c->nxh;
     a.otherstride = c->nxh;
     a.alpha_row = c->p.alpha_z;
+    a.n_other = c->p.ny;
+    a.alpha_other = c->p.alpha_y;
   } else {          // y: rows ky/y, tiles over z
     a.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[1]);
     a.rowstride = c->nxh;
@@ -211,58 +254,91 @@ static int run_strided(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<T> &
   return DNSBOX_OK;
 }
 
-// 3D C2R of nf spectral fields (in[] -> out[] physical), through W1/W2.
-// Inputs must not live in W1 slots [0, nf) or W2 slots [0, nf).
+// One output of a batched C2R: sum over terms of in * (a + i b k), with k
+// the kx (ks 0), kz (ks 1) or ky (ks 2) wavenumber of the mode, applied in
+// the first (z) pass while all three axes are spectral.
+struct SpecTerm {
+  const void *in;
+  double a, b;
+  int ks;
+};
+struct SpecJob {
+  SpecTerm t[2];
+  int nt;
+};
+
+// 3D C2R of nf outputs described by jobs, through W1/W2 in chunks of 6.
+// Inputs must not live in W1 or W2 slots [0, 6).
 template <typename T>
-static int c2r_fields(dnsbox_ctx *c, int nf, const void *const *in, void *const *out, double scale) {
-  StridedArgs<T> a = strided_base<T>(c, 2);
-  a.njobs = nf;
-  for (int f = 0; f < nf; ++f) set_job<T>(a, f, in[f], field(c->W1, c, f));
-  RET(run_strided<T>(c, 2, true, a));
-  StridedArgs<T> b = strided_base<T>(c, 1);
-  b.njobs = nf;
-  for (int f = 0; f < nf; ++f) set_job<T>(b, f, field(c->W1, c, f), field(c->W2, c, f));
-  RET(run_strided<T>(c, 1, true, b));
-  XlineArgs<T> x;
-  memset(&x, 0, sizeof(x));
-  for (int f = 0; f < nf; ++f) {
-    x.in[f] = field(c->W2, c, f);
-    x.out[f] = out[f];
+static int c2r_jobs(dnsbox_ctx *c, int nf, const SpecJob *jobs, void *const *out, double scale) {
+  for (int f0 = 0; f0 < nf; f0 += 6) {
+    const int m = nf - f0 < 6 ? nf - f0 : 6;
+    StridedArgs<T> a = strided_base<T>(c, 2);
+    a.njobs = m;
+    for (int j = 0; j < m; ++j) {
+      const SpecJob &J = jobs[f0 + j];
+      set_job<T>(a, j, J.t[0].in, field(c->W1, c, j), J.t[0].a, J.t[0].b, J.t[0].ks,
+                 J.nt > 1 ? J.t[1].in : nullptr, J.nt > 1 ? J.t[1].a : 1.0, J.nt > 1 ? J.t[1].b : 0.0,
+                 J.nt > 1 ? J.t[1].ks : 0);
+    }
+    RET(run_strided<T>(c, 2, true, a));
+    StridedArgs<T> b = strided_base<T>(c, 1);
+    b.njobs = m;
+    for (int j = 0; j < m; ++j) set_job<T>(b, j, field(c->W1, c, j), field(c->W2, c, j));
+    RET(run_strided<T>(c, 1, true, b));
+    XlineArgs<T> x;
+    memset(&x, 0, sizeof(x));
+    for (int j = 0; j < m; ++j) {
+      x.in[j] = field(c->W2, c, j);
+      x.out[j] = out[f0 + j];
+    }
+    x.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[0]);
+    x.nlines = c->p.ny * c->p.nz;
+    x.nxh = c->nxh;
+    x.scale = scale;
+    Prof pr(c, DNSBOX_PASS_OTHER);
+    CK(Ops<T>::xline_c2r(c->p.nx, x, m, c->stream));
   }
-  x.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[0]);
-  x.nlines = c->p.ny * c->p.nz;
-  x.nxh = c->nxh;
-  x.scale = scale;
-  Prof pr(c, DNSBOX_PASS_OTHER);
-  CK(Ops<T>::xline_c2r(c->p.nx, x, nf, c->stream));
   return DNSBOX_OK;
 }
 
-// 3D R2C of nf physical fields.  Inputs must not live in W1 slots [0, nf).
+// 3D C2R of nf spectral fields (in[] -> out[] physical).
+template <typename T>
+static int c2r_fields(dnsbox_ctx *c, int nf, const void *const *in, void *const *out, double scale) {
+  SpecJob jobs[16];
+  for (int f = 0; f < nf; ++f) jobs[f] = SpecJob{{{in[f], 1.0, 0.0, 0}, {nullptr, 0, 0, 0}}, 1};
+  return c2r_jobs<T>(c, nf, jobs, out, scale);
+}
+
+// 3D R2C of nf physical fields, chunks of 6.  Inputs must not live in W1
+// slots [0, 6).
 template <typename T>
 static int r2c_fields(dnsbox_ctx *c, int nf, const void *const *in, void *const *out) {
-  XlineArgs<T> x;
-  memset(&x, 0, sizeof(x));
-  for (int f = 0; f < nf; ++f) {
-    x.in[f] = in[f];
-    x.out[f] = field(c->W1, c, f);
+  for (int f0 = 0; f0 < nf; f0 += 6) {
+    const int m = nf - f0 < 6 ? nf - f0 : 6;
+    XlineArgs<T> x;
+    memset(&x, 0, sizeof(x));
+    for (int j = 0; j < m; ++j) {
+      x.in[j] = in[f0 + j];
+      x.out[j] = field(c->W1, c, j);
+    }
+    x.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[0]);
+    x.nlines = c->p.ny * c->p.nz;
+    x.nxh = c->nxh;
+    x.scale = 1.0;
+    {
+      Prof pr(c, DNSBOX_PASS_OTHER);
+      CK(Ops<T>::xline_r2c(c->p.nx, x, m, c->stream));
+    }
+    StridedArgs<T> b = strided_base<T>(c, 1);
+    b.njobs = m;
+    for (int j = 0; j < m; ++j) set_job<T>(b, j, field(c->W1, c, j), field(c->W2, c, j));
+    RET(run_strided<T>(c, 1, false, b));
+    StridedArgs<T> a = strided_base<T>(c, 2);
+    a.njobs = m;
+    for (int j = 0; j < m; ++j) set_job<T>(a, j, field(c->W2, c, j), out[f0 + j]);
+    RET(run_strided<T>(c, 2, false, a));
   }
-  x.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[0]);
-  x.nlines = c->p.ny * c->p.nz;
-  x.nxh = c->nxh;
-  x.scale = 1.0;
-  {
-    Prof pr(c, DNSBOX_PASS_OTHER);
-    CK(Ops<T>::xline_r2c(c->p.nx, x, nf, c->stream));
-  }
-  StridedArgs<T> b = strided_base<T>(c, 1);
-  b.njobs = nf;
-  for (int f = 0; f < nf; ++f) set_job<T>(b, f, field(c->W1, c, f), field(c->W2, c, f));
-  RET(run_strided<T>(c, 1, false, b));
-  StridedArgs<T> a = strided_base<T>(c, 2);
-  a.njobs = nf;
-  for (int f = 0; f < nf; ++f) set_job<T>(a, f, field(c->W2, c, f), out[f]);
-  RET(run_strided<T>(c, 2, false, a));
   return DNSBOX_OK;
 }
 

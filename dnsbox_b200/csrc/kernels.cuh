@@ -54,7 +54,7 @@ template <typename T> struct StridedJob {
   const C *in2;
   C *out;
   double a1, b1, a2, b2;   // multiplier a + i b k
-  int ks1, ks2;            // 0: kx of the column, 1: wavenumber of the row index
+  int ks1, ks2;            // k: 0 kx of the column, 1 the row index's, 2 the tile's other-axis index's
 };
 
 template <typename T> struct StridedArgs {
@@ -68,6 +68,9 @@ template <typename T> struct StridedArgs {
   long long rowstride;     // elements between consecutive rows of the axis
   long long otherstride;   // elements between consecutive tiles of the other axis
   double alpha_row, alpha_x;
+  int n_other;             // length of the other axis (for ks = 2)
+  int pad1;
+  double alpha_other;
 };
 
 template <typename T, typename C>
@@ -104,19 +107,22 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
     const C *in1 = J.in1 + base;
 #pragma unroll
     for (int i = 0; i < E; ++i) v[i] = in1[(long long)EN::in_row(p, i) * a.rowstride];
+    // wavenumber of the column (0) or of the tile's other-axis index (2)
+    const double kcol = k_half(kx, a.nx, a.alpha_x);
+    const double koth = a.n_other ? k_full(other, a.n_other, a.alpha_other) : 0.0;
     if (!(J.a1 == 1.0 && J.b1 == 0.0)) {
-      const double kc = k_half(kx, a.nx, a.alpha_x);
+      const double kc = J.ks1 == 2 ? koth : kcol;
 #pragma unroll
       for (int i = 0; i < E; ++i)
-        v[i] = apply_mult<T>(v[i], J.a1, J.b1, J.ks1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc);
+        v[i] = apply_mult<T>(v[i], J.a1, J.b1, J.ks1 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc);
     }
     if (J.in2) {
       const C *in2 = J.in2 + base;
-      const double kc = k_half(kx, a.nx, a.alpha_x);
+      const double kc = J.ks2 == 2 ? koth : kcol;
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const C w = in2[(long long)EN::in_row(p, i) * a.rowstride];
-        v[i] = cadd(v[i], apply_mult<T>(w, J.a2, J.b2, J.ks2 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc));
+        v[i] = cadd(v[i], apply_mult<T>(w, J.a2, J.b2, J.ks2 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc));
       }
     }
   } else {
@@ -423,6 +429,7 @@ template <typename T> struct FinishArgs {
   C *out;                  // FIN_RHS / FIN_PRED output (3 fields)
   C *state;                // FIN_CORR state (3 fields)
   C *nold;                 // AB2 history (3 fields)
+  const C *force;          // fixed spectral forcing added to N (3 fields) or null
   const StepState *st;
   double *partials;        // per-CTA (E, D) of the new state, or null
   const C *tw;
@@ -536,6 +543,11 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
             if (forced) {
               re += fc * (double)uu[h][c].x;
               im += fc * (double)uu[h][c].y;
+            }
+            if (a.force) {
+              const C q = a.force[c * a.nh + (long long)kz * rowstride + base];
+              re += (double)q.x;
+              im += (double)q.y;
             }
             Nc[c] = mkc<C>(T(re), T(im));
           }

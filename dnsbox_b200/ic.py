@@ -104,3 +104,13 @@ def beltrami(n: int, nu: float, t: float = 0.0, alpha=(1.0, 1.0, 1.0)) -> np.nda
 def to_spectral(u: np.ndarray) -> np.ndarray:
     """Unnormalised R2C of a physical vector field (3, nz, ny, nx)."""
     return sfft.rfftn(u, axes=(-3, -2, -1), workers=_workers())
+
+
+def kolmogorov_forcing(n: int, amplitude: float = 1.0, kf: int = 4) -> np.ndarray:
+    """Spectral Kolmogorov forcing f = (F sin(kf y), 0, 0) on the reference grid
+    (unnormalised R2C, (3, n, n, n//2+1)); nonzero only at (kx, ky, kz) = (0, +-kf, 0)."""
+    L = 2 * np.pi
+    y = np.array([i * L / n for i in range(-n // 2, n // 2)])
+    f = np.zeros((3, n, n, n))
+    f[0] = amplitude * np.sin(kf * y)[None, :, None]
+    return to_spectral(f)

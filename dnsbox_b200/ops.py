@@ -217,6 +217,58 @@ class Box:
         _lib.check(self._lib.dnsbox_courant(self._h, _ptr(uh), float(dt), ctypes.byref(c), m))
         return c.value, tuple(m)
 
+    # ---------------------------------------------------------------- adjoint
+    def set_forcing(self, f: torch.Tensor | None):
+        """Fixed spectral forcing added to the nonlinear term (None clears).
+        The Box keeps a reference so the memory stays valid."""
+        if f is not None:
+            self._check_state(f, "forcing")
+        self._force = f
+        _lib.check(self._lib.dnsbox_set_forcing(self._h, _ptr(f) if f is not None else None))
+
+    def rhs_adj(self, uh):
+        """rhsAdj (rhsAdj.f90:356-381): returns (r~, rhsadj)."""
+        self._check_state(uh)
+        rt, out = torch.empty_like(uh), torch.empty_like(uh)
+        self._sync_stream()
+        _lib.check(self._lib.dnsbox_rhs_adj(self._h, _ptr(uh), _ptr(rt), _ptr(out)))
+        return rt, out
+
+    def rhs_nonlinear_vjp(self, uh, g):
+        """Exact transpose of the linearised rhs_nonlinear at uh applied to g."""
+        self._check_state(uh)
+        g = g.contiguous()
+        self._check_state(g, "g")
+        out = torch.empty_like(uh)
+        self._sync_stream()
+        _lib.check(self._lib.dnsbox_rhs_nonlinear_vjp(self._h, _ptr(uh), _ptr(g), _ptr(out)))
+        return out
+
+    def residual(self, uh) -> float:
+        self._check_state(uh)
+        self._sync_stream()
+        v = ctypes.c_double()
+        _lib.check(self._lib.dnsbox_residual(self._h, _ptr(uh), ctypes.byref(v)))
+        return v.value
+
+    def residual_grad(self, uh):
+        self._check_state(uh)
+        grad = torch.empty_like(uh)
+        self._sync_stream()
+        v = ctypes.c_double()
+        _lib.check(self._lib.dnsbox_residual_grad(self._h, _ptr(uh), _ptr(grad), ctypes.byref(v)))
+        return v.value, grad
+
+    def adjoint_descent(self, uh, niter, alpha=1.0):
+        """niter descent iterations on J in place; returns (J history, step length)."""
+        self._check_state(uh)
+        self._sync_stream()
+        hist = np.full(niter + 1, np.nan)
+        a = ctypes.c_double(alpha)
+        _lib.check(self._lib.dnsbox_adjoint_descent(self._h, _ptr(uh), int(niter),
+                                                    hist.ctypes.data_as(_lib._DP), ctypes.byref(a)))
+        return hist, a.value
+
     # ---------------------------------------------------------------- transforms
     def c2r(self, spec: torch.Tensor) -> torch.Tensor:
         """Unnormalised 3D C2R of one spectral field (nz, ny, nxh)."""

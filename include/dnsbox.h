@@ -180,12 +180,30 @@ int dnsbox_download_physical(dnsbox_ctx *ctx, const void *uhat3_dev, double *u3_
 /* rhsAdj, rhsAdj.f90:356-381: r~ (rhsupptilde, :177-213) and rhsadj. */
 int dnsbox_rhs_adj(dnsbox_ctx *ctx, const void *uhat3_dev, void *rtilde3_dev,
                    void *rhsadj3_dev);
+/* Fixed spectral forcing f (3 fields, kept by the caller; NULL clears) added to
+ * the nonlinear term of rhs_nonlinear and of every step.  No reference
+ * counterpart (the reference forces only through Q and the band term); used for
+ * the Kolmogorov flow f = (F sin(4y), 0, 0). */
+int dnsbox_set_forcing(dnsbox_ctx *ctx, const void *f3_dev);
 /* Exact transpose of the linearised rhs_nonlinear at uhat, applied to g
  * (Euclidean inner product on the Re/Im parts of the half spectrum).  No
  * reference counterpart: the reference's rhsNonlinearAdj (rhsAdj.f90:261-354)
  * is its continuous-adjoint analogue. */
 int dnsbox_rhs_nonlinear_vjp(dnsbox_ctx *ctx, const void *uhat3_dev, const void *g3_dev,
                              void *out3_dev);
+/* J(u) = 1/2 <r, H^-1 r> with r = (nu k.k + Q) uhat + N(uhat) (+ forcing), the
+ * residual of rhsupptilde (rhsAdj.f90:177-213) in the physical L2 norm
+ * (H^-1 = 1/(1+|k|^2) when hminone, else 1), accumulated in FP64. */
+int dnsbox_residual(dnsbox_ctx *ctx, const void *uhat3_dev, double *J);
+/* J and its gradient (Euclidean on Re/Im of the half spectrum) through the
+ * exact adjoint; the reference's counterpart is the descent direction of
+ * dnsboxAdj.f90:76-117. */
+int dnsbox_residual_grad(dnsbox_ctx *ctx, const void *uhat3_dev, void *grad3_dev, double *J);
+/* niter steepest-descent iterations on J in place (direction -P D W^-1 grad,
+ * FP64 Armijo backtracking line search); replaces the pseudo-time Heun loop of
+ * dnsboxAdj.f90:76-199.  J_host (niter+1 values) and alpha_io (initial/final
+ * step length) may be NULL. */
+int dnsbox_adjoint_descent(dnsbox_ctx *ctx, void *uhat3_dev, int niter, double *J_host, double *alpha_io);
 
 /* ---- measurement ------------------------------------------------------------
  * No reference counterpart (the reference times nothing; Makefile:3 passes
