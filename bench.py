@@ -217,6 +217,45 @@ def profile_passes(box, u, k):
     return pr
 
 
+def extra_sizes(args):
+    """Steps/s of the same forced workload at 512^3 (FP64 and FP32), seeded on
+    the device, K/2 steps after W warm-up steps each."""
+    from dnsbox_b200 import ic
+    out = {}
+    for prec in ("fp64", "fp32"):
+        box = make_box(512, prec, 0)
+        u = ic.random_field_gpu(box, seed=0, k0=WORKLOAD["k0"])
+        box.step(u, args.warmup, diag=False)
+        k = max(2, args.steps // 2)
+        ms = timed_steps(box, u, k, False)
+        out[f"{prec}_512"] = {"value": k / (ms / 1e3), "ms_per_step": ms / k, "steps": k}
+        box.close()
+        del u
+        torch.cuda.empty_cache()
+    return out
+
+
+def adjoint_rate(iters=40):
+    """Adjoint-descent iterations/s on the 64^3 Kolmogorov residual (FP32 bulk,
+    FP64 J and line search, nu = 1/40, F = 1, kf = 4)."""
+    from dnsbox_b200 import ic
+    from dnsbox_b200.ops import Box
+    box = Box(64, precision="fp32", nu=1.0 / 40.0, bandlim=False, hminone=True, tstep_fix=True, dt=5e-3)
+    f = box.from_numpy(ic.kolmogorov_forcing(64, 1.0, 4))
+    box.set_forcing(f)
+    u = box.from_numpy(ic.random_field(64, seed=0, k0=4.0))
+    box.step(u, 200, diag=False)          # leave the initial transient
+    hist, alpha = box.adjoint_descent(u, 5, alpha=1.0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist, alpha = box.adjoint_descent(u, iters, alpha=alpha)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    box.close()
+    return {"value": iters / el, "unit": "iterations/s", "n": 64, "iters": iters,
+            "J_first": float(hist[0]), "J_last": float(hist[np.isfinite(hist)][-1])}
+
+
 def read_traffic(prec, n):
     """DRAM bytes per launch from a committed ncu summary, if one exists."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
@@ -314,6 +353,9 @@ def run_ours(args, rank, world, dist_on):
         line.setdefault("variants", {})[prec] = {
             "value": world * args.steps / (rr["ms"] / 1e3), "ms_per_step": rr["ms"] / args.steps,
             "gpu_launches": rr["launches"], "clocks": rr["clocks"]}
+    if world == 1 and not args.no_extra:
+        line["extra"] = extra_sizes(args)
+        line["extra"]["adjoint_descent_64"] = adjoint_rate()
     if world == 1 and not args.no_cpu_baseline:
         from oracle import dnsbox_oracle as O
         rate, done, el = cpu_reference_rate(n, 3, budget_s=args.cpu_budget, warmup=0)
@@ -332,6 +374,7 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--precisions", default="fp64,fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the 512^3 and adjoint legs")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-budget", type=float, default=90.0)
     args = ap.parse_args()

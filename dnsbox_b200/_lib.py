@@ -93,6 +93,8 @@ SIGNATURES = {
     "dnsbox_r2c": (ctypes.c_int, [_VP, _VP, _VP]),
     "dnsbox_c2r": (ctypes.c_int, [_VP, _VP, _VP]),
     "dnsbox_c2r_noalloc": (ctypes.c_int, [ctypes.c_int] * 4 + [_VP, _VP, _VP]),
+    "dnsbox_state_alloc": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+    "dnsbox_state_free": (ctypes.c_int, [_VP, _VP]),
     "dnsbox_upload_state": (ctypes.c_int, [_VP, _VP, _VP]),
     "dnsbox_download_state": (ctypes.c_int, [_VP, _VP, _VP]),
     "dnsbox_upload_physical": (ctypes.c_int, [_VP, _VP, _VP]),

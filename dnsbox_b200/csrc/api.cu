@@ -1023,3 +1023,19 @@ extern "C" int dnsbox_set_forcing(dnsbox_ctx *ctx, const void *f3_dev) {
   ctx->force = f3_dev;
   return DNSBOX_OK;
 }
+
+extern "C" int dnsbox_state_alloc(dnsbox_ctx *ctx, void **out) {
+  BEGIN(ctx);
+  if (!out) return set_err(DNSBOX_ERR_ARG, "null output");
+  *out = nullptr;
+  CK(cudaMalloc(out, 3 * ctx->nh * ctx->cbytes));
+  CK(cudaMemset(*out, 0, 3 * ctx->nh * ctx->cbytes));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_state_free(dnsbox_ctx *ctx, void *p) {
+  BEGIN(ctx);
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaFree(p));
+  return DNSBOX_OK;
+}

@@ -114,3 +114,44 @@ def kolmogorov_forcing(n: int, amplitude: float = 1.0, kf: int = 4) -> np.ndarra
     f = np.zeros((3, n, n, n))
     f[0] = amplitude * np.sin(kf * y)[None, :, None]
     return to_spectral(f)
+
+
+def random_field_gpu(box, seed: int = 0, k0: float = 4.0, energy: float = 0.5):
+    """Device-side counterpart of ``random_field`` for large grids: white noise
+    from torch's counter-based generator on the device, the library's R2C,
+    Nyquist planes and mean mode zeroed, ``dealias`` + ``project`` and the same
+    shell rescale to A k^4 exp(-2 k^2/k0^2) with total energy ``energy``.
+    Returns a state tensor of the Box's precision (cubic grids)."""
+    import torch
+    n = box.nx
+    gen = torch.Generator(device=box.device).manual_seed(int(seed))
+    uh = box.zeros()
+    for c in range(3):
+        phys = torch.randn((n, n, n), generator=gen, device=box.device, dtype=box.rdtype)
+        uh[c] = box.r2c(phys)
+        del phys
+    uh[:, :, :, n // 2] = 0
+    uh[:, :, n // 2, :] = 0
+    uh[:, n // 2, :, :] = 0
+    uh[:, 0, 0, 0] = 0
+    box.dealias(uh)
+    box.project(uh)
+    kz, ky, kx = [torch.from_numpy(np.ascontiguousarray(k)).to(box.device) for k in broadcast_k(n, n, n)]
+    absk = torch.sqrt(kx * kx + ky * ky + kz * kz).expand(n, n, n // 2 + 1)
+    base = torch.floor(absk)
+    nk = torch.where(absk < base + 0.5, base, base + 1).to(torch.int64)
+    w = torch.ones(n // 2 + 1, dtype=torch.float64, device=box.device)
+    w[0] = 0.5
+    w[n // 2] = 0.5
+    s2 = (1.0 / float(n) ** 3) ** 2
+    e2 = (uh.abs().to(torch.float64) ** 2).sum(0) * w * s2
+    nmax = int(nk.max().item()) + 1
+    ecur = torch.bincount(nk.reshape(-1), weights=e2.reshape(-1), minlength=nmax)
+    shells = torch.arange(nmax, dtype=torch.float64, device=box.device)
+    etgt = shells ** 4 * torch.exp(-2.0 * shells ** 2 / (k0 * k0))
+    fac = torch.where((ecur > 0) & (shells > 0), torch.sqrt(etgt / torch.clamp(ecur, min=1e-300)),
+                      torch.zeros_like(ecur))
+    uh *= fac[nk].to(box.rdtype)
+    e = box.kinetic(uh)
+    uh *= float(np.sqrt(energy / e))
+    return uh

@@ -166,6 +166,12 @@ int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec_dev, void *phys_dev);
 int dnsbox_c2r_noalloc(int nx, int ny, int nz, int precision, const void *spec_dev, void *phys_dev,
                        void *cuda_stream);
 
+/* Device storage for one spectral state (3 fields) in the context's precision,
+ * for callers without a CUDA allocator of their own (the Fortran driver's
+ * uhat/vhat/what, variables.f90:193-213).  Freed with dnsbox_state_free. */
+int dnsbox_state_alloc(dnsbox_ctx *ctx, void **uhat3_dev);
+int dnsbox_state_free(dnsbox_ctx *ctx, void *uhat3_dev);
+
 /* ---- host <-> device state (replaces the module arrays uhat/vhat/what and
  *      u/v/w; io.f90:100-278 / 455-626 read and write the physical form) --- */
 /* complex(8) (kz, ky, kx), kz fastest, 3 components -> device state */
