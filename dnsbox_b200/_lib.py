@@ -32,7 +32,7 @@ class Params(ctypes.Structure):
         ("precision", ctypes.c_int32), ("stepper", ctypes.c_int32), ("ab2_mode", ctypes.c_int32),
         ("bandlim", ctypes.c_int32), ("spherical", ctypes.c_int32), ("tstep_fix", ctypes.c_int32),
         ("hminone", ctypes.c_int32), ("spectrum_mode", ctypes.c_int32), ("adj_phat", ctypes.c_int32),
-        ("device", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 3),
+        ("device", ctypes.c_int32), ("nbatch", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 2),
         ("alpha_x", ctypes.c_double), ("alpha_y", ctypes.c_double), ("alpha_z", ctypes.c_double),
         ("nu", ctypes.c_double), ("Q", ctypes.c_double), ("kCutOff", ctypes.c_double),
         ("Pin", ctypes.c_double), ("Deltak", ctypes.c_double),
@@ -105,6 +105,13 @@ SIGNATURES = {
     "dnsbox_residual": (ctypes.c_int, [_VP, _VP, _DP]),
     "dnsbox_residual_grad": (ctypes.c_int, [_VP, _VP, _VP, _DP]),
     "dnsbox_adjoint_descent": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _DP, _DP]),
+    "dnsbox_batch_size": (ctypes.c_int, [_VP]),
+    "dnsbox_set_batch_nu": (ctypes.c_int, [_VP, _DP]),
+    "dnsbox_diag_read": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(Diag)]),
+    "dnsbox_ensemble_create": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.c_int,
+                                              ctypes.POINTER(_VP)]),
+    "dnsbox_ensemble_run": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "dnsbox_ensemble_destroy": (ctypes.c_int, [_VP]),
     "dnsbox_profile_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dnsbox_profile_read": (ctypes.c_int, [_VP, ctypes.POINTER(Profile), ctypes.c_int]),
 }

@@ -61,9 +61,12 @@ extern "C" void dnsbox_default_params(dnsbox_params *p) {
 // ------------------------------------------------------------ small kernels
 // io_Courant (io.f90:664-676) on the fused max|u_i| and, when control is on,
 // set_time_step (dnsboxheun.f90:153-157, 227-246).
-__global__ void k_cfl(StepState *st, double dx, double dy, double dz, int control, int force,
-                      double cmin, double cmax, double dtmax, dnsbox_diag *drec) {
-  if (threadIdx.x != 0) return;
+__global__ void k_cfl(StepState *sts, int nbatch, double dx, double dy, double dz, int control, int force,
+                      double cmin, double cmax, double dtmax, dnsbox_diag *ring, int ring_cap) {
+  const int box = blockIdx.x * blockDim.x + threadIdx.x;
+  if (box >= nbatch) return;
+  StepState *st = sts + box;
+  dnsbox_diag *drec = ring ? ring + ((long long)st->step % ring_cap) * nbatch + box : nullptr;
   double dt = st->dt;
   double C = st->umax[0] * dt / dx + st->umax[1] * dt / dy + st->umax[2] * dt / dz;
   if (control && (force || C > cmax || (C < cmin && dt < dtmax))) {
@@ -87,9 +90,16 @@ __global__ void k_cfl(StepState *st, double dx, double dy, double dz, int contro
 
 // Sums the finish-kernel partials (fixed order), writes the step record and
 // advances the clock.
-__global__ void k_finalize(StepState *st, const double *partials, int np, double s2, double nu,
-                           double Q, double Pin, int bandlim, dnsbox_diag *drec) {
+// one block per box
+__global__ void k_finalize(StepState *sts, const double *partials, int np, double s2, double nu,
+                           const double *nu_box, double Q, double Pin, int bandlim, dnsbox_diag *ring,
+                           int ring_cap) {
   __shared__ double red[2 * 32];
+  const int box = blockIdx.x, nbatch = gridDim.x;
+  StepState *st = sts + box;
+  partials += 2 * (long long)box * np;
+  if (nu_box) nu = nu_box[box];
+  dnsbox_diag *drec = ring ? ring + ((long long)st->step % ring_cap) * nbatch + box : nullptr;
   double e = 0.0, d = 0.0;
   for (int i = threadIdx.x; i < np; i += blockDim.x) {
     e += partials[2 * i];
@@ -114,6 +124,17 @@ __global__ void k_finalize(StepState *st, const double *partials, int np, double
     st->t = st->t + dt;
     st->step += 1.0;
   }
+}
+
+__global__ void k_reset_umax(StepState *st, int nbatch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nbatch) st[b].umax[0] = st[b].umax[1] = st[b].umax[2] = 0.0;
+}
+
+// sets the double at byte offset `off` of every box's StepState
+__global__ void k_set_state(StepState *st, int nbatch, int off, double v) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nbatch) *reinterpret_cast<double *>(reinterpret_cast<char *>(st + b) + off) = v;
 }
 
 // Spectral diagnostics over the half spectrum: shell spectrum (state.f90:350-411
@@ -360,10 +381,11 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   // rhs_Eband (rhs.f90:22-24) and reset of the CFL maxima
   if (p.bandlim) {
     Prof pr(c, DNSBOX_PASS_SMALL);
-    k_eband<C><<<1, 256, 0, c->stream>>>(reinterpret_cast<const C *>(uin), (long long)c->nh, c->band,
-                                         c->nband, p.nx, c->st, s * s, 1);
+    k_eband<C><<<c->nbatch, 256, 0, c->stream>>>(reinterpret_cast<const C *>(uin), (long long)c->fstride, c->band,
+                                                 c->nband, p.nx, c->st, s * s, 1, (long long)c->nh);
   } else {
-    CK(cudaMemsetAsync(&c->st->umax[0], 0, 3 * sizeof(double), c->stream));
+    Prof pr(c, DNSBOX_PASS_SMALL);
+    k_reset_umax<<<(c->nbatch + 127) / 128, 128, 0, c->stream>>>(c->st, c->nbatch);
   }
   CK(cudaGetLastError());
   const char *u = reinterpret_cast<const char *>(uin);
@@ -400,8 +422,9 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   x.NY = reinterpret_cast<C *>(field(c->W1, c, 1));
   x.NZ = reinterpret_cast<C *>(field(c->W1, c, 2));
   x.tw = reinterpret_cast<const C *>(c->tw[0]);
-  x.umax = &c->st->umax[0];
-  x.nlines = p.ny * p.nz;
+  x.st = c->st;
+  x.lines_per_box = p.ny * p.nz;
+  x.nlines = c->nbatch * p.ny * p.nz;
   x.nxh = c->nxh;
   x.alpha_x = p.alpha_x;
   x.s = s;
@@ -413,8 +436,9 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
     const double dx = (2 * M_PI / p.alpha_x) / p.nx, dy = (2 * M_PI / p.alpha_y) / p.ny,
                  dz = (2 * M_PI / p.alpha_z) / p.nz;
     Prof pr(c, DNSBOX_PASS_SMALL);
-    k_cfl<<<1, 32, 0, c->stream>>>(c->st, dx, dy, dz, !p.tstep_fix, c->cfl_first, p.courant_min,
-                                   p.courant_max, p.dt_max, drec);
+    k_cfl<<<(c->nbatch + 127) / 128, 128, 0, c->stream>>>(c->st, c->nbatch, dx, dy, dz, !p.tstep_fix,
+                                                          c->cfl_first, p.courant_min, p.courant_max, p.dt_max,
+                                                          c->ddiag, c->ring_cap);
     CK(cudaGetLastError());
     c->cfl_first = 0;
   }
@@ -432,43 +456,71 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   e.nold = reinterpret_cast<C *>(nold);
   e.force = reinterpret_cast<const C *>(c->force);
   e.partials = partials ? c->partials : nullptr;
+  e.nu_box = c->d_nu;
+  e.nh = (long long)c->fstride;
+  e.bstride = (long long)c->nh;
   e.mode = mode;
   const int ztc = Ops<T>::zfinish_cols(p.nz);
   const int ntx = (c->nxh + ztc - 1) / ztc;
   Prof pr(c, DNSBOX_PASS_Z_FIN);
-  CK(Ops<T>::zfinish(p.nz, e, ntx * p.ny, c->stream));
+  CK(Ops<T>::zfinish(p.nz, e, ntx * p.ny, c->nbatch, c->stream));
+  return DNSBOX_OK;
+}
+
+// Copies the records of steps [first, first + n) (n <= ring_cap) from the
+// device ring into host[(step - first) * nbatch + box].
+static int ring_read(dnsbox_ctx *c, long long first, int n, dnsbox_diag *host) {
+  int done = 0;
+  while (done < n) {
+    const long long step = first + done;
+    const int pos = (int)(step % c->ring_cap);
+    int run = c->ring_cap - pos;
+    if (run > n - done) run = n - done;
+    CK(cudaMemcpyAsync(host + (size_t)done * c->nbatch, c->ddiag + (size_t)pos * c->nbatch,
+                       (size_t)run * c->nbatch * sizeof(dnsbox_diag), cudaMemcpyDeviceToHost, c->stream));
+    done += run;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return DNSBOX_OK;
+}
+
+// One step of every box of the context (no host synchronisation).
+template <typename T> static int step_once(dnsbox_ctx *c, void *uh) {
+  const dnsbox_params &p = c->p;
+  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
+  const bool pc = (p.stepper == DNSBOX_HEUN) || !c->ab2_started;
+  if (pc) {
+    // dnsboxheun.f90:85-126 (and dnsbox.f90:87-141 for the AB2 first step)
+    RET(run_rhs<T>(c, uh, FIN_PRED, c->ustar, nullptr, p.stepper == DNSBOX_AB2 ? c->nold : nullptr, false, 1,
+                   nullptr));
+    RET(run_rhs<T>(c, c->ustar, FIN_CORR, nullptr, uh, nullptr, true, 0, nullptr));
+    if (p.stepper == DNSBOX_AB2) c->ab2_started = 1;
+  } else {
+    // dnsbox.f90:143-191
+    RET(run_rhs<T>(c, uh, FIN_AB2, nullptr, uh, c->nold, true, 1, nullptr));
+  }
+  const int ztc = Ops<T>::zfinish_cols(p.nz);
+  const int ntx = (c->nxh + ztc - 1) / ztc;
+  Prof pr(c, DNSBOX_PASS_SMALL);
+  k_finalize<<<c->nbatch, 1024, 0, c->stream>>>(c->st, c->partials, ntx * p.ny, s * s, p.nu, c->d_nu, p.Q, p.Pin,
+                                                 p.bandlim, c->ddiag, c->ring_cap);
+  CK(cudaGetLastError());
+  c->host_step += 1;
   return DNSBOX_OK;
 }
 
 template <typename T> static int step_impl(dnsbox_ctx *c, void *uh, int nsteps, dnsbox_diag *dh) {
-  const dnsbox_params &p = c->p;
-  const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
-  if (dh) RET(ensure_diag(c, nsteps));
+  long long chunk_first = c->host_step;
   for (int n = 0; n < nsteps; ++n) {
-    dnsbox_diag *drec = dh ? c->ddiag + n : nullptr;
-    const bool pc = (p.stepper == DNSBOX_HEUN) || !c->ab2_started;
-    if (pc) {
-      // dnsboxheun.f90:85-126 (and dnsbox.f90:87-141 for the AB2 first step)
-      RET(run_rhs<T>(c, uh, FIN_PRED, c->ustar, nullptr, p.stepper == DNSBOX_AB2 ? c->nold : nullptr,
-                     false, 1, drec));
-      RET(run_rhs<T>(c, c->ustar, FIN_CORR, nullptr, uh, nullptr, true, 0, nullptr));
-      if (p.stepper == DNSBOX_AB2) c->ab2_started = 1;
-    } else {
-      // dnsbox.f90:143-191
-      RET(run_rhs<T>(c, uh, FIN_AB2, nullptr, uh, c->nold, true, 1, drec));
+    RET(step_once<T>(c, uh));
+    const int in_chunk = (int)(c->host_step - chunk_first);
+    if (dh && (in_chunk == c->ring_cap || n == nsteps - 1)) {
+      RET(ring_read(c, chunk_first, in_chunk, dh + (size_t)(n + 1 - in_chunk) * c->nbatch));
+      chunk_first = c->host_step;
     }
-    const int ztc = Ops<T>::zfinish_cols(p.nz);
-    const int ntx = (c->nxh + ztc - 1) / ztc;
-    Prof pr(c, DNSBOX_PASS_SMALL);
-    k_finalize<<<1, 1024, 0, c->stream>>>(c->st, c->partials, ntx * p.ny, s * s, p.nu, p.Q, p.Pin,
-                                          p.bandlim, drec);
-    CK(cudaGetLastError());
   }
   if (dh) {
-    CK(cudaMemcpyAsync(dh, c->ddiag, (size_t)nsteps * sizeof(dnsbox_diag), cudaMemcpyDeviceToHost,
-                       c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (int n = 0; n < nsteps; ++n)
+    for (int n = 0; n < nsteps * c->nbatch; ++n)
       if (dh[n].nonfinite) return set_err(DNSBOX_ERR_NONFINITE, "non-finite energy at step %d", dh[n].step);
   }
   return DNSBOX_OK;
@@ -507,6 +559,7 @@ static void free_ctx(dnsbox_ctx *c) {
   cudaFree(c->band);
   cudaFree(c->ddiag);
   cudaFree(c->adj);
+  cudaFree(c->d_nu);
   if (c->hstage) cudaFreeHost(c->hstage);
   delete c;
 }
@@ -524,25 +577,31 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
   if (p->stepper != DNSBOX_HEUN && p->stepper != DNSBOX_AB2)
     return set_err(DNSBOX_ERR_ARG, "invalid stepper %d", p->stepper);
   CK(cudaSetDevice(p->device));
+  if (p->nbatch < 0 || p->nbatch > 65535) return set_err(DNSBOX_ERR_ARG, "nbatch %d out of range", p->nbatch);
   dnsbox_ctx *c = new dnsbox_ctx();
   c->p = *p;
+  c->nbatch = p->nbatch > 1 ? p->nbatch : 1;
   c->fp64 = p->precision == DNSBOX_FP64;
   c->cbytes = c->fp64 ? 16 : 8;
   c->nxh = p->nx / 2 + 1;
   c->nh = (size_t)p->nz * p->ny * c->nxh;
   c->np = (size_t)p->nz * p->ny * p->nx;
+  c->fstride = c->nh * c->nbatch;
   int rc = DNSBOX_OK;
   auto fail = [&](int r) {
     free_ctx(c);
     return r;
   };
-  const size_t fb = c->nh * c->cbytes;
+  const size_t fb = c->fstride * c->cbytes;
+  c->ring_cap = 1024;
   cudaError_t e;
   if ((e = cudaMalloc(&c->W1, 6 * fb)) != cudaSuccess ||
       (e = cudaMalloc(&c->W2, 6 * fb)) != cudaSuccess ||
       (e = cudaMalloc(&c->ustar, 3 * fb)) != cudaSuccess ||
       (p->stepper == DNSBOX_AB2 && (e = cudaMalloc(&c->nold, 3 * fb)) != cudaSuccess) ||
-      (e = cudaMalloc(&c->st, sizeof(StepState))) != cudaSuccess) {
+      (e = cudaMalloc(&c->st, c->nbatch * sizeof(StepState))) != cudaSuccess ||
+      (e = cudaMalloc(&c->ddiag, (size_t)c->ring_cap * c->nbatch * sizeof(dnsbox_diag))) != cudaSuccess ||
+      (c->nbatch > 1 && (e = cudaMalloc(&c->d_nu, c->nbatch * sizeof(double))) != cudaSuccess)) {
     cudaGetLastError();
     return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed: %s", cudaGetErrorString(e)));
   }
@@ -553,7 +612,7 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
     const int ztc = c->fp64 ? Ops<double>::zfinish_cols(p->nz) : Ops<float>::zfinish_cols(p->nz);
     c->npartials = ((c->nxh + ztc - 1) / ztc) * p->ny;
   }
-  if ((e = cudaMalloc(&c->partials, 2 * (size_t)c->npartials * sizeof(double))) != cudaSuccess)
+  if ((e = cudaMalloc(&c->partials, 2 * (size_t)c->npartials * c->nbatch * sizeof(double))) != cudaSuccess)
     return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed"));
   // band modes |k| <= kCutOff (rhs.f90:145-149), stored as (offset lo, offset hi, kx)
   std::vector<int> band;
@@ -587,11 +646,18 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
         return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
     }
   }
-  StepState hs;
-  memset(&hs, 0, sizeof(hs));
-  hs.dt = p->dt;
-  if ((e = cudaMemcpy(c->st, &hs, sizeof(hs), cudaMemcpyHostToDevice)) != cudaSuccess)
-    return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
+  {
+    std::vector<StepState> hs(c->nbatch);
+    memset(hs.data(), 0, hs.size() * sizeof(StepState));
+    for (auto &x : hs) x.dt = p->dt;
+    if ((e = cudaMemcpy(c->st, hs.data(), hs.size() * sizeof(StepState), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
+    if (c->d_nu) {
+      std::vector<double> nus(c->nbatch, p->nu);
+      if ((e = cudaMemcpy(c->d_nu, nus.data(), nus.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
+    }
+  }
   if ((e = cudaMallocHost(&c->hstage, 64 * sizeof(double))) != cudaSuccess)
     return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
   // variables.f90:112-123
@@ -633,12 +699,17 @@ extern "C" int dnsbox_nspec(const dnsbox_ctx *ctx) { return ctx ? ctx->nspec : -
 #define BEGIN(ctx)                                              \
   if (!(ctx)) return set_err(DNSBOX_ERR_ARG, "null context");   \
   CK(cudaSetDevice((ctx)->p.device));
+// entry points that take one box's fields
+#define SINGLE(ctx)                                                                              \
+  if ((ctx)->nbatch > 1)                                                                         \
+    return set_err(DNSBOX_ERR_UNSUPPORTED, "not available on a batched context (nbatch = %d)", \
+                   (ctx)->nbatch);
 
 extern "C" int dnsbox_set_dt(dnsbox_ctx *ctx, double dt) {
   BEGIN(ctx);
   if (!(dt > 0.0) || !isfinite(dt)) return set_err(DNSBOX_ERR_ARG, "dt must be positive and finite");
-  ctx->hstage[0] = dt;
-  CK(cudaMemcpyAsync(&ctx->st->dt, ctx->hstage, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  k_set_state<<<(ctx->nbatch + 127) / 128, 128, 0, ctx->stream>>>(ctx->st, ctx->nbatch, offsetof(StepState, dt), dt);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   return DNSBOX_OK;
 }
@@ -654,9 +725,10 @@ extern "C" int dnsbox_get_dt(dnsbox_ctx *ctx, double *dt) {
 
 extern "C" int dnsbox_set_time(dnsbox_ctx *ctx, double t) {
   BEGIN(ctx);
-  ctx->hstage[0] = t;
-  ctx->hstage[1] = t;
-  CK(cudaMemcpyAsync(&ctx->st->t, ctx->hstage, 2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  k_set_state<<<(ctx->nbatch + 127) / 128, 128, 0, ctx->stream>>>(ctx->st, ctx->nbatch, offsetof(StepState, t), t);
+  k_set_state<<<(ctx->nbatch + 127) / 128, 128, 0, ctx->stream>>>(ctx->st, ctx->nbatch, offsetof(StepState, t_prev),
+                                                                   t);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   return DNSBOX_OK;
 }
@@ -701,6 +773,7 @@ extern "C" int dnsbox_step(dnsbox_ctx *ctx, void *uh, int nsteps, dnsbox_diag *d
 
 extern "C" int dnsbox_project(dnsbox_ctx *ctx, void *uh) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const dnsbox_params &p = ctx->p;
   const int g = grid_for((long long)ctx->nh);
@@ -716,6 +789,7 @@ extern "C" int dnsbox_project(dnsbox_ctx *ctx, void *uh) {
 
 extern "C" int dnsbox_dealias(dnsbox_ctx *ctx, void *uh) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const dnsbox_params &p = ctx->p;
   const int g = grid_for((long long)ctx->nh);
@@ -763,6 +837,7 @@ static int specdiag(dnsbox_ctx *ctx, const void *uh, int single, std::vector<dou
 extern "C" int dnsbox_spectrum(dnsbox_ctx *ctx, const void *uh, double *espec, double *ezero, double *eone,
                                double *esqrt2) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
   std::vector<double> v;
   RET(specdiag(ctx, uh, ctx->p.spectrum_mode == DNSBOX_SPECTRUM_SINGLE, v));
@@ -776,6 +851,7 @@ extern "C" int dnsbox_spectrum(dnsbox_ctx *ctx, const void *uh, double *espec, d
 
 extern "C" int dnsbox_kinetic(dnsbox_ctx *ctx, const void *uh, double *ekin) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!uh || !ekin) return set_err(DNSBOX_ERR_ARG, "null pointer");
   std::vector<double> v;
   RET(specdiag(ctx, uh, 0, v));
@@ -787,6 +863,7 @@ extern "C" int dnsbox_kinetic(dnsbox_ctx *ctx, const void *uh, double *ekin) {
 
 extern "C" int dnsbox_dissipation(dnsbox_ctx *ctx, const void *uh, double *disp) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!uh || !disp) return set_err(DNSBOX_ERR_ARG, "null pointer");
   std::vector<double> v;
   RET(specdiag(ctx, uh, 0, v));
@@ -798,6 +875,7 @@ extern "C" int dnsbox_dissipation(dnsbox_ctx *ctx, const void *uh, double *disp)
 
 extern "C" int dnsbox_eband(dnsbox_ctx *ctx, const void *uh, double *eband) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!uh || !eband) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const dnsbox_params &p = ctx->p;
   const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
@@ -851,6 +929,7 @@ static int reduce_max(dnsbox_ctx *ctx, const void *f, bool fp64, long long n, in
 
 extern "C" int dnsbox_courant(dnsbox_ctx *ctx, const void *uh, double dt, double *courant, double *umax3) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!uh || !courant) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const dnsbox_params &p = ctx->p;
   const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
@@ -868,6 +947,7 @@ extern "C" int dnsbox_courant(dnsbox_ctx *ctx, const void *uh, double dt, double
 
 extern "C" int dnsbox_divergence(dnsbox_ctx *ctx, const void *uh, double *divmax) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!uh || !divmax) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const dnsbox_params &p = ctx->p;
   const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
@@ -889,6 +969,7 @@ extern "C" int dnsbox_divergence(dnsbox_ctx *ctx, const void *uh, double *divmax
 
 extern "C" int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec, void *phys) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!spec || !phys) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const void *in[1] = {spec};
   void *out[1] = {phys};
@@ -897,6 +978,7 @@ extern "C" int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec, void *phys) {
 
 extern "C" int dnsbox_r2c(dnsbox_ctx *ctx, const void *phys, void *spec) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!spec || !phys) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const void *in[1] = {phys};
   void *out[1] = {spec};
@@ -905,6 +987,7 @@ extern "C" int dnsbox_r2c(dnsbox_ctx *ctx, const void *phys, void *spec) {
 
 extern "C" int dnsbox_upload_state(dnsbox_ctx *ctx, const double *host, void *uh) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!host || !uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const dnsbox_params &p = ctx->p;
   // 3 complex-double fields fit in W1 (6 fields of the context precision >= 3 x 16 B)
@@ -924,6 +1007,7 @@ extern "C" int dnsbox_upload_state(dnsbox_ctx *ctx, const double *host, void *uh
 
 extern "C" int dnsbox_download_state(dnsbox_ctx *ctx, const void *uh, double *host) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!host || !uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const dnsbox_params &p = ctx->p;
   dim3 grid((p.nz + 31) / 32, (ctx->nxh + 31) / 32, 3 * p.ny), blk(32, 8);
@@ -941,6 +1025,7 @@ extern "C" int dnsbox_download_state(dnsbox_ctx *ctx, const void *uh, double *ho
 
 extern "C" int dnsbox_upload_physical(dnsbox_ctx *ctx, const double *host, void *uh) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!host || !uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
   // host doubles -> W2 (3 physical double fields fit: 6 nh cbytes >= 3 np 8 for both precisions)
   const size_t pbytes = ctx->np * sizeof(double);
@@ -968,6 +1053,7 @@ extern "C" int dnsbox_upload_physical(dnsbox_ctx *ctx, const double *host, void 
 
 extern "C" int dnsbox_download_physical(dnsbox_ctx *ctx, const void *uh, double *host) {
   BEGIN(ctx);
+  SINGLE(ctx);
   if (!host || !uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
   const dnsbox_params &p = ctx->p;
   const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
@@ -1037,5 +1123,131 @@ extern "C" int dnsbox_state_free(dnsbox_ctx *ctx, void *p) {
   BEGIN(ctx);
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaFree(p));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_set_batch_nu(dnsbox_ctx *ctx, const double *nu_host) {
+  BEGIN(ctx);
+  if (!nu_host) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  for (int b = 0; b < ctx->nbatch; ++b)
+    if (!(nu_host[b] >= 0.0)) return set_err(DNSBOX_ERR_ARG, "invalid viscosity for box %d", b);
+  if (ctx->nbatch == 1) {
+    ctx->p.nu = nu_host[0];
+    return DNSBOX_OK;
+  }
+  CK(cudaMemcpy(ctx->d_nu, nu_host, ctx->nbatch * sizeof(double), cudaMemcpyHostToDevice));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_diag_read(dnsbox_ctx *ctx, int nrecent, dnsbox_diag *host) {
+  BEGIN(ctx);
+  if (!host || nrecent < 0) return set_err(DNSBOX_ERR_ARG, "invalid argument");
+  if (nrecent > ctx->ring_cap || nrecent > ctx->host_step)
+    return set_err(DNSBOX_ERR_ARG, "only the last %d steps are kept (%lld issued)", ctx->ring_cap,
+                   (long long)ctx->host_step);
+  return ring_read(ctx, ctx->host_step - nrecent, nrecent, host);
+}
+
+extern "C" int dnsbox_batch_size(const dnsbox_ctx *ctx) { return ctx ? ctx->nbatch : -1; }
+
+// ------------------------------------------------------------------ ensemble
+// The graph is captured and replayed on a private stream (the legacy default
+// stream cannot be captured); events order it after the contexts' stream on
+// entry and make that stream wait for it on exit.
+struct dnsbox_ensemble {
+  std::vector<dnsbox_ctx *> ctxs;
+  std::vector<void *> states;
+  cudaStream_t user = 0, own = nullptr;
+  cudaEvent_t in = nullptr, out = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static int step_any(dnsbox_ctx *c, void *u) {
+  return c->fp64 ? step_once<double>(c, u) : step_once<float>(c, u);
+}
+
+static void ensemble_free(dnsbox_ensemble *e) {
+  if (!e) return;
+  if (e->own) cudaStreamSynchronize(e->own);
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  if (e->in) cudaEventDestroy(e->in);
+  if (e->out) cudaEventDestroy(e->out);
+  if (e->own) cudaStreamDestroy(e->own);
+  for (auto *c : e->ctxs) c->stream = e->user;
+  delete e;
+}
+
+extern "C" int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *states, int n, dnsbox_ensemble **out) {
+  if (!ctxs || !states || !out || n <= 0) return set_err(DNSBOX_ERR_ARG, "invalid argument");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i] || !states[i]) return set_err(DNSBOX_ERR_ARG, "null context or state %d", i);
+    if (ctxs[i]->p.device != ctxs[0]->p.device) return set_err(DNSBOX_ERR_ARG, "contexts on different devices");
+    if (ctxs[i]->prof_on) return set_err(DNSBOX_ERR_STATE, "profiling must be off while capturing");
+  }
+  CK(cudaSetDevice(ctxs[0]->p.device));
+  dnsbox_ensemble *e = new dnsbox_ensemble();
+  e->ctxs.assign(ctxs, ctxs + n);
+  e->states.assign(states, states + n);
+  e->user = ctxs[0]->stream;
+  auto fail = [&](cudaError_t err, const char *what) {
+    ensemble_free(e);
+    return set_err(DNSBOX_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
+  };
+  cudaError_t err;
+  if ((err = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking)) != cudaSuccess) return fail(err, "stream");
+  if ((err = cudaEventCreateWithFlags(&e->in, cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
+  if ((err = cudaEventCreateWithFlags(&e->out, cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
+  for (auto *c : e->ctxs) c->stream = e->user;
+  // one eager step on the contexts' stream, so the captured step is a steady
+  // one (the first step's forced dt update and the AB2 start-up are host-side
+  // decisions)
+  for (int i = 0; i < n; ++i) {
+    const int rc = step_any(e->ctxs[i], e->states[i]);
+    if (rc != DNSBOX_OK) {
+      ensemble_free(e);
+      return rc;
+    }
+  }
+  if ((err = cudaEventRecord(e->in, e->user)) != cudaSuccess) return fail(err, "event record");
+  if ((err = cudaStreamWaitEvent(e->own, e->in, 0)) != cudaSuccess) return fail(err, "stream wait");
+  for (auto *c : e->ctxs) c->stream = e->own;
+  if ((err = cudaStreamBeginCapture(e->own, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return fail(err, "cudaStreamBeginCapture");
+  int rc = DNSBOX_OK;
+  for (int i = 0; i < n && rc == DNSBOX_OK; ++i) rc = step_any(e->ctxs[i], e->states[i]);
+  err = cudaStreamEndCapture(e->own, &e->graph);
+  for (auto *c : e->ctxs) c->host_step -= 1;   // the captured step has not run
+  if (rc != DNSBOX_OK) {
+    ensemble_free(e);
+    return rc;
+  }
+  if (err != cudaSuccess) return fail(err, "cudaStreamEndCapture");
+  if ((err = cudaGraphInstantiate(&e->exec, e->graph, 0)) != cudaSuccess) return fail(err, "cudaGraphInstantiate");
+  for (auto *c : e->ctxs) c->stream = e->user;
+  *out = e;
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_ensemble_run(dnsbox_ensemble *e, int nsteps) {
+  if (!e || nsteps < 0) return set_err(DNSBOX_ERR_ARG, "invalid argument");
+  CK(cudaSetDevice(e->ctxs[0]->p.device));
+  CK(cudaEventRecord(e->in, e->user));
+  CK(cudaStreamWaitEvent(e->own, e->in, 0));
+  for (int i = 0; i < nsteps; ++i) {
+    CK(cudaGraphLaunch(e->exec, e->own));
+    for (auto *c : e->ctxs) c->host_step += 1;
+  }
+  CK(cudaEventRecord(e->out, e->own));
+  CK(cudaStreamWaitEvent(e->user, e->out, 0));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_ensemble_destroy(dnsbox_ensemble *e) {
+  if (!e) return DNSBOX_OK;
+  cudaSetDevice(e->ctxs[0]->p.device);
+  ensemble_free(e);
   return DNSBOX_OK;
 }

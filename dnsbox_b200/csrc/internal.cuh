@@ -58,6 +58,11 @@ struct dnsbox_ctx {
   int nspec = 0;
   int ab2_started = 0;
   int cfl_first = 1;                     // reference calls set_time_step before the loop
+  int nbatch = 1;                        // boxes of this size advanced together
+  size_t fstride = 0;                    // elements between components / work slots (nbatch * nh)
+  double *d_nu = nullptr;                // per-box viscosity (nbatch > 1) or null
+  int ring_cap = 0;                      // device ring of step records: ring_cap steps x nbatch
+  long long host_step = 0;               // steps issued so far (ring position)
   const void *force = nullptr;           // fixed spectral forcing (3 fields) or null
   char *adj = nullptr;                   // adjoint arena
   size_t adj_bytes = 0;
@@ -100,10 +105,13 @@ struct Prof {
 // ------------------------------------------------------------ shared kernels
 // rhs_Eband (rhs.f90:137-168) over the precomputed band-mode list, stored as
 // (offset lo, offset hi, kx) triples; optionally resets the CFL maxima.
+// One block per box: u + box * bstride, components fstride apart.
 template <typename C>
 __global__ void k_eband(const C *u, long long nh, const int *band, int nband, int nx, StepState *st, double s2,
-                        int reset_umax) {
+                        int reset_umax, long long bstride = 0) {
   __shared__ double red[32];
+  u += (long long)blockIdx.x * bstride;
+  st += blockIdx.x;
   double acc = 0.0;
   for (int i = threadIdx.x; i < nband; i += blockDim.x) {
     const long long off = (long long)(unsigned)band[3 * i] | ((long long)band[3 * i + 1] << 32);
@@ -168,8 +176,8 @@ template <typename T> struct Ops {
     return 1;
   }
 #define DNSBOX_CASE_FIN(NN) \
-  case NN: return Launcher<T, NN>::zfinish(a, nb, st);
-  static cudaError_t zfinish(int n, const FinishArgs<T> &a, int nb, cudaStream_t st) {
+  case NN: return Launcher<T, NN>::zfinish(a, nb, nbatch, st);
+  static cudaError_t zfinish(int n, const FinishArgs<T> &a, int nb, int nbatch, cudaStream_t st) {
     switch (n) { DNSBOX_SIZES(DNSBOX_CASE_FIN) }
     return cudaErrorInvalidValue;
   }
@@ -183,9 +191,11 @@ static inline int grid_for(long long n, int threads = 256, int cap = 148 * 16) {
   return (int)b;
 }
 
-static inline char *field(char *base, const dnsbox_ctx *c, int slot) { return base + (size_t)slot * c->nh * c->cbytes; }
+static inline char *field(char *base, const dnsbox_ctx *c, int slot) {
+  return base + (size_t)slot * c->fstride * c->cbytes;
+}
 static inline const char *cfield(const char *base, const dnsbox_ctx *c, int slot) {
-  return base + (size_t)slot * c->nh * c->cbytes;
+  return base + (size_t)slot * c->fstride * c->cbytes;
 }
 
 static inline int ensure_red(dnsbox_ctx *c, size_t ndoubles) {
@@ -212,6 +222,8 @@ template <typename T> static StridedArgs<T> strided_base(const dnsbox_ctx *c, in
   a.ncols = c->nxh;
   a.nx = c->p.nx;
   a.alpha_x = c->p.alpha_x;
+  a.nbatch = c->nbatch;
+  a.bstride = (long long)c->nh;
   if (axis == 2) {  // z: rows kz/z, tiles over y (ky while y is spectral)
     a.tw = reinterpret_cast<const typename CT<T>::type *>(c->tw[2]);
     a.rowstride = (long long)c->p.ny * c->nxh;

@@ -69,8 +69,9 @@ template <typename T> struct StridedArgs {
   long long otherstride;   // elements between consecutive tiles of the other axis
   double alpha_row, alpha_x;
   int n_other;             // length of the other axis (for ks = 2)
-  int pad1;
+  int nbatch;              // boxes (blockIdx.y), each job pointer advanced by bstride per box
   double alpha_other;
+  long long bstride;
 };
 
 template <typename T, typename C>
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
   const int col = threadIdx.x % TC, p = threadIdx.x / TC;
   const int kx = kx0 + col;
   const bool valid = act && kx < a.ncols;
-  const long long base = (long long)other * a.otherstride + kx;
+  const long long base = (long long)other * a.otherstride + kx + (long long)blockIdx.y * a.bstride;
   C v[E];
   if (valid) {
     // all E loads of the first stage are independent and issued together
@@ -143,8 +144,10 @@ template <typename T> struct XlineNLArgs {
   const C *U, *V, *W, *OX, *OY, *OZ;  // (kx, y, z) space, rows of nxh; omega scaled by 1/N^3
   C *NX, *NY, *NZ;                     // forward x transforms of (omega x u) * s
   const C *tw;
-  double *umax;                        // 3 values, max |u_i| (true scale)
+  StepState *st;                       // per-box step state: umax[3] gets max |u_i| (true scale)
   int nlines, nxh;
+  int lines_per_box;                   // ny * nz
+  int pad0;
   double alpha_x;
   double s;                            // scalemodes
 };
@@ -304,10 +307,12 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
     x0 = warp_max(x0);
     x1 = warp_max(x1);
     x2 = warp_max(x2);
-    if (lane == 0 && a.umax) {
-      atomic_max_nonneg(a.umax + 0, x0 * a.s);
-      atomic_max_nonneg(a.umax + 1, x1 * a.s);
-      atomic_max_nonneg(a.umax + 2, x2 * a.s);
+    if (lane == 0 && a.st) {
+      // B divides ny*nz, so every line of the CTA belongs to one box
+      double *um = a.st[line0 / a.lines_per_box].umax;
+      atomic_max_nonneg(um + 0, x0 * a.s);
+      atomic_max_nonneg(um + 1, x1 * a.s);
+      atomic_max_nonneg(um + 2, x2 * a.s);
     }
   }
 }
@@ -430,10 +435,12 @@ template <typename T> struct FinishArgs {
   C *state;                // FIN_CORR state (3 fields)
   C *nold;                 // AB2 history (3 fields)
   const C *force;          // fixed spectral forcing added to N (3 fields) or null
-  const StepState *st;
-  double *partials;        // per-CTA (E, D) of the new state, or null
+  const StepState *st;     // per-box step state (blockIdx.y)
+  const double *nu_box;    // per-box viscosity or null (use nu)
+  double *partials;        // per-CTA (E, D) of the new state, or null; gridDim.x pairs per box
   const C *tw;
-  long long nh;            // elements per field
+  long long nh;            // elements between components (all boxes of one component)
+  long long bstride;       // elements between boxes
   int nx, ny, nz, nxh;
   double ax, ay, az;
   double nu, Q, Pin, kcut;
@@ -462,7 +469,8 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
   const int col = threadIdx.x % TC, p = threadIdx.x / TC;
   const int kx = kx0 + col;
   const bool valid = act && kx < a.nxh;
-  const long long base = (long long)ky * a.nxh + kx;
+  const int box = blockIdx.y;
+  const long long base = (long long)ky * a.nxh + kx + (long long)box * a.bstride;
   // forward z transforms of the three components, each using its own tile as
   // scratch; fields 0 and 1 park their outputs in this thread's own slots of
   // tiles 0 and 1, field 2 stays in v
@@ -479,7 +487,8 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
     }
   }
 
-  const StepState *st = a.st;
+  const StepState *st = a.st + box;
+  const double nu = a.nu_box ? a.nu_box[box] : a.nu;
   const double dt = st->dt;
   const double fc = a.bandlim ? a.Pin / (2.0 * st->eband) : 0.0;
   double c1 = 0, c2 = 0, tau2 = 0;
@@ -557,7 +566,7 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
           for (int c = 0; c < 3; ++c) a.out[c * a.nh + idx] = Nc[c];
           continue;
         }
-        const T IF = T(exp((a.Q - a.nu * k2) * dt));
+        const T IF = T(exp((a.Q - nu * k2) * dt));
         const T tdt = T(dt);
         if (a.mode == FIN_PRED) {
 #pragma unroll
@@ -579,7 +588,7 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
           }
         } else {  // FIN_AB2
           const T e1c1 = T(c1) * IF;
-          const T e2c2 = T(c2 * exp((a.Q - a.nu * k2) * tau2));
+          const T e2c2 = T(c2 * exp((a.Q - nu * k2) * tau2));
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             const C u = uu[h][c], o = no[h][c];
@@ -600,8 +609,9 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
     double r2[2] = {esum, dsum};
     block_sum<2>(r2, red);
     if (threadIdx.x == 0) {
-      a.partials[2 * blockIdx.x] = r2[0];
-      a.partials[2 * blockIdx.x + 1] = r2[1];
+      double *pp = a.partials + 2 * ((long long)box * gridDim.x + blockIdx.x);
+      pp[0] = r2[0];
+      pp[1] = r2[1];
     }
   }
 }

@@ -12,7 +12,7 @@ template <typename T, int N> struct Launcher {
   static cudaError_t xline_nl(const XlineNLArgs<T> &a, cudaStream_t st);
   static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);
   static cudaError_t xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_t st);
-  static cudaError_t zfinish(const FinishArgs<T> &a, int nblocks, cudaStream_t st);
+  static cudaError_t zfinish(const FinishArgs<T> &a, int nblocks, int nbatch, cudaStream_t st);
   static int strided_threads();
   static int zfinish_threads();
   static int zfinish_cols();
@@ -43,7 +43,7 @@ cudaError_t Launcher<T, N>::strided(const StridedArgs<T> &a, bool inv, int ntile
   using C = typename CT<T>::type;
   const size_t smem = (size_t)N * TileCols<T>::v * sizeof(C);
   const int nt = strided_threads();
-  const unsigned nb = (unsigned)ntiles * a.njobs;
+  const dim3 nb((unsigned)ntiles * a.njobs, (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
   cudaError_t e;
   if (inv) {
     if ((e = set_smem(k_strided<T, N, true>, smem)) != cudaSuccess) return e;
@@ -95,13 +95,13 @@ cudaError_t Launcher<T, N>::xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_
 }
 
 template <typename T, int N>
-cudaError_t Launcher<T, N>::zfinish(const FinishArgs<T> &a, int nblocks, cudaStream_t st) {
+cudaError_t Launcher<T, N>::zfinish(const FinishArgs<T> &a, int nblocks, int nbatch, cudaStream_t st) {
   using C = typename CT<T>::type;
   const size_t smem = (size_t)3 * N * FinishCols<T, N>::v * sizeof(C);
   const int nt = zfinish_threads();
   cudaError_t e;
   if ((e = set_smem(k_zfinish<T, N>, smem)) != cudaSuccess) return e;
-  k_zfinish<T, N><<<(unsigned)nblocks, nt, smem, st>>>(a);
+  k_zfinish<T, N><<<dim3((unsigned)nblocks, (unsigned)nbatch), nt, smem, st>>>(a);
   return cudaGetLastError();
 }
 #endif

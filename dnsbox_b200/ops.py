@@ -51,7 +51,7 @@ class Box:
                  ab2="reference", nu=0.005, Q=0.0, kCutOff=2.0, Pin=0.1, Deltak=1.0,
                  courant_min=0.15, courant_max=0.2, dt_max=1.0e-2, dt=1.0e-3, bandlim=True,
                  spherical=False, tstep_fix=False, hminone=True, spectrum_mode="mpi",
-                 adj_phat="intent", alpha=(1.0, 1.0, 1.0), device=None):
+                 adj_phat="intent", alpha=(1.0, 1.0, 1.0), device=None, nbatch=1):
         if not torch.cuda.is_available():
             raise RuntimeError("dnsbox_b200 needs a CUDA device (there is no CPU path)")
         lib = _lib.load()
@@ -71,12 +71,14 @@ class Box:
         p.spectrum_mode = SPECTRUM_MODE[spectrum_mode]
         p.adj_phat = ADJ_PHAT[adj_phat]
         p.device = device
+        p.nbatch = int(nbatch)
         p.alpha_x, p.alpha_y, p.alpha_z = alpha
         p.nu, p.Q, p.kCutOff, p.Pin, p.Deltak = nu, Q, kCutOff, Pin, Deltak
         p.courant_min, p.courant_max, p.dt_max, p.dt = courant_min, courant_max, dt_max, dt
         self.params = p
         self.nx, self.ny, self.nz = nx, ny, nz
         self.nxh = nx // 2 + 1
+        self.nbatch = max(1, int(nbatch))
         self.precision = precision
         self.cdtype = torch.complex128 if precision == "fp64" else torch.complex64
         self.rdtype = torch.float64 if precision == "fp64" else torch.float32
@@ -104,16 +106,19 @@ class Box:
         _lib.check(self._lib.dnsbox_set_stream(self._h, ctypes.c_void_p(s)))
 
     def _check_state(self, t: torch.Tensor, name="uhat"):
-        shape = (3, self.nz, self.ny, self.nxh)
+        shape = self.spectral_shape()
         if t.shape != shape or t.dtype != self.cdtype or not t.is_contiguous() or t.device != self.device:
             raise ValueError(f"{name} must be a contiguous {self.cdtype} tensor of shape {shape} on "
                              f"{self.device}, got {tuple(t.shape)} {t.dtype} {t.device}")
 
     def spectral_shape(self):
+        """(3, nz, ny, nxh), or (3, nbatch, nz, ny, nxh) for a batched Box."""
+        if self.nbatch > 1:
+            return (3, self.nbatch, self.nz, self.ny, self.nxh)
         return (3, self.nz, self.ny, self.nxh)
 
-    def zeros(self, ncomp=3):
-        return torch.zeros((ncomp, self.nz, self.ny, self.nxh), dtype=self.cdtype, device=self.device)
+    def zeros(self):
+        return torch.zeros(self.spectral_shape(), dtype=self.cdtype, device=self.device)
 
     def from_numpy(self, uh: np.ndarray) -> torch.Tensor:
         return torch.from_numpy(np.ascontiguousarray(uh)).to(self.device, self.cdtype)
@@ -159,15 +164,28 @@ class Box:
         if not diag:
             _lib.check(self._lib.dnsbox_step(self._h, _ptr(uh), int(nsteps), None))
             return None
-        recs = (_lib.Diag * nsteps)()
+        recs = (_lib.Diag * (nsteps * self.nbatch))()
         _lib.check(self._lib.dnsbox_step(self._h, _ptr(uh), int(nsteps), recs))
-        out = []
-        for r in recs:
-            out.append(dict(t=r.t, dt=r.dt, ekin=r.ekin, dissipation=r.dissipation,
-                            production_literal=r.production_literal,
-                            injected_power=r.injected_power, courant=r.courant,
-                            umax=tuple(r.umax), eband=r.eband, step=r.step))
-        return out
+        return self._records(recs, nsteps)
+
+    def _records(self, recs, nsteps):
+        out = [dict(t=r.t, dt=r.dt, ekin=r.ekin, dissipation=r.dissipation,
+                    production_literal=r.production_literal, injected_power=r.injected_power,
+                    courant=r.courant, umax=tuple(r.umax), eband=r.eband, step=r.step) for r in recs]
+        if self.nbatch == 1:
+            return out
+        return [out[i * self.nbatch:(i + 1) * self.nbatch] for i in range(nsteps)]
+
+    def diag_read(self, nrecent: int):
+        """Step records of the last nrecent steps (kept on the device)."""
+        self._sync_stream()
+        recs = (_lib.Diag * (nrecent * self.nbatch))()
+        _lib.check(self._lib.dnsbox_diag_read(self._h, int(nrecent), recs))
+        return self._records(recs, nrecent)
+
+    def set_batch_nu(self, nus):
+        v = np.ascontiguousarray(np.broadcast_to(np.asarray(nus, np.float64), (self.nbatch,)))
+        _lib.check(self._lib.dnsbox_set_batch_nu(self._h, v.ctypes.data_as(_lib._DP)))
 
     def project(self, uh):
         self._check_state(uh)

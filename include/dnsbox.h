@@ -66,7 +66,8 @@ typedef struct dnsbox_params {
   int32_t spectrum_mode;         /* enum dnsbox_spectrum_mode                */
   int32_t adj_phat;              /* enum dnsbox_adj_phat                     */
   int32_t device;                /* CUDA device ordinal                      */
-  int32_t reserved_i[3];
+  int32_t nbatch;                /* boxes of this size advanced together (0 or 1: one box) */
+  int32_t reserved_i[2];
   double alpha_x, alpha_y, alpha_z; /* parameters.f90:18-20                  */
   double nu;                     /* parameters.f90:21                        */
   double Q;                      /* parameters.f90:22                        */
@@ -96,6 +97,7 @@ typedef struct dnsbox_diag {
 } dnsbox_diag;
 
 typedef struct dnsbox_ctx dnsbox_ctx;
+typedef struct dnsbox_ensemble dnsbox_ensemble;
 
 /* ---- context (replaces var_init, variables.f90:99-280) ------------------ */
 void dnsbox_default_params(dnsbox_params *p);
@@ -210,6 +212,28 @@ int dnsbox_residual_grad(dnsbox_ctx *ctx, const void *uhat3_dev, void *grad3_dev
  * dnsboxAdj.f90:76-199.  J_host (niter+1 values) and alpha_io (initial/final
  * step length) may be NULL. */
 int dnsbox_adjoint_descent(dnsbox_ctx *ctx, void *uhat3_dev, int niter, double *J_host, double *alpha_io);
+
+/* ---- batched boxes and ensembles (SURVEY config 2: independent boxes of
+ *      mixed N and nu; no reference counterpart -- the reference runs one box
+ *      per MPI job).  A context created with nbatch > 1 holds nbatch boxes of
+ *      one size; its states are component-major, [3][nbatch][nz][ny][nx/2+1],
+ *      and dnsbox_step / dnsbox_rhs_nonlinear advance all boxes in the same
+ *      launches (box index on the grid's y dimension), each box with its own
+ *      dt, clock, band energy, CFL control, diagnostics and viscosity.  The
+ *      single-box operators (project, spectrum, transforms, upload/download,
+ *      adjoint) return DNSBOX_ERR_UNSUPPORTED on batched contexts. -------- */
+int dnsbox_batch_size(const dnsbox_ctx *ctx);
+int dnsbox_set_batch_nu(dnsbox_ctx *ctx, const double *nu_host);
+/* Step records of the last nrecent steps (nrecent * nbatch records, step
+ * major); the device keeps the last 1024 steps. */
+int dnsbox_diag_read(dnsbox_ctx *ctx, int nrecent, dnsbox_diag *diag_host);
+/* Captures one step of every (context, state) pair into a CUDA graph on the
+ * first context's stream (all contexts are switched to it).  Every state is
+ * first advanced by one step eagerly, so the captured step is a steady one. */
+int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *states_dev, int n, dnsbox_ensemble **out);
+/* Replays the captured step nsteps times (asynchronous). */
+int dnsbox_ensemble_run(dnsbox_ensemble *ens, int nsteps);
+int dnsbox_ensemble_destroy(dnsbox_ensemble *ens);
 
 /* ---- measurement ------------------------------------------------------------
  * No reference counterpart (the reference times nothing; Makefile:3 passes
