@@ -158,6 +158,18 @@ def make_box(n, precision, rank):
                device=torch.cuda.current_device())
 
 
+def max_over_ranks(ms, device="cuda"):
+    """Slowest rank's time (all ranks take part; NCCL on GPUs, gloo on CPU)."""
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world, steps, max_ms):
+    """Whole-job steps/s of `world` independent boxes timed by the slowest rank."""
+    return world * steps / (max_ms / 1e3)
+
+
 def timed_steps(box, u, k, dist_on):
     """K steps bracketed by barrier + synchronize; CUDA events on the launch stream."""
     stream = torch.cuda.current_stream()
@@ -175,9 +187,7 @@ def timed_steps(box, u, k, dist_on):
         torch.distributed.barrier()
     ms = e0.elapsed_time(e1)
     if dist_on:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms)
     return ms
 
 
@@ -256,6 +266,37 @@ def adjoint_rate(iters=40):
             "J_first": float(hist[0]), "J_last": float(hist[np.isfinite(hist)][-1])}
 
 
+def ensemble_rate(steps=50):
+    """Config 2: 96 independent boxes (32 each of 32^3, 64^3, 96^3), FP32 state,
+    FP64 diagnostics, seeds 0..95, nu log-uniform in [5e-3, 5e-2] (seed 1000),
+    k0 = 3, fixed dt = 1e-3, IF-Heun; one CUDA-graph replay advances all 96."""
+    from dnsbox_b200.ensemble import Ensemble, config2_nus, make_group
+    nus = config2_nus(96, seed=1000)
+    groups = []
+    for g, n in enumerate((32, 64, 96)):
+        sl = slice(32 * g, 32 * (g + 1))
+        groups.append(make_group(n, 32, seeds=range(32 * g, 32 * (g + 1)), nus=nus[sl], dt=1e-3))
+    ens = Ensemble(groups)
+    ens.run(3)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.run(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    recs = [box.diag_read(1)[0] for box, _ in groups]
+    finite = all(np.isfinite(r["ekin"]) for grp in recs for r in grp)
+    ens.close()
+    for box, _ in groups:
+        box.close()
+    return {"value": 96 * steps / (ms / 1e3), "unit": "box-steps/s", "boxes": 96, "steps": steps,
+            "ms_per_ensemble_step": ms / steps, "finite": finite,
+            "graph": "one CUDA-graph replay per ensemble step (3 batched size groups)"}
+
+
 def read_traffic(prec, n):
     """DRAM bytes per launch from a committed ncu summary, if one exists."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
@@ -304,7 +345,7 @@ def run_ours(args, rank, world, dist_on):
         return
     main = args.precisions[0]
     r = results[main]
-    steps_s = world * args.steps / (r["ms"] / 1e3)
+    steps_s = replica_rate(world, args.steps, r["ms"])
     # dominant kernel roofline
     pr = r["profile"]
     per_pass = {}
@@ -350,12 +391,18 @@ def run_ours(args, rank, world, dist_on):
                        "d2h_bytes_per_step": e2e[2]}
     for prec in args.precisions[1:]:
         rr = results[prec]
+        prr = rr["profile"]
         line.setdefault("variants", {})[prec] = {
             "value": world * args.steps / (rr["ms"] / 1e3), "ms_per_step": rr["ms"] / args.steps,
-            "gpu_launches": rr["launches"], "clocks": rr["clocks"]}
+            "gpu_launches": rr["launches"], "clocks": rr["clocks"],
+            "passes": {k: {"avg_us": round(1e3 * prr["ms"][k] / prr["launches"][k], 2),
+                           "gbs": round(sum(f[i % len(f)] for i in range(prr["launches"][k])) * rr["field_bytes"]
+                                        / (prr["ms"][k] / 1e3) / 1e9, 1)}
+                       for k, f in PASS_FIELDS_HEUN.items() if prr["launches"][k]}}
     if world == 1 and not args.no_extra:
         line["extra"] = extra_sizes(args)
         line["extra"]["adjoint_descent_64"] = adjoint_rate()
+        line["extra"]["ensemble_96"] = ensemble_rate()
     if world == 1 and not args.no_cpu_baseline:
         from oracle import dnsbox_oracle as O
         rate, done, el = cpu_reference_rate(n, 3, budget_s=args.cpu_budget, warmup=0)

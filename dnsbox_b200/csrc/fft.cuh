@@ -21,6 +21,7 @@ namespace dnsbox {
 template <int N> struct FftPlan;
 #define DNSBOX_PLAN(NN, EE, ...)                                               \
   template <> struct FftPlan<NN> {                                             \
+    static constexpr int N = NN;                                               \
     static constexpr int E = EE;                                               \
     static constexpr int R[] = {__VA_ARGS__};                                  \
     static constexpr int NST = sizeof(R) / sizeof(int);                        \
@@ -40,6 +41,39 @@ DNSBOX_PLAN(256, 16, 16, 16)
 DNSBOX_PLAN(512, 8, 8, 8, 8)
 DNSBOX_PLAN(1024, 16, 16, 16, 4)
 #undef DNSBOX_PLAN
+
+// Plans with 32 threads per sequence (E = N / 32), for kernels in which one
+// warp owns whole sequences and synchronises with __syncwarp only.
+template <int N> struct WarpPlan;
+#define DNSBOX_WPLAN(NN, EE, ...)                                              \
+  template <> struct WarpPlan<NN> {                                            \
+    static constexpr int N = NN;                                               \
+    static constexpr int E = EE;                                               \
+    static constexpr int R[] = {__VA_ARGS__};                                  \
+    static constexpr int NST = sizeof(R) / sizeof(int);                        \
+    __host__ __device__ static constexpr int ns(int s) { int p = 1; for (int i = 0; i < s; ++i) p *= R[i]; return p; } \
+  };
+DNSBOX_WPLAN(256, 8, 8, 8, 4)
+DNSBOX_WPLAN(512, 16, 16, 8, 4)
+DNSBOX_WPLAN(1024, 32, 16, 16, 4)
+#undef DNSBOX_WPLAN
+
+// Shared-memory addressing of element (row, col) of a tile.  Row-major tiles
+// (column fastest) suit kernels whose threads run along columns; the skewed
+// column-major layout suits one warp per sequence: with the skew row / R0 the
+// first stage's stride-R0 writes and all consecutive-row accesses of a plan
+// fall in distinct 16-byte bank groups.
+struct AddrRM {
+  __device__ static __forceinline__ int at(int row, int col, int ld) { return row * ld + col; }
+};
+template <int R0> struct AddrSkew {
+  __device__ static __forceinline__ int at(int row, int col, int ld) { return col * ld + row + row / R0; }
+};
+
+template <bool WARP> __device__ __forceinline__ void fft_sync() {
+  if constexpr (WARP) __syncwarp();
+  else __syncthreads();
+}
 
 // ----------------------------------------------------------------- butterflies
 template <typename C, bool INV> __device__ __forceinline__ void dft2(C &a, C &b) {
@@ -148,10 +182,10 @@ template <int R, typename C, bool INV> __device__ __forceinline__ void dft(C *v)
 // ----------------------------------------------------------------- stages
 // One Stockham stage on column `col` of the tile; p in [0, N/E).  All threads
 // of the block call it (barriers inside); `active` masks idle threads.
-template <typename C, int N, int S, bool INV>
-__device__ __forceinline__ void fft_stage(C *s, int LD, int col, int p, bool active,
-                                          const C *__restrict__ tw) {
-  using PL = FftPlan<N>;
+template <typename C, class PL, int S, bool INV, bool WARP, class AD = AddrRM>
+__device__ __forceinline__ void fft_stage_p(C *s, int LD, int col, int p, bool active,
+                                            const C *__restrict__ tw) {
+  constexpr int N = PL::N;
   constexpr int R = PL::R[S];
   constexpr int NS = PL::ns(S);
   constexpr int E = PL::E;
@@ -164,10 +198,10 @@ __device__ __forceinline__ void fft_stage(C *s, int LD, int col, int p, bool act
     for (int m = 0; m < M; ++m) {
       const int b = p + m * P;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[m][r] = s[(b + r * NB) * LD + col];
+      for (int r = 0; r < R; ++r) v[m][r] = s[AD::at(b + r * NB, col, LD)];
     }
   }
-  __syncthreads();
+  fft_sync<WARP>();
   if (active) {
 #pragma unroll
     for (int m = 0; m < M; ++m) {
@@ -184,10 +218,15 @@ __device__ __forceinline__ void fft_stage(C *s, int LD, int col, int p, bool act
       dft<R, C, INV>(v[m]);
       const int o = (b / NS) * NS * R + j;
 #pragma unroll
-      for (int r = 0; r < R; ++r) s[(o + r * NS) * LD + col] = v[m][r];
+      for (int r = 0; r < R; ++r) s[AD::at(o + r * NS, col, LD)] = v[m][r];
     }
   }
-  __syncthreads();
+  fft_sync<WARP>();
+}
+
+template <typename C, int N, int S, bool INV>
+__device__ __forceinline__ void fft_stage(C *s, int LD, int col, int p, bool active, const C *__restrict__ tw) {
+  fft_stage_p<C, FftPlan<N>, S, INV, false>(s, LD, col, p, active, tw);
 }
 
 template <typename C, int N, bool INV, int S = 0>
@@ -206,8 +245,8 @@ __device__ __forceinline__ void fft_columns(C *s, int LD, int col, int p, bool a
 // can load the first stage's inputs straight from global memory and store the
 // last stage's outputs straight back, with only the middle exchanges in
 // shared memory.
-template <int N> struct FftEnds {
-  using PL = FftPlan<N>;
+template <class PL> struct FftEndsP {
+  static constexpr int N = PL::N;
   static constexpr int E = PL::E;
   static constexpr int P = N / E;
   static constexpr int R0 = PL::R[0];
@@ -217,13 +256,14 @@ template <int N> struct FftEnds {
   __device__ static __forceinline__ int in_row(int p, int i) { return p + (i / R0) * P + (i % R0) * NB0; }
   __device__ static __forceinline__ int out_row(int p, int i) { return p + (i / RL) * P + (i % RL) * NBL; }
 };
+template <int N> using FftEnds = FftEndsP<FftPlan<N>>;
 
 // Stage 0 on registers (no twiddles since Ns = 1), result stored to shared
-// memory in Stockham order, then barrier.  For a single-stage plan the result
-// stays in v (in out_row order) and nothing touches shared memory.
-template <typename C, int N, bool INV>
-__device__ __forceinline__ void fft_first_regs(C *v, C *s, int LD, int col, int p, bool active) {
-  using PL = FftPlan<N>;
+// memory in Stockham order, then a barrier.  For a single-stage plan the
+// result stays in v (in out_row order) and nothing touches shared memory.
+template <typename C, class PL, bool INV, bool WARP, class AD = AddrRM>
+__device__ __forceinline__ void fft_first_regs_p(C *v, C *s, int LD, int col, int p, bool active) {
+  constexpr int N = PL::N;
   constexpr int R = PL::R[0];
   constexpr int M = PL::E / R;
   constexpr int P = N / PL::E;
@@ -237,19 +277,19 @@ __device__ __forceinline__ void fft_first_regs(C *v, C *s, int LD, int col, int 
       for (int m = 0; m < M; ++m) {
         const int b = p + m * P;
 #pragma unroll
-        for (int r = 0; r < R; ++r) s[(b * R + r) * LD + col] = v[m * R + r];
+        for (int r = 0; r < R; ++r) s[AD::at(b * R + r, col, LD)] = v[m * R + r];
       }
     }
-    __syncthreads();
+    fft_sync<WARP>();
   }
 }
 
 // Last stage from shared memory into registers (v in out_row order).  The
 // caller owns the barrier that must follow before shared memory is reused.
-template <typename C, int N, bool INV>
-__device__ __forceinline__ void fft_last_regs(C *v, const C *s, int LD, int col, int p, bool active,
-                                              const C *__restrict__ tw) {
-  using PL = FftPlan<N>;
+template <typename C, class PL, bool INV, class AD = AddrRM>
+__device__ __forceinline__ void fft_last_regs_p(C *v, const C *s, int LD, int col, int p, bool active,
+                                                const C *__restrict__ tw) {
+  constexpr int N = PL::N;
   constexpr int S = PL::NST - 1;
   constexpr int R = PL::R[S];
   constexpr int NS = PL::ns(S);
@@ -261,7 +301,7 @@ __device__ __forceinline__ void fft_last_regs(C *v, const C *s, int LD, int col,
   for (int m = 0; m < M; ++m) {
     const int b = p + m * P;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[m * R + r] = s[(b + r * NB) * LD + col];
+    for (int r = 0; r < R; ++r) v[m * R + r] = s[AD::at(b + r * NB, col, LD)];
     const int j = b % NS;
     constexpr int TS = N / (NS * R);
 #pragma unroll
@@ -274,26 +314,32 @@ __device__ __forceinline__ void fft_last_regs(C *v, const C *s, int LD, int col,
 }
 
 // Stages 1 .. NST-2 in shared memory.
-template <typename C, int N, bool INV, int S = 1>
-__device__ __forceinline__ void fft_middle(C *s, int LD, int col, int p, bool active, const C *__restrict__ tw) {
-  if constexpr (S + 1 < FftPlan<N>::NST) {
-    fft_stage<C, N, S, INV>(s, LD, col, p, active, tw);
-    fft_middle<C, N, INV, S + 1>(s, LD, col, p, active, tw);
+template <typename C, class PL, bool INV, bool WARP, class AD = AddrRM, int S = 1>
+__device__ __forceinline__ void fft_middle_p(C *s, int LD, int col, int p, bool active, const C *__restrict__ tw) {
+  if constexpr (S + 1 < PL::NST) {
+    fft_stage_p<C, PL, S, INV, WARP, AD>(s, LD, col, p, active, tw);
+    fft_middle_p<C, PL, INV, WARP, AD, S + 1>(s, LD, col, p, active, tw);
   }
 }
 
 // Whole transform with v holding the first stage's inputs on entry and the
 // last stage's outputs on exit.  Shared memory (N x LD tile) is scratch;
-// ends with a barrier so the tile may be reused.
+// ends with a barrier (block or warp) so the tile may be reused.
+template <typename C, class PL, bool INV, bool WARP, class AD = AddrRM>
+__device__ __forceinline__ void fft_regs_p(C *v, C *s, int LD, int col, int p, bool active,
+                                           const C *__restrict__ tw) {
+  fft_first_regs_p<C, PL, INV, WARP, AD>(v, s, LD, col, p, active);
+  if constexpr (PL::NST > 1) {
+    fft_middle_p<C, PL, INV, WARP, AD>(s, LD, col, p, active, tw);
+    fft_last_regs_p<C, PL, INV, AD>(v, s, LD, col, p, active, tw);
+    fft_sync<WARP>();
+  }
+}
+
 template <typename C, int N, bool INV>
 __device__ __forceinline__ void fft_regs(C *v, C *s, int LD, int col, int p, bool active,
                                          const C *__restrict__ tw) {
-  fft_first_regs<C, N, INV>(v, s, LD, col, p, active);
-  if constexpr (FftPlan<N>::NST > 1) {
-    fft_middle<C, N, INV>(s, LD, col, p, active, tw);
-    fft_last_regs<C, N, INV>(v, s, LD, col, p, active, tw);
-    __syncthreads();
-  }
+  fft_regs_p<C, FftPlan<N>, INV, false>(v, s, LD, col, p, active, tw);
 }
 
 }  // namespace dnsbox

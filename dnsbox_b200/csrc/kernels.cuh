@@ -24,6 +24,9 @@ namespace dnsbox {
 // shuffle reductions); threads beyond the FFT's own count only take part in
 // the strided element loops and barriers.
 __host__ __device__ constexpr int round32(int x) { return (x + 31) / 32 * 32; }
+// Resident CTAs to ask the register allocator for: `want` for blocks of up
+// to 256 threads, one for larger blocks (which hold enough warps alone).
+__host__ __device__ constexpr int min_ctas(int threads, int want) { return threads <= 256 ? want : 1; }
 
 // Host/device step bookkeeping kept in device memory (one per context).
 struct StepState {
@@ -169,7 +172,8 @@ __device__ __forceinline__ C pack_pair(int n, C X1, C X2) {
 }
 
 template <typename T, int N>
-__global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::E)))
+__global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::E)),
+                                  min_ctas(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::E)), 3))
     k_xline_nl(const __grid_constant__ XlineNLArgs<T> a) {
   using C = typename CT<T>::type;
   using EN = FftEnds<N>;
@@ -317,6 +321,133 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
   }
 }
 
+// Warp-granular variant of the fused x pass for N >= 256: each warp owns one
+// line pair from its loads to its stores and synchronises only with
+// __syncwarp, so the SM overlaps one warp's memory phases with another's
+// transforms (the block-wide barriers of k_xline_nl serialise them).  Columns
+// of a warp's tile are the six sequences of k_xline_nl, stored column-major
+// with the row / R0 skew (conflict-free for the 32-threads-per-sequence plan).
+template <typename T, int N> struct XlineWarp {
+  static constexpr bool on = N == 256 || N == 512;
+  static constexpr int wpb = sizeof(T) == 8 ? (N >= 512 ? 1 : 2) : (N >= 1024 ? 1 : (N >= 512 ? 2 : 4));
+};
+
+template <typename T, int N>
+__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
+    k_xline_nl_w(const __grid_constant__ XlineNLArgs<T> a) {
+  using C = typename CT<T>::type;
+  using PL = WarpPlan<N>;
+  using EN = FftEndsP<PL>;
+  using AD = AddrSkew<PL::R[0]>;
+  constexpr int E = PL::E;
+  constexpr int H = N / 2 + 1;
+  constexpr int LDC = N + N / PL::R[0];   // column length with the skew
+  constexpr int WPB = XlineWarp<T, N>::wpb;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C *s = reinterpret_cast<C *>(smem_raw) + (size_t)warp * 6 * LDC;
+  const long long la = 2 * ((long long)blockIdx.x * WPB + warp), lb = la + 1;
+  if (la >= a.nlines) return;
+  const T sc = T(a.s);
+  const C *f1s[6] = {a.U, a.U, a.W, a.OX, a.OX, a.OZ};
+  const C *f2s[6] = {a.V, a.V, a.W, a.OY, a.OY, a.OZ};
+  const long long l1s[6] = {la, lb, la, la, lb, la};
+  const long long l2s[6] = {la, lb, lb, la, lb, lb};
+  // inverse transforms, loads of sequence q+1 issued before the transform of q
+  C x1[E], x2[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int n = EN::in_row(lane, i);
+    const int kk = n <= N / 2 ? n : N - n;
+    x1[i] = f1s[0][l1s[0] * a.nxh + kk];
+    x2[i] = f2s[0][l2s[0] * a.nxh + kk];
+  }
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) {
+    C v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = pack_pair<C, N>(EN::in_row(lane, i), x1[i], x2[i]);
+    if (q < 5) {
+      const C *g1 = f1s[q + 1] + l1s[q + 1] * a.nxh, *g2 = f2s[q + 1] + l2s[q + 1] * a.nxh;
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const int n = EN::in_row(lane, i);
+        const int kk = n <= N / 2 ? n : N - n;
+        x1[i] = g1[kk];
+        x2[i] = g2[kk];
+      }
+    }
+    fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, lane, true, a.tw);
+#pragma unroll
+    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(lane, i), q, LDC)] = v[i];
+  }
+  __syncwarp();
+  // (omega x u) * s, written back as (px_a,py_a) (pz_a,pz_b) (px_b,py_b) in columns 0..2
+  double m0 = 0, m1 = 0, m2 = 0;
+#pragma unroll 4
+  for (int n = lane; n < N; n += 32) {
+    const C c0 = s[AD::at(n, 0, LDC)], c1 = s[AD::at(n, 1, LDC)], c2 = s[AD::at(n, 2, LDC)];
+    const C c3 = s[AD::at(n, 3, LDC)], c4 = s[AD::at(n, 4, LDC)], c5 = s[AD::at(n, 5, LDC)];
+    const T uu[2] = {c0.x, c1.x}, vv[2] = {c0.y, c1.y}, ww[2] = {c2.x, c2.y};
+    const T ox[2] = {c3.x, c4.x}, oy[2] = {c3.y, c4.y}, oz[2] = {c5.x, c5.y};
+    T px[2], py[2], pz[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      px[h] = (oy[h] * ww[h] - oz[h] * vv[h]) * sc;
+      py[h] = (oz[h] * uu[h] - ox[h] * ww[h]) * sc;
+      pz[h] = (ox[h] * vv[h] - oy[h] * uu[h]) * sc;
+      m0 = fmax(m0, fabs((double)uu[h]));
+      m1 = fmax(m1, fabs((double)vv[h]));
+      m2 = fmax(m2, fabs((double)ww[h]));
+    }
+    s[AD::at(n, 0, LDC)] = mkc<C>(px[0], py[0]);
+    s[AD::at(n, 1, LDC)] = mkc<C>(pz[0], pz[1]);
+    s[AD::at(n, 2, LDC)] = mkc<C>(px[1], py[1]);
+  }
+  __syncwarp();
+  // forward transforms of the three product sequences
+#pragma unroll 1
+  for (int q = 0; q < 3; ++q) {
+    C v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = s[AD::at(EN::in_row(lane, i), q, LDC)];
+    __syncwarp();
+    fft_regs_p<C, PL, false, true, AD>(v, s, LDC, q, lane, true, a.tw);
+#pragma unroll
+    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(lane, i), q, LDC)] = v[i];
+  }
+  __syncwarp();
+  // unpack two real transforms per sequence and store
+  for (int k = lane; k < H; k += 32) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const C zk = s[AD::at(k, q, LDC)], zn = s[AD::at((N - k) % N, q, LDC)];
+      const C X1 = mkc<C>(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
+      const C X2 = mkc<C>(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
+      if (q == 0) {
+        a.NX[la * a.nxh + k] = X1;
+        a.NY[la * a.nxh + k] = X2;
+      } else if (q == 1) {
+        a.NZ[la * a.nxh + k] = X1;
+        a.NZ[lb * a.nxh + k] = X2;
+      } else {
+        a.NX[lb * a.nxh + k] = X1;
+        a.NY[lb * a.nxh + k] = X2;
+      }
+    }
+  }
+  // CFL maxima of this line pair (both lines lie in one box: ny*nz is even)
+  m0 = warp_max(m0);
+  m1 = warp_max(m1);
+  m2 = warp_max(m2);
+  if (lane == 0 && a.st) {
+    double *um = a.st[la / a.lines_per_box].umax;
+    atomic_max_nonneg(um + 0, m0 * a.s);
+    atomic_max_nonneg(um + 1, m1 * a.s);
+    atomic_max_nonneg(um + 2, m2 * a.s);
+  }
+}
+
 // Plain x-line transforms of nf fields (blockIdx.y = field).
 template <typename T> struct XlineArgs {
   using C = typename CT<T>::type;
@@ -450,7 +581,8 @@ template <typename T> struct FinishArgs {
 };
 
 template <typename T, int N>
-__global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::E)))
+__global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::E)),
+                                  min_ctas(round32(FinishCols<T, N>::v *(N / FftPlan<N>::E)), 2))
     k_zfinish(const __grid_constant__ FinishArgs<T> a) {
   using C = typename CT<T>::type;
   using EN = FftEnds<N>;

@@ -58,6 +58,18 @@ cudaError_t Launcher<T, N>::strided(const StridedArgs<T> &a, bool inv, int ntile
 template <typename T, int N>
 cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, cudaStream_t st) {
   using C = typename CT<T>::type;
+  if constexpr (XlineWarp<T, N>::on) {
+    // warp-granular kernel: one warp per line pair
+    constexpr int WPB = XlineWarp<T, N>::wpb;
+    constexpr int LDC = N + N / WarpPlan<N>::R[0];
+    const size_t smem = (size_t)WPB * 6 * LDC * sizeof(C);
+    cudaError_t e;
+    if ((e = set_smem(k_xline_nl_w<T, N>, smem)) != cudaSuccess) return e;
+    const long long pairs = (a.nlines + 1) / 2;
+    const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
+    k_xline_nl_w<T, N><<<nb, 32 * WPB, smem, st>>>(a);
+    return cudaGetLastError();
+  }
   constexpr int B = XlineB<T, N>::v;
   const size_t smem = (size_t)N * (3 * B + 1) * sizeof(C);
   const int nt = round32(3 * B * (N / FftPlan<N>::E));

@@ -307,3 +307,39 @@ def test_gpu_initial_condition(prec):
     shape = k ** 4 * np.exp(-2 * k ** 2 / 9.0)
     ratio = es[:6] / shape[:6]
     assert np.all(np.abs(ratio / ratio[2] - 1) < 0.6)   # MPI spectrum: kx=0 planes double counted
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_rhs_nonlinear_256(prec):
+    n = 256
+    uh = ic.random_field(n, seed=2, k0=3.0)
+    p = O.Params(nx=n, ny=n, nz=n, nu=2e-3, kCutOff=2.5, Pin=0.1, bandlim=True)
+    want = O.rhs_nonlinear(O.Grid(p), uh)
+    b = box(n, prec, nu=2e-3, kCutOff=2.5, Pin=0.1, bandlim=True)
+    got, _ = b.rhs_nonlinear(b.from_numpy(uh))
+    assert rel(got.cpu().numpy(), want) < tol(prec)
+
+
+def test_rhs_nonlinear_512_properties():
+    """512^3: the unforced rotational term conserves energy, <uhat, N(uhat)> = 0
+    (W-weighted over the half spectrum), and FP32 agrees with FP64."""
+    from dnsbox_b200.ic import random_field_gpu
+    n = 512
+    b64 = box(n, "fp64", bandlim=False)
+    u64 = random_field_gpu(b64, seed=1, k0=3.0)
+    N64, _ = b64.rhs_nonlinear(u64)
+    W = torch.full((n // 2 + 1,), 2.0, dtype=torch.float64, device=u64.device)
+    W[0] = W[n // 2] = 1.0
+    dot = float((W * (u64.conj() * N64).real).sum())
+    norm = float(u64.abs().norm() * N64.abs().norm())
+    assert abs(dot) < 1e-12 * norm
+    host = u64.cpu()
+    del N64
+    b64.close()
+    b32 = box(n, "fp32", bandlim=False)
+    u32 = host.to(b32.device, torch.complex64)
+    N32, _ = b32.rhs_nonlinear(u32)
+    b32.close()
+    b64 = box(n, "fp64", bandlim=False)
+    N64, _ = b64.rhs_nonlinear(host.to(b64.device))
+    assert float((N32.to(torch.complex128) - N64).abs().norm() / N64.abs().norm()) < 2e-5
