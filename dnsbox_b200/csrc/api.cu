@@ -467,6 +467,20 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   return DNSBOX_OK;
 }
 
+// Synchronises the stream and reports a tensor-core pass whose MMA
+// completion wait gave up (the flag is cleared).
+static int tc_check(dnsbox_ctx *c) {
+  int *flag = reinterpret_cast<int *>(c->hstage + 63);
+  if (c->tc) CK(cudaMemcpyAsync(flag, c->tc_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->tc && *flag) {
+    CK(cudaMemsetAsync(c->tc_status, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return set_err(DNSBOX_ERR_TIMEOUT, "tensor-core DFT pass: MMA completion wait gave up");
+  }
+  return DNSBOX_OK;
+}
+
 // Copies the records of steps [first, first + n) (n <= ring_cap) from the
 // device ring into host[(step - first) * nbatch + box].
 static int ring_read(dnsbox_ctx *c, long long first, int n, dnsbox_diag *host) {
@@ -480,7 +494,7 @@ static int ring_read(dnsbox_ctx *c, long long first, int n, dnsbox_diag *host) {
                        (size_t)run * c->nbatch * sizeof(dnsbox_diag), cudaMemcpyDeviceToHost, c->stream));
     done += run;
   }
-  CK(cudaStreamSynchronize(c->stream));
+  RET(tc_check(c));
   return DNSBOX_OK;
 }
 
@@ -545,8 +559,44 @@ static int alloc_twiddles(dnsbox_ctx *c, int axis, int n) {
   return DNSBOX_OK;
 }
 
+// DFT-64 operands of the tensor-core passes (kernels_tc.cuh): for each
+// direction the real and imaginary parts of F[k][n] = exp(-+2 pi i k n / 64)
+// as rows 2k and 2k + 1 of A, split into f16 hi = rn(A) and lo = rn(A - hi),
+// each stored as a 128 x 64 K-major operand.
+static int alloc_dft64(dnsbox_ctx *c) {
+  std::vector<__half> h((size_t)kTcDftBytes / 2);
+  for (int dir = 0; dir < 2; ++dir) {
+    __half *hi = h.data() + (size_t)dir * 2 * 128 * 64;
+    __half *lo = hi + 128 * 64;
+    const double sgn = dir == 0 ? -1.0 : 1.0;
+    for (int k = 0; k < 64; ++k)
+      for (int n = 0; n < 64; ++n) {
+        const long double ang = 2.0L * 3.141592653589793238462643383279502884L * (long double)((k * n) % 64) / 64.0L;
+        const double val[2] = {(double)cosl(ang), sgn * (double)sinl(ang)};
+        for (int rb = 0; rb < 2; ++rb) {
+          const __half vh = __double2half(val[rb]);
+          const __half vl = __double2half(val[rb] - (double)__half2float(vh));
+          const int off = tc::kmajor_offset(2 * k + rb, n, 128) / 2;
+          hi[off] = vh;
+          lo[off] = vl;
+        }
+      }
+  }
+  CK(cudaMalloc(&c->adft, (size_t)kTcDftBytes));
+  CK(cudaMemcpy(c->adft, h.data(), (size_t)kTcDftBytes, cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&c->tc_status, sizeof(int)));
+  CK(cudaMemset(c->tc_status, 0, sizeof(int)));
+  int dev = 0, nsm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  c->tc_ctas = TcPlan<256>::CTAS_PER_SM * nsm;   // persistent: every resident CTA slot
+  return DNSBOX_OK;
+}
+
 static void free_ctx(dnsbox_ctx *c) {
   if (!c) return;
+  cudaFree(c->adft);
+  cudaFree(c->tc_status);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   cudaFree(c->W1);
   cudaFree(c->W2);
@@ -569,7 +619,7 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
   *out = nullptr;
   if (!dnsbox_supported_size(p->nx) || !dnsbox_supported_size(p->ny) || !dnsbox_supported_size(p->nz))
     return set_err(DNSBOX_ERR_SIZE, "unsupported grid %dx%dx%d", p->nx, p->ny, p->nz);
-  if (p->precision != DNSBOX_FP64 && p->precision != DNSBOX_FP32)
+  if (p->precision != DNSBOX_FP64 && p->precision != DNSBOX_FP32 && p->precision != DNSBOX_TC_SPLIT)
     return set_err(DNSBOX_ERR_UNSUPPORTED, "precision %d not available", p->precision);
   if (!(p->nu >= 0.0) || !(p->Deltak > 0.0) || !(p->dt > 0.0) || !(p->alpha_x > 0) || !(p->alpha_y > 0) ||
       !(p->alpha_z > 0))
@@ -608,6 +658,10 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
   if ((rc = alloc_twiddles(c, 0, p->nx)) || (rc = alloc_twiddles(c, 1, p->ny)) ||
       (rc = alloc_twiddles(c, 2, p->nz)))
     return fail(rc);
+  if (p->precision == DNSBOX_TC_SPLIT) {
+    c->tc = 1;
+    if ((rc = alloc_dft64(c))) return fail(rc);
+  }
   {
     const int ztc = c->fp64 ? Ops<double>::zfinish_cols(p->nz) : Ops<float>::zfinish_cols(p->nz);
     c->npartials = ((c->nxh + ztc - 1) / ztc) * p->ny;

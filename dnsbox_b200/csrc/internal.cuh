@@ -64,6 +64,10 @@ struct dnsbox_ctx {
   int ring_cap = 0;                      // device ring of step records: ring_cap steps x nbatch
   long long host_step = 0;               // steps issued so far (ring position)
   const void *force = nullptr;           // fixed spectral forcing (3 fields) or null
+  int tc = 0;                            // DNSBOX_TC_SPLIT: tensor-core strided passes
+  void *adft = nullptr;                  // device DFT-64 operands (forward hi, lo, inverse hi, lo)
+  int *tc_status = nullptr;              // device flag: an MMA completion wait gave up
+  int tc_ctas = 0;                       // persistent grid of the tensor-core passes
   char *adj = nullptr;                   // adjoint arena
   size_t adj_bytes = 0;
   // measurement
@@ -150,6 +154,19 @@ template <typename T> struct Ops {
   static cudaError_t strided(int n, const StridedArgs<T> &a, bool inv, int ntiles, cudaStream_t st) {
     switch (n) { DNSBOX_SIZES(DNSBOX_CASE_STRIDED) }
     return cudaErrorInvalidValue;
+  }
+#define DNSBOX_CASE_TC(NN) \
+  case NN: return Launcher<T, NN>::strided_tc(a, inv, nother, adft, status, nctas, st);
+  static cudaError_t strided_tc(int n, const StridedArgs<T> &a, bool inv, int nother, const void *adft,
+                                int *status, int nctas, cudaStream_t st) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_TC) }
+    return cudaErrorInvalidValue;
+  }
+#define DNSBOX_CASE_HASTC(NN) \
+  case NN: return Launcher<T, NN>::has_tc();
+  static bool has_tc(int n) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_HASTC) }
+    return false;
   }
 #define DNSBOX_CASE_NL(NN) \
   case NN: return Launcher<T, NN>::xline_nl(a, st);
@@ -262,6 +279,10 @@ static int run_strided(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<T> &
   const int nother = axis == 2 ? c->p.ny : c->p.nz;
   const int n = axis == 2 ? c->p.nz : c->p.ny;
   Prof pr(c, kind);
+  if (c->tc && Ops<T>::has_tc(n)) {
+    CK(Ops<T>::strided_tc(n, a, inv, nother, c->adft, c->tc_status, c->tc_ctas, c->stream));
+    return DNSBOX_OK;
+  }
   CK(Ops<T>::strided(n, a, inv, ntx * nother, c->stream));
   return DNSBOX_OK;
 }

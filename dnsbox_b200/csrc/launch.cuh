@@ -3,12 +3,20 @@
 // pair), so the library compiles in parallel; api.cu sees declarations only.
 #pragma once
 
+#include <type_traits>
+
 #include "kernels.cuh"
+#include "kernels_tc.cuh"
 
 namespace dnsbox {
 
 template <typename T, int N> struct Launcher {
   static cudaError_t strided(const StridedArgs<T> &a, bool inv, int ntiles, cudaStream_t st);
+  // tensor-core split-precision form of `strided` (FP32, N = 128 .. 1024);
+  // adft: the four DFT-64 operands, status: set to 1 if an MMA wait gave up
+  static cudaError_t strided_tc(const StridedArgs<T> &a, bool inv, int nother, const void *adft, int *status,
+                                int nctas, cudaStream_t st);
+  static bool has_tc();
   static cudaError_t xline_nl(const XlineNLArgs<T> &a, cudaStream_t st);
   static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);
   static cudaError_t xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_t st);
@@ -53,6 +61,46 @@ cudaError_t Launcher<T, N>::strided(const StridedArgs<T> &a, bool inv, int ntile
     k_strided<T, N, false><<<nb, nt, smem, st>>>(a);
   }
   return cudaGetLastError();
+}
+
+template <typename T, int N> bool Launcher<T, N>::has_tc() {
+  return std::is_same<T, float>::value && TcPlan<N>::on;
+}
+
+template <typename T, int N>
+cudaError_t Launcher<T, N>::strided_tc(const StridedArgs<T> &a, bool inv, int nother, const void *adft,
+                                       int *status, int nctas, cudaStream_t st) {
+  if constexpr (std::is_same<T, float>::value && TcPlan<N>::on) {
+    using PL = TcPlan<N>;
+    TcArgs g;
+    g.ntx = (a.ncols + PL::TCW - 1) / PL::TCW;
+    g.nother = nother;
+    const long long total = (long long)a.njobs * g.ntx * nother * (a.nbatch > 0 ? a.nbatch : 1);
+    if (total == 0) return cudaSuccess;
+    if (total + 2LL * nctas >= (1LL << 31)) return cudaErrorInvalidValue;
+    g.total = (int)total;
+    g.per_box.init((unsigned)(a.njobs * g.ntx * nother));
+    g.njobs.init((unsigned)a.njobs);
+    g.ntxd.init((unsigned)g.ntx);
+    const unsigned nb = (unsigned)(g.total < nctas ? g.total : nctas);
+    const __half *A = reinterpret_cast<const __half *>(adft) + (inv ? 2 * 128 * 64 : 0);
+    cudaError_t e;
+    // two 96 KB CTAs per SM: ask for the largest shared-memory carveout
+    if ((e = cudaFuncSetAttribute(inv ? k_strided_tc<N, true> : k_strided_tc<N, false>,
+                                  cudaFuncAttributePreferredSharedMemoryCarveout, 100)) != cudaSuccess)
+      return e;
+    if (inv) {
+      if ((e = set_smem(k_strided_tc<N, true>, PL::SMEM)) != cudaSuccess) return e;
+      k_strided_tc<N, true><<<nb, PL::THREADS, PL::SMEM, st>>>(a, g, A, status);
+    } else {
+      if ((e = set_smem(k_strided_tc<N, false>, PL::SMEM)) != cudaSuccess) return e;
+      k_strided_tc<N, false><<<nb, PL::THREADS, PL::SMEM, st>>>(a, g, A, status);
+    }
+    return cudaGetLastError();
+  } else {
+    (void)a, (void)inv, (void)nother, (void)adft, (void)status, (void)nctas, (void)st;
+    return cudaErrorInvalidValue;
+  }
 }
 
 template <typename T, int N>

@@ -1,0 +1,180 @@
+"""Tensor-core split-precision form (precision "tc_split") on the GPU.
+
+The strided (y and z) transforms of lengths 128 .. 1024 run their 64-point
+first stage as tcgen05 MMAs on hi + lo f16 splits of per-pencil scaled FP32
+data (FP32 accumulation in tensor memory); the x axis, the fused z finish and
+axes of other lengths use the FP32 kernels, and the state is FP32.
+
+Bars: transforms and one right-hand side against the FP64 oracle within
+single-precision tolerances; trajectories against the plain FP64 GPU form for
+the velocity (relative L2), the E(k) shells and the dissipation, with the
+tolerance written beside each case."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import dnsbox_oracle as O
+from dnsbox_b200 import ic
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def box(precision="tc_split", n=None, **kw):
+    from dnsbox_b200.ops import Box
+    return Box(n, precision=precision, **kw)
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 128), (64, 256, 128), (96, 128, 512), (16, 1024, 256)])
+def test_tc_transforms_match_pocketfft(shape):
+    nx, ny, nz = shape
+    b = box(nx=nx, ny=ny, nz=nz)
+    g = O.Grid(O.Params(nx=nx, ny=ny, nz=nz))
+    rng = np.random.default_rng(7)
+    f = rng.standard_normal((nz, ny, nx))
+    F = g.r2c(f)
+    Fg = b.r2c(torch.from_numpy(f).to(b.device, b.rdtype)).cpu().numpy()
+    e_r2c = rel(Fg, F)
+    fg = b.c2r(torch.from_numpy(F).to(b.device, b.cdtype)).cpu().numpy()
+    e_c2r = rel(fg, g.c2r(F))
+    print(f"tc transforms {shape}: r2c {e_r2c:.3e} c2r {e_c2r:.3e}")
+    assert e_r2c < 1e-6 and e_c2r < 1e-6   # FP32 storage: a few ulp of 2^-24 per pass
+
+
+def test_tc_path_is_taken_and_close_to_fp32():
+    """The TC form differs bitwise from the FP32 kernels (a different DFT
+    evaluation) but agrees with them to single-precision accuracy."""
+    n = 128
+    rng = np.random.default_rng(3)
+    f = rng.standard_normal((n, n, n)).astype(np.float32)
+    b32, btc = box("fp32", n), box("tc_split", n)
+    a = b32.r2c(torch.from_numpy(f).to(b32.device)).cpu().numpy()
+    t = btc.r2c(torch.from_numpy(f).to(btc.device)).cpu().numpy()
+    assert not np.array_equal(a, t)
+    assert rel(t, a) < 1e-6
+
+
+@pytest.mark.parametrize("e", [-60, 60])
+def test_tc_power_of_two_scale_invariance(e):
+    """Per-pencil power-of-two scaling makes the split exact under a global
+    2^e scale: fields far outside the f16 range (2^-60, 2^60) give the
+    unit-scale result times 2^e, bit for bit."""
+    n = 128
+    rng = np.random.default_rng(5)
+    f = torch.from_numpy(rng.standard_normal((n, n, n)).astype(np.float32))
+    b = box(n=n)
+    one = b.r2c(f.to(b.device))
+    scaled = b.r2c((f * 2.0 ** e).to(b.device))
+    assert torch.equal(scaled, one * 2.0 ** e)
+    back = b.c2r(one * 2.0 ** e)
+    assert torch.equal(back, b.c2r(one) * 2.0 ** e)
+
+
+@pytest.mark.parametrize("n", [128, 256])
+def test_tc_rhs_nonlinear(n):
+    uh = ic.random_field(n, seed=n + 1, k0=3.0)
+    p = O.Params(nx=n, ny=n, nz=n, nu=2e-3, kCutOff=2.5, Pin=0.1, bandlim=True)
+    want, eb = O.rhs_nonlinear(O.Grid(p), uh, return_eband=True)
+    b = box(n=n, nu=2e-3, kCutOff=2.5, Pin=0.1, bandlim=True)
+    got, ebg = b.rhs_nonlinear(b.from_numpy(uh))
+    e = rel(got.cpu().numpy(), want)
+    print(f"tc rhs {n}: {e:.3e}")
+    assert e < 2e-5   # same bar as the FP32 form
+    assert abs(ebg - eb) < 1e-6 * eb
+
+
+def _trajectory(prec, n, uh64, nsteps, **kw):
+    b = box(prec, n, **kw)
+    u = uh64.to(b.device, b.cdtype).clone()
+    recs = b.step(u, nsteps)
+    es, *_ = b.spectrum(u)
+    out = u.to(torch.complex128)
+    b.close()
+    return out, recs, es
+
+
+def _errors(u, recs, es, u64, recs64, es64, floor=1e-9):
+    """Velocity relative L2; the largest relative E(k) error over shells
+    holding at least `floor` of the energy, and over the shells between 1e-14
+    and `floor` (reported only: there the modes are 1e-7 .. 1e-5 of the peak
+    amplitude and FP32 storage round-off dominates both FP32 forms; shells
+    past the dealiasing cube hold FP64 round-off only); the largest relative
+    dissipation error over the steps."""
+    ev = float((u - u64).abs().norm() / u64.abs().norm())
+    sh = np.abs(es - es64) / np.where(es64 > 0, es64, 1.0)
+    tot = es64.sum()
+    ek = float(np.max(sh[es64 >= floor * tot]))
+    tail = (es64 >= 1e-14 * tot) & (es64 < floor * tot)
+    ek_all = float(np.max(sh[tail])) if tail.any() else 0.0
+    dd = max(abs(a["dissipation"] - r["dissipation"]) / r["dissipation"] for a, r in zip(recs, recs64))
+    return ev, ek, ek_all, dd
+
+
+def test_tc_heun_trajectory_128():
+    """Forced turbulence at 128^3, CFL-controlled Heun, 40 steps against the
+    plain FP64 GPU form; the FP32 SIMT form is run beside it for scale."""
+    n, ns = 128, 40
+    kw = dict(nu=2e-3, kCutOff=2.5, Pin=0.1, courant_min=0.5, courant_max=0.5)
+    b64 = box("fp64", n, **kw)
+    u0 = b64.from_numpy(ic.random_field(n, seed=4, k0=3.0))
+    b64.close()
+    u64, r64, e64 = _trajectory("fp64", n, u0, ns, **kw)
+    res = {}
+    for prec in ("fp32", "tc_split"):
+        res[prec] = _errors(*_trajectory(prec, n, u0, ns, **kw), u64, r64, e64)
+        print(f"{prec} 128^3 {ns} steps: vel {res[prec][0]:.3e} E(k) {res[prec][1]:.3e} "
+              f"(tail shells {res[prec][2]:.3e}) D {res[prec][3]:.3e}")
+    ev, ek, _, dd = res["tc_split"]
+    assert ev < 1e-6 and ek < 1e-5 and dd < 1e-6
+    # no worse than the FP32 SIMT form by more than a small factor
+    assert ev < 4 * res["fp32"][0] + 1e-7
+
+
+def test_tc_batched_matches_single():
+    n, ns = 128, 3
+    kw = dict(nu=2e-3, kCutOff=2.5, Pin=0.1, tstep_fix=True, dt=2e-3)
+    us = [ic.random_field(n, seed=s, k0=3.0) for s in (1, 2)]
+    from dnsbox_b200.ops import Box
+    bb = Box(n, precision="tc_split", nbatch=2, **kw)
+    ub = torch.stack([torch.from_numpy(u) for u in us], dim=1).to(bb.device, bb.cdtype).contiguous()
+    bb.step(ub, ns)
+    for i, u in enumerate(us):
+        b1 = box(n=n, **kw)
+        u1 = b1.from_numpy(u)
+        b1.step(u1, ns)
+        assert torch.equal(ub[:, i], u1)
+
+
+def test_tc_512_accuracy_against_fp64():
+    """512^3 forced turbulence (nu = 8e-4, band forcing eps = 0.1, Courant 0.5),
+    100 Heun steps from the seeded k0 = 3 field: TC-split against the plain
+    FP64 GPU form.  Bars: velocity relative L2 <= 1e-6; E(k) <= 1e-5 on every
+    shell holding at least 1e-9 of the energy (the deeper tail is printed);
+    dissipation <= 1e-5 on every step."""
+    from dnsbox_b200.ic import random_field_gpu
+    n, ns = 512, 100
+    kw = dict(nu=8e-4, kCutOff=2.5, Pin=0.1, courant_min=0.5, courant_max=0.5)
+    b64 = box("fp64", n, **kw)
+    u0 = random_field_gpu(b64, seed=0, k0=3.0)
+    b64.close()
+    u0h = u0.cpu()
+    del u0
+    u64, r64, e64 = _trajectory("fp64", n, u0h.cuda(), ns, **kw)
+    u64h = u64.cpu()
+    del u64
+    torch.cuda.empty_cache()
+    res = {}
+    for prec in ("fp32", "tc_split"):
+        u, r, e = _trajectory(prec, n, u0h.cuda(), ns, **kw)
+        res[prec] = _errors(u.cpu(), r, e, u64h, r64, e64)
+        del u
+        torch.cuda.empty_cache()
+        print(f"{prec} 512^3 {ns} steps: vel {res[prec][0]:.3e} E(k) {res[prec][1]:.3e} "
+              f"(tail shells {res[prec][2]:.3e}) D {res[prec][3]:.3e}")
+    ev, ek, _, dd = res["tc_split"]
+    assert ev < 1e-6 and ek < 1e-5 and dd < 1e-5
