@@ -3,10 +3,13 @@
 Workload (the forced-isotropic-turbulence configuration the metric is quoted
 on): N = 256^3 in a 2 pi box, seeded spectrum E(k) ~ k^4 exp(-2 k^2/k0^2) with
 k0 = 3 and E = 0.5, band forcing on |k| <= 2.5 with Pin = 0.1, nu = 2e-3,
-integrating-factor Heun step with CFL control at Courant 0.5, FP64 (the plain
-form; the FP32 form is reported beside it).  One "step" is one time step of
-the whole box.  Inputs (the spectral velocity) are synthetic and larger than
-L2 (3 x 135 MB in FP64).
+integrating-factor Heun step with CFL control at Courant 0.5.  The headline
+form is the tensor-core split-precision one (FP32 state, DFT-64 stages of the
+strided passes on tcgen05 with f16 hi + lo operands); the plain FP64 form and
+the FP32 SIMT form are timed beside it on the same seeded field, with the
+TC-split velocity error against FP64 after the timed steps, and the 512^3
+legs of all three.  One "step" is one time step of the whole box.  Inputs (the
+spectral velocity) are synthetic and larger than L2 (3 x 68 MB in FP32).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -30,7 +33,9 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-METRIC = "steps/s @256^3 forced turbulence (IF-Heun, CFL 0.5, band forcing), FP64 plain form"
+METRIC = ("steps/s @256^3 forced turbulence (IF-Heun, CFL 0.5, band forcing), tensor-core split-precision form "
+          "(FP64 and FP32 forms and 512^3 beside it)")
+DTYPE = {"fp64": "f64", "fp32": "f32", "tc_split": "f32 (f16 hi+lo tensor-core DFT stages, f32 accumulate)"}
 UNIT = "steps/s"
 WORKLOAD = dict(n=256, k0=3.0, nu=2e-3, kCutOff=2.5, Pin=0.1, courant=0.5, dt_max=1e-2, dt0=1e-3)
 
@@ -138,8 +143,9 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"forced isotropic turbulence {n}^3, IF-Heun, CFL 0.5, band forcing Pin 0.1",
-                   "n": n, "precision": "fp64"},
+        "config": {"workload": f"forced isotropic turbulence {n}^3, IF-Heun, CFL 0.5, band forcing Pin 0.1, "
+                               f"nu 2e-3, k0 3 (independent box per GPU)",
+                   "n": n, "precision": "fp64 (the reference's CPU arithmetic)", "parallelism": "rank 0 host cores"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{done} full Heun steps at {n}^3 ({el:.1f} s) of the NumPy/scipy.fft "
                                    f"restatement of rhs.f90 + dnsboxheun.f90 (the Fortran/MPI/p3dfft "
@@ -150,10 +156,11 @@ def run_reference(args, rank, world):
 
 
 # ----------------------------------------------------------------- our arm
-def make_box(n, precision, rank):
+def make_box(n, precision, rank, nu=None):
     from dnsbox_b200.ops import Box
     w = WORKLOAD
-    return Box(n, precision=precision, nu=w["nu"], kCutOff=w["kCutOff"], Pin=w["Pin"], bandlim=True,
+    return Box(n, precision=precision, nu=w["nu"] if nu is None else nu, kCutOff=w["kCutOff"], Pin=w["Pin"],
+               bandlim=True,
                courant_min=w["courant"], courant_max=w["courant"], dt_max=w["dt_max"], dt=w["dt0"],
                device=torch.cuda.current_device())
 
@@ -228,20 +235,21 @@ def profile_passes(box, u, k):
 
 
 def extra_sizes(args):
-    """Steps/s of the same forced workload at 512^3 (FP64 and FP32), seeded on
-    the device, K/2 steps after W warm-up steps each."""
+    """Steps/s of the same forced workload at 512^3 (nu 8e-4; FP64, FP32 and
+    TC-split), seeded on the device, K/2 steps after W warm-up steps each."""
     from dnsbox_b200 import ic
     out = {}
-    for prec in ("fp64", "fp32"):
-        box = make_box(512, prec, 0)
+    for prec in ("fp64", "fp32", "tc_split"):
+        box = make_box(512, prec, 0, nu=8e-4)
         u = ic.random_field_gpu(box, seed=0, k0=WORKLOAD["k0"])
         box.step(u, args.warmup, diag=False)
         k = max(2, args.steps // 2)
         ms = timed_steps(box, u, k, False)
-        out[f"{prec}_512"] = {"value": k / (ms / 1e3), "ms_per_step": ms / k, "steps": k}
+        out[f"{prec}_512"] = {"value": k / (ms / 1e3), "ms_per_step": ms / k, "steps": k, "nu": 8e-4}
         box.close()
         del u
         torch.cuda.empty_cache()
+    out["tc_split_vs_fp64_512"] = out["tc_split_512"]["value"] / out["fp64_512"]["value"]
     return out
 
 
@@ -321,6 +329,7 @@ def run_ours(args, rank, world, dist_on):
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     uh_np = ic.random_field(n, seed=rank, k0=WORKLOAD["k0"])
     results = {}
+    final = {}
     for prec in args.precisions:
         box = make_box(n, prec, rank)
         u = box.from_numpy(uh_np)
@@ -331,6 +340,8 @@ def run_ours(args, rank, world, dist_on):
         with sampler:
             ms = timed_steps(box, u, args.steps, dist_on)
         launches = box.profile_read(reset=True)["total_launches"]
+        if rank == 0 and prec in ("fp64", "tc_split", "fp32"):
+            final[prec] = u.to(torch.complex128).cpu()   # after W + K steps from the same field
         pr = profile_passes(box, u, args.steps)
         res = {"ms": ms, "launches": launches, "profile": pr, "clocks": sampler.summary()}
         if prec == args.precisions[0] and rank == 0:
@@ -368,7 +379,7 @@ def run_ours(args, rank, world, dist_on):
     line = {
         "metric": METRIC, "value": steps_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if main == "fp64" else "f32",
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[main],
         "data": "synthetic",
         "config": {"workload": f"forced isotropic turbulence {n}^3, IF-Heun, CFL 0.5, band forcing Pin 0.1, "
                                f"nu 2e-3, k0 3 (independent box per GPU)",
@@ -389,6 +400,14 @@ def run_ours(args, rank, world, dist_on):
     if e2e:
         line["e2e"] = {"value": e2e[0] * world, "unit": UNIT, "h2d_bytes_per_step": e2e[1],
                        "d2h_bytes_per_step": e2e[2]}
+    if "fp64" in final:
+        ref = final["fp64"]
+        line["accuracy_vs_fp64"] = {
+            p: {"steps": args.warmup + args.steps,
+                "vel_rel_l2": float((final[p] - ref).abs().norm() / ref.abs().norm())}
+            for p in final if p != "fp64"}
+    if "fp64" in results and main != "fp64":
+        line["speedup_vs_fp64"] = results["fp64"]["ms"] / r["ms"]
     for prec in args.precisions[1:]:
         rr = results[prec]
         prr = rr["profile"]
@@ -419,7 +438,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--precisions", default="fp64,fp32")
+    ap.add_argument("--precisions", default="tc_split,fp64,fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 512^3 and adjoint legs")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
