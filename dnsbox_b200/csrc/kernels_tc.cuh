@@ -27,7 +27,7 @@
 // whole persistent launch), X hi + lo (32 KB; the FP32 tile D of the combined
 // accumulators reuses it once the MMAs have completed, XOR-swizzled so that
 // the TMEM drain and the stage-2 reads are free of bank conflicts), 128 TMEM
-// columns and 256 threads, plus a 32 KB ring into which the next tile's first
+// columns and 512 threads, plus a 32 KB ring into which the next tile's first
 // input is copied asynchronously.  Two CTAs share an SM, and each fetches its
 // next tile while the current one is split, multiplied, drained and stored,
 // so the loads, MMAs and stores of different tiles overlap.
@@ -49,7 +49,8 @@ template <int N> struct TcPlan {
   static constexpr int B_PART = 64 * 128 * 2;      // bytes of one f16 64 x 128 X operand (Re | Im)
   static constexpr int TILE = 64 * 64 * 8;         // bytes of one FP32 complex tile (N x TCW)
   static constexpr int SMEM = 2 * A_PART + 2 * B_PART + TILE;
-  static constexpr int THREADS = 256;              // two 8-row runs of one pencil per thread
+  static constexpr int THREADS = 512;              // 8-row runs of one pencil: RUNS per thread
+  static constexpr int RUNS = 512 / THREADS;
   static constexpr int CTAS_PER_SM = 2;
   static constexpr int TMEM_COLS = 128;            // DR, DI: 64 columns each
 };
@@ -140,12 +141,12 @@ __device__ __forceinline__ TcItem tc_item(const StridedArgs<float> &a, const TcA
 }
 
 template <int N, bool INV>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
     k_strided_tc(const __grid_constant__ StridedArgs<float> a, const TcArgs g, const __half *__restrict__ Adft,
                  int *status) {
   using C = float2;
   using PL = TcPlan<N>;
-  constexpr int N2 = PL::N2, TCW = PL::TCW, LG_R = PL::LG_R, NT = PL::THREADS;
+  constexpr int N2 = PL::N2, TCW = PL::TCW, LG_R = PL::LG_R, NT = PL::THREADS, RUNS = PL::RUNS;
   constexpr int XIM = 1 << (4 - LG_R);   // swizzle bit flipped for imaginary rows
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char *sAh = smem_raw;
@@ -158,6 +159,7 @@ __global__ void __launch_bounds__(256, 2)
   __shared__ uint32_t taddr_s;
   __shared__ unsigned pmax_s[2][64];   // per-pencil max |Re|, |Im| bits, alternating tiles
   __shared__ int abort_s;
+  __shared__ float usc[64];            // this tile's per-pencil unscale factors 2^e
   __shared__ float krow[N];            // wavenumber of each row index along the transformed axis
   __shared__ StridedJob<float> sjob[6];   // the job table (read with a per-tile index)
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -185,19 +187,19 @@ __global__ void __launch_bounds__(256, 2)
   constexpr uint32_t idesc = tc::idesc_f16_f32(128, 64);
   uint32_t phase = 0;
   int slot = 0;
-  // Thread t owns, for h = 0, 1, the 8-row run u = t + 256 h of the tile:
+  // Thread t owns, for h < RUNS, the 8-row run u = t + NT h of the tile:
   // rows n = N2 (8q + i) + n2 (i < 8) of column c, with c = u % TCW,
   // n2 = (u / TCW) % N2, q = u / 64, i.e. pencil j = u % 64.  The next tile's
-  // first input is copied asynchronously into the thread's own 16 ring slots
-  // (slot (8 h + i) * 256 + t, consecutive across a warp; no barrier guards
+  // first input is copied asynchronously into the thread's own 8 RUNS ring
+  // slots (slot (8 h + i) * NT + t, consecutive across a warp; no barrier guards
   // the ring) and its second input, if any, is loaded into registers, both
   // while the current tile is processed.
-  C y[2][8];
+  C y[RUNS][8];
   auto fetch = [&](unsigned w) {
     const TcItem it = tc_item<TCW>(a, g, w);
     const StridedJob<float> &J = sjob[it.job];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < RUNS; ++h) {
       const int u = t + NT * h;
       const int c = u % TCW, n2 = (u / TCW) % N2, q = u / 64;
       const bool valid = it.kx0 + c < a.ncols;
@@ -219,10 +221,10 @@ __global__ void __launch_bounds__(256, 2)
     const TcItem it = tc_item<TCW>(a, g, w);
     const StridedJob<float> &J = sjob[it.job];
     unsigned *pmax = pmax_s[slot];
-    C v[2][8];
+    C v[RUNS][8];
     cp_async_wait_all();
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+    for (int h = 0; h < RUNS; ++h)
 #pragma unroll
       for (int i = 0; i < 8; ++i) v[h][i] = ring[(8 * h + i) * NT + t];
     // 1. the second input and the job multipliers x (a + i b k), in FP32
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(256, 2)
       const float a1 = (float)J.a1, b1 = (float)J.b1, a2 = (float)J.a2, b2 = (float)J.b2;
       const float koth = a.n_other ? (float)k_full(it.other, a.n_other, a.alpha_other) : 0.f;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < RUNS; ++h) {
         const int u = t + NT * h;
         const int c = u % TCW, n2 = (u / TCW) % N2, q = u / 64;
         const float kcol = (float)k_half(it.kx0 + c, a.nx, a.alpha_x);
@@ -252,18 +254,21 @@ __global__ void __launch_bounds__(256, 2)
       }
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < RUNS; ++h) {
       float m = 0.f;
 #pragma unroll
       for (int i = 0; i < 8; ++i) m = fmaxf(m, fmaxf(fabsf(v[h][i].x), fabsf(v[h][i].y)));
       atomicMax(&pmax[(t + NT * h) % 64], __float_as_uint(m));   // non-negative floats order as unsigned
     }
     __syncthreads();
-    if (t < 64) pmax_s[slot ^ 1][t] = 0u;   // for the next tile (its atomics follow the end barrier)
+    if (t < 64) {
+      pmax_s[slot ^ 1][t] = 0u;   // for the next tile (its atomics follow the end barrier)
+      usc[t] = __int_as_float((127 + tc_exp(pmax[t])) << 23);   // 2^e, read back in stage 2
+    }
     // 2. scale, split into f16 hi + lo, 16-byte stores of 8 consecutive K
     //    (K = n1 for the real parts, 64 + n1 for the imaginary parts)
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < RUNS; ++h) {
       const int u = t + NT * h;
       const int j = u % 64, q = u / 64;
       const float sc = __int_as_float((127 - tc_exp(pmax[j])) << 23);   // 2^-e
@@ -310,28 +315,31 @@ __global__ void __launch_bounds__(256, 2)
     // the next tile is fetched while the tensor core runs (after the proxy
     // fence above, which would otherwise wait for these copies)
     if (w + gridDim.x < (unsigned)g.total) fetch(w + gridDim.x);
-    if (!tc::mbar_wait_bounded(&mbar, phase, kTcWaitLimit)) abort_s = 1;
+    // one thread polls the MMA completion (the others wait at the barrier,
+    // which costs no issue slots or shared-memory accesses)
+    if (t == 0 && !tc::mbar_wait_bounded(&mbar, phase, kTcWaitLimit)) abort_s = 1;
     tc::fence_after_sync();
     __syncthreads();
     if (abort_s) break;
     phase ^= 1u;
-    // 4. drain: warp w reads TMEM lanes 32 (w % 4) + lane, columns 32 (w / 4) .. + 31,
-    //    of DR and DI; lane pair (2k, 2k + 1) forms Re y[k] and Im y[k]
+    // 4. drain: warp w reads TMEM lanes 32 (w % 4) + lane and DCOL columns from
+    //    DCOL (w / 4) of DR and DI; lane pair (2k, 2k + 1) forms Re y[k] and Im y[k]
     {
+      constexpr int DCOL = 64 / (NT / 128);   // columns per warp
       const int k1 = 16 * (warp & 3) + (lane >> 1);
       const bool odd = lane & 1;
       const int sw = tc_swz<LG_R>(k1) ^ (odd ? XIM : 0);
       float *row = sD + (odd ? 64 + k1 : k1) * 64;
       const uint32_t ta = taddr + ((uint32_t)(32 * (warp & 3)) << 16);
 #pragma unroll
-      for (int half = 0; half < 2; ++half) {
-        const int c0 = 32 * (warp >> 2) + 16 * half;
-        float dr[16], di[16];
-        tc::tmem_ld16(ta + (uint32_t)c0, dr);
-        tc::tmem_ld16(ta + 64u + (uint32_t)c0, di);
+      for (int part = 0; part < DCOL / 8; ++part) {
+        const int c0 = DCOL * (warp >> 2) + 8 * part;
+        float dr[8], di[8];
+        tc::tmem_ld8(ta + (uint32_t)c0, dr);
+        tc::tmem_ld8(ta + 64u + (uint32_t)c0, di);
         tc::tmem_ld_wait();
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
+        for (int k = 0; k < 8; ++k) {
           const float dip = __shfl_xor_sync(0xffffffffu, di[k], 1);
           row[(c0 + k) ^ sw] = odd ? dr[k] + dip : dr[k] - dip;
         }
@@ -348,7 +356,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
       for (int m2 = 0; m2 < N2; ++m2) {
         const int jj = m2 * TCW + cc;
-        const float us = __int_as_float((127 + tc_exp(pmax[jj])) << 23);
+        const float us = usc[jj];
         C yy = mkc<C>(sD[k1 * 64 + (jj ^ sw)] * us, sD[(64 + k1) * 64 + (jj ^ swi)] * us);
         if (m2) {
           const C tw = __ldg(&a.tw[m2 * k1]);
@@ -366,10 +374,10 @@ __global__ void __launch_bounds__(256, 2)
     __syncthreads();
   }
   cp_async_wait_all();
-  if (abort_s) {
+  if (abort_s && t == 0) {
     // give the outstanding MMAs a second bounded wait before their TMEM is freed
     tc::mbar_wait_bounded(&mbar, phase, kTcWaitLimit);
-    if (t == 0) atomicExch(status, 1);
+    atomicExch(status, 1);
   }
   tc::fence_before_sync();
   __syncthreads();
