@@ -253,6 +253,31 @@ def extra_sizes(args):
     return out
 
 
+def tc_1024_rate(args):
+    """Config 4's large case: 1024^3 forced turbulence in the TC-split form
+    (FP32 state, nu 4e-4), seeded on the device; steps/s over K/4 steps after
+    W warm-up steps, with the largest energy-budget residual
+    |dE/dt - (Pin - D)| over the timed steps."""
+    from dnsbox_b200 import ic
+    box = make_box(1024, "tc_split", 0, nu=4e-4)
+    u = ic.random_field_gpu(box, seed=0, k0=WORKLOAD["k0"])
+    torch.cuda.empty_cache()
+    box.step(u, args.warmup, diag=False)
+    k = max(2, args.steps // 4)
+    ms = timed_steps(box, u, k, False)
+    e0 = box.kinetic(u)
+    recs = box.step(u, 3)
+    es = [e0] + [r["ekin"] for r in recs]
+    resid = max(abs((es[i + 1] - es[i]) / recs[i]["dt"]
+                    - (WORKLOAD["Pin"] - 0.5 * (recs[i - 1]["dissipation"] + recs[i]["dissipation"])))
+                for i in range(1, len(recs)))
+    box.close()
+    del u
+    torch.cuda.empty_cache()
+    return {"value": k / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / k, "steps": k, "nu": 4e-4,
+            "energy_budget_residual": resid, "memory_gb": 18 * 1024 ** 2 * 513 * 8 / 1e9}
+
+
 def adjoint_rate(iters=40):
     """Adjoint-descent iterations/s on the 64^3 Kolmogorov residual (FP32 bulk,
     FP64 J and line search, nu = 1/40, F = 1, kf = 4)."""
@@ -420,6 +445,7 @@ def run_ours(args, rank, world, dist_on):
                        for k, f in PASS_FIELDS_HEUN.items() if prr["launches"][k]}}
     if world == 1 and not args.no_extra:
         line["extra"] = extra_sizes(args)
+        line["extra"]["tc_split_1024"] = tc_1024_rate(args)
         line["extra"]["adjoint_descent_64"] = adjoint_rate()
         line["extra"]["ensemble_96"] = ensemble_rate()
     if world == 1 and not args.no_cpu_baseline:

@@ -343,3 +343,25 @@ def test_rhs_nonlinear_512_properties():
     b64 = box(n, "fp64", bandlim=False)
     N64, _ = b64.rhs_nonlinear(host.to(b64.device))
     assert float((N32.to(torch.complex128) - N64).abs().norm() / N64.abs().norm()) < 2e-5
+
+
+# ---------------------------------------------------------------- 1024-point axes
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "tc_split"])
+@pytest.mark.parametrize("shape", [(1024, 16, 16), (16, 1024, 16), (16, 16, 1024)])
+def test_axes_of_1024(prec, shape):
+    """Every pass at its largest size on small boxes (one axis of 1024): the
+    transforms against pocketfft and one right-hand side against the oracle."""
+    nx, ny, nz = shape
+    from dnsbox_b200.ops import Box
+    b = Box(nx=nx, ny=ny, nz=nz, precision=prec, nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True)
+    p = O.Params(nx=nx, ny=ny, nz=nz, nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True)
+    g = O.Grid(p)
+    rng = np.random.default_rng(11)
+    f = rng.standard_normal((nz, ny, nx))
+    F = g.r2c(f)
+    t = 1e-13 if prec == "fp64" else 2e-6
+    assert rel(b.r2c(torch.from_numpy(f).to(b.device, b.rdtype)).cpu().numpy(), F) < t
+    assert rel(b.c2r(torch.from_numpy(F).to(b.device, b.cdtype)).cpu().numpy(), g.c2r(F)) < t
+    uh = O.state_dealias(g, O.state_project(g, O.state_u2uhat(g, rng.standard_normal((3, nz, ny, nx)))))
+    got, _ = b.rhs_nonlinear(b.from_numpy(uh))
+    assert rel(got.cpu().numpy(), O.rhs_nonlinear(g, uh)) < tol("fp64" if prec == "fp64" else "fp32")
