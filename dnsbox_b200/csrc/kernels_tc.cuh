@@ -195,8 +195,10 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
   // the ring) and its second input, if any, is loaded into registers, both
   // while the current tile is processed.
   C y[RUNS][8];
+  TcItem nxt;   // decoded work item of the tile being fetched
   auto fetch = [&](unsigned w) {
-    const TcItem it = tc_item<TCW>(a, g, w);
+    nxt = tc_item<TCW>(a, g, w);
+    const TcItem &it = nxt;
     const StridedJob<float> &J = sjob[it.job];
 #pragma unroll
     for (int h = 0; h < RUNS; ++h) {
@@ -218,8 +220,8 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
   };
   if (blockIdx.x < (unsigned)g.total) fetch(blockIdx.x);   // (sjob is visible: init barrier above)
   for (unsigned w = blockIdx.x; w < (unsigned)g.total; w += gridDim.x, slot ^= 1) {
-    const TcItem it = tc_item<TCW>(a, g, w);
-    const StridedJob<float> &J = sjob[it.job];
+    const TcItem it = nxt;   // decoded by the fetch of this tile
+    const StridedJob<float> J = sjob[it.job];   // job fields in registers for the tile
     unsigned *pmax = pmax_s[slot];
     C v[RUNS][8];
     cp_async_wait_all();
