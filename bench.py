@@ -278,6 +278,29 @@ def tc_1024_rate(args):
             "energy_budget_residual": resid, "memory_gb": 18 * 1024 ** 2 * 513 * 8 / 1e9}
 
 
+def orbit_rate():
+    """Periodic-orbit variant of the adjoint configuration: seconds per J and
+    gradient of J = 1/2 <|u(T) - u(0)|^2> at 96^3, T = 5 (500 fixed steps of
+    dt = 1e-2, Kolmogorov forcing, nu = 1/40, FP32 bulk, FP64 J), checkpoints
+    every 32 steps."""
+    from dnsbox_b200 import ic
+    from dnsbox_b200.ops import Box
+    n, ns = 96, 500
+    box = Box(n, precision="fp32", nu=1.0 / 40.0, bandlim=False, tstep_fix=True, dt=1e-2)
+    f = box.from_numpy(ic.kolmogorov_forcing(n, 1.0, 4))
+    box.set_forcing(f)
+    u = box.from_numpy(ic.random_field(n, seed=0, k0=4.0))
+    box.step(u, ns, diag=False)
+    box.orbit_residual(u, 20, every=32)   # warm-up (allocates the checkpoint arena)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, _ = box.orbit_residual(u, ns, every=32)
+    el = time.perf_counter() - t0
+    box.close()
+    return {"value": 1.0 / el, "unit": "gradients/s", "seconds_per_gradient": el, "n": n, "steps": ns,
+            "checkpoint_every": 32, "J": J}
+
+
 def adjoint_rate(iters=40):
     """Adjoint-descent iterations/s on the 64^3 Kolmogorov residual (FP32 bulk,
     FP64 J and line search, nu = 1/40, F = 1, kf = 4)."""
@@ -447,6 +470,7 @@ def run_ours(args, rank, world, dist_on):
         line["extra"] = extra_sizes(args)
         line["extra"]["tc_split_1024"] = tc_1024_rate(args)
         line["extra"]["adjoint_descent_64"] = adjoint_rate()
+        line["extra"]["periodic_orbit_grad_96"] = orbit_rate()
         line["extra"]["ensemble_96"] = ensemble_rate()
     if world == 1 and not args.no_cpu_baseline:
         from oracle import dnsbox_oracle as O

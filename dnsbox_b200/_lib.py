@@ -105,6 +105,9 @@ SIGNATURES = {
     "dnsbox_residual": (ctypes.c_int, [_VP, _VP, _DP]),
     "dnsbox_residual_grad": (ctypes.c_int, [_VP, _VP, _VP, _DP]),
     "dnsbox_adjoint_descent": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _DP, _DP]),
+    "dnsbox_heun_step_vjp": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "dnsbox_heun_steps_vjp": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
+    "dnsbox_orbit_residual": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _DP]),
     "dnsbox_batch_size": (ctypes.c_int, [_VP]),
     "dnsbox_set_batch_nu": (ctypes.c_int, [_VP, _DP]),
     "dnsbox_diag_read": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(Diag)]),

@@ -1,4 +1,5 @@
-"""torch.autograd bindings of the nonlinear term and of the residual J.
+"""torch.autograd bindings of the nonlinear term, the residual J and the
+time stepper.
 
 ``rhs_nonlinear(box, uhat)`` is differentiable: its backward is the exact
 adjoint kernel chain of libdnsbox_gpu.so (``dnsbox_rhs_nonlinear_vjp``), the
@@ -48,3 +49,27 @@ class Residual(torch.autograd.Function):
 
 def residual(box, uh: torch.Tensor) -> torch.Tensor:
     return Residual.apply(uh, box)
+
+
+class HeunSteps(torch.autograd.Function):
+    """u(T) = S^nsteps(u0) for fixed-dt IF-Heun steps; the backward is the
+    checkpointed step-transpose chain (dnsbox_heun_steps_vjp)."""
+
+    @staticmethod
+    def forward(ctx, u0, box, nsteps, every):
+        u = u0.detach().contiguous().clone()
+        box.step(u, nsteps, diag=False)
+        ctx.box, ctx.nsteps, ctx.every = box, nsteps, every
+        ctx.save_for_backward(u0)
+        return u
+
+    @staticmethod
+    def backward(ctx, gT):
+        (u0,) = ctx.saved_tensors
+        g0 = ctx.box.heun_steps_vjp(u0.detach().contiguous(), ctx.nsteps, gT.contiguous(), every=ctx.every)
+        return g0, None, None, None
+
+
+def heun_steps(box, u0: torch.Tensor, nsteps: int, every: int = 32) -> torch.Tensor:
+    """Differentiable state after nsteps fixed-dt IF-Heun steps from u0."""
+    return HeunSteps.apply(u0, box, nsteps, every)

@@ -16,6 +16,15 @@
 //  dnsbox_residual(_grad)    J = 1/2 s^2 sum_half W h |r|^2 with r = L u + N(u) + f
 //                            (h = 1/(1+|k|^2) when hminone), and its gradient.
 //  dnsbox_adjoint_descent    steepest descent on J with an FP64 Armijo line search.
+//  dnsbox_heun_step_vjp      transpose of one fixed-dt IF-Heun step
+//                              S(u) = IF u + dt/2 IF N(u) + dt/2 N(u*), u* = IF (u + dt N(u)):
+//                              a = N'(u*)^T (dt/2 g),
+//                              S'(u)^T g = IF (g + a) + N'(u)^T (IF (dt/2 g + dt a)).
+//  dnsbox_heun_steps_vjp     the transpose of nsteps such steps, with the states
+//                            recomputed per segment from checkpoints taken every
+//                            `every` steps (memory: nsteps/every + every states).
+//  dnsbox_orbit_residual     J = 1/2 <(u(T) - u(0))^2> (physical mean square) of the
+//                            periodic-orbit problem and its gradient (Phi'^T - I)(s^2 W r).
 //
 // W is the half-spectrum multiplicity (1 on the kx = 0 and Nyquist planes, 2
 // elsewhere); L = Q - nu |k|^2 (the reference's nu (k.k) + Q with imaginary k).
@@ -313,6 +322,81 @@ __global__ void k_axpy(const C *x, const C *d, C *y, long long n, double alpha) 
   }
 }
 
+// out = IF (u + dt n), IF = exp((Q - nu |k|^2) dt): the FIN_PRED arithmetic of k_zfinish
+template <typename C>
+__global__ void k_if_pred(const C *u, const C *n, C *out, long long nh, Grid3 gr, double nu, double Q, double dt) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    const T IF = T(exp((Q - nu * (kx * kx + ky * ky + kz * kz)) * dt));
+    const T tdt = T(dt);
+    for (int c = 0; c < 3; ++c) {
+      const C a = u[c * nh + m], b = n[c * nh + m];
+      out[c * nh + m] = mkc<C>((a.x + tdt * b.x) * IF, (a.y + tdt * b.y) * IF);
+    }
+  }
+}
+
+// y = s x over n complex values
+template <typename C>
+__global__ void k_scale(const C *x, C *y, long long n, double s) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(i, n) {
+    const C a = x[i];
+    y[i] = mkc<C>(T(s * a.x), T(s * a.y));
+  }
+}
+
+// partial = IF (g + a), arg = IF (dt/2 g + dt a)
+template <typename C>
+__global__ void k_step_mix(const C *g, const C *a, C *partial, C *arg, long long nh, Grid3 gr, double nu, double Q,
+                           double dt) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    const double IF = exp((Q - nu * (kx * kx + ky * ky + kz * kz)) * dt);
+    for (int c = 0; c < 3; ++c) {
+      const C gg = g[c * nh + m], aa = a[c * nh + m];
+      partial[c * nh + m] = mkc<C>(T(IF * ((double)gg.x + aa.x)), T(IF * ((double)gg.y + aa.y)));
+      arg[c * nh + m] = mkc<C>(T(IF * (0.5 * dt * gg.x + dt * aa.x)), T(IF * (0.5 * dt * gg.y + dt * aa.y)));
+    }
+  }
+}
+
+// y += x over n complex values
+template <typename C>
+__global__ void k_accum(C *y, const C *x, long long n, double sx) {
+  using T = decltype(C{}.x);
+  GRID_LOOP(i, n) {
+    const C a = y[i], b = x[i];
+    y[i] = mkc<C>(T(a.x + sx * b.x), T(a.y + sx * b.y));
+  }
+}
+
+// r = uT - u0, g = s^2 W r, per-block partial sums of 1/2 s^2 W |r|^2
+template <typename C>
+__global__ void k_orbit_res(const C *uT, const C *u0, C *g, long long nh, Grid3 gr, double s2, double *partials) {
+  using T = decltype(C{}.x);
+  __shared__ double red[32];
+  double acc = 0.0;
+  GRID_LOOP(m, nh) {
+    double kx, ky, kz;
+    mode_k(gr, m, kx, ky, kz);
+    const double w = (kx == 0.0) ? 1.0 : 2.0;   // half-spectrum multiplicity (kx = 0 and Nyquist planes: 1)
+    for (int c = 0; c < 3; ++c) {
+      const C a = uT[c * nh + m], b = u0[c * nh + m];
+      const double re = (double)a.x - b.x, im = (double)a.y - b.y;
+      acc += 0.5 * s2 * w * (re * re + im * im);
+      g[c * nh + m] = mkc<C>(T(s2 * w * re), T(s2 * w * im));
+    }
+  }
+  double v[1] = {acc};
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
 constexpr int kRedBlocks = 148 * 2;
 
 Grid3 grid3(const dnsbox_ctx *c) {
@@ -532,7 +616,163 @@ int descent_impl(dnsbox_ctx *c, void *uh, int niter, double *Jhist, double *alph
   return DNSBOX_OK;
 }
 
+// Checks that a context can be differentiated step by step: one box, IF-Heun,
+// fixed dt (the CFL rule makes dt depend on max |u_i|, which has no useful
+// derivative).
+int step_vjp_ok(dnsbox_ctx *c) {
+  if (c->nbatch > 1) return set_err(DNSBOX_ERR_UNSUPPORTED, "not available on a batched context");
+  if (c->p.stepper != DNSBOX_HEUN) return set_err(DNSBOX_ERR_UNSUPPORTED, "step transpose needs the Heun stepper");
+  if (!c->p.tstep_fix) return set_err(DNSBOX_ERR_UNSUPPORTED, "step transpose needs a fixed time step (tstep_fix)");
+  return DNSBOX_OK;
+}
+
+// One step transpose: out = S'(u)^T g.  Arena spectral slots 21-32 (0-5 belong
+// to the rhs VJP).  out may not alias u or g.
+template <typename T>
+int step_vjp_impl(dnsbox_ctx *c, const void *uh, const void *g, void *out, double dt) {
+  using C = typename CT<T>::type;
+  const dnsbox_params &p = c->p;
+  const size_t sb = c->nh * sizeof(C);
+  char *P = nullptr, *S = nullptr;
+  RET(ensure_adj(c, 9, 33, &P, &S));
+  char *n0 = S + 21 * sb, *ust = S + 24 * sb, *A = S + 27 * sb, *tmp = S + 30 * sb;
+  const Grid3 gr = grid3(c);
+  const long long nh = (long long)c->nh, n3 = 3 * nh;
+  {
+    const int rc = dnsbox_rhs_nonlinear(c, uh, n0, nullptr);
+    if (rc != DNSBOX_OK) return rc;
+  }
+  k_if_pred<C><<<grid_for(nh), 256, 0, c->stream>>>(reinterpret_cast<const C *>(uh), reinterpret_cast<const C *>(n0),
+                                                     reinterpret_cast<C *>(ust), nh, gr, p.nu, p.Q, dt);
+  k_scale<C><<<grid_for(n3), 256, 0, c->stream>>>(reinterpret_cast<const C *>(g), reinterpret_cast<C *>(tmp), n3,
+                                                   0.5 * dt);
+  CK(cudaGetLastError());
+  RET(vjp_impl<T>(c, ust, tmp, A));                       // a = N'(u*)^T (dt/2 g)
+  k_step_mix<C><<<grid_for(nh), 256, 0, c->stream>>>(reinterpret_cast<const C *>(g), reinterpret_cast<const C *>(A),
+                                                      reinterpret_cast<C *>(out), reinterpret_cast<C *>(tmp), nh, gr,
+                                                      p.nu, p.Q, dt);
+  CK(cudaGetLastError());
+  RET(vjp_impl<T>(c, uh, tmp, n0));                       // N'(u)^T (IF (dt/2 g + dt a))
+  k_accum<C><<<grid_for(n3), 256, 0, c->stream>>>(reinterpret_cast<C *>(out), reinterpret_cast<const C *>(n0), n3,
+                                                   1.0);
+  CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+int ensure_orbit(dnsbox_ctx *c, size_t bytes) {
+  if (bytes <= c->orbit_bytes) return DNSBOX_OK;
+  if (c->orbit) cudaFree(c->orbit);
+  c->orbit = nullptr;
+  c->orbit_bytes = 0;
+  CK(cudaMalloc(&c->orbit, bytes));
+  c->orbit_bytes = bytes;
+  return DNSBOX_OK;
+}
+
+// g0 = (Phi^nsteps)'(u0)^T gT, checkpoints every `every` steps.  Also leaves
+// u(T) in *uT_out when non-null.  States advance with dnsbox_step, the
+// library's fused step.
+template <typename T>
+int steps_vjp_impl(dnsbox_ctx *c, const void *u0, int nsteps, int every, const void *gT, void *g0, void *uT_out) {
+  using C = typename CT<T>::type;
+  const size_t sb3 = 3 * c->nh * sizeof(C);
+  const int ncp = (nsteps + every - 1) / every;
+  RET(ensure_orbit(c, (size_t)(ncp + every + 2) * sb3));
+  char *cp = c->orbit, *seg = cp + (size_t)ncp * sb3, *ga = seg + (size_t)every * sb3, *gb = ga + sb3;
+  double dt = 0.0;
+  RET(dnsbox_get_dt(c, &dt));
+  // forward sweep: checkpoints
+  CK(cudaMemcpyAsync(seg, u0, sb3, cudaMemcpyDeviceToDevice, c->stream));
+  for (int n = 0; n < nsteps; ++n) {
+    if (n % every == 0) CK(cudaMemcpyAsync(cp + (size_t)(n / every) * sb3, seg, sb3, cudaMemcpyDeviceToDevice, c->stream));
+    RET(dnsbox_step(c, seg, 1, nullptr));
+  }
+  if (uT_out) CK(cudaMemcpyAsync(uT_out, seg, sb3, cudaMemcpyDeviceToDevice, c->stream));
+  // backward sweep, one segment at a time
+  CK(cudaMemcpyAsync(ga, gT, sb3, cudaMemcpyDeviceToDevice, c->stream));
+  for (int k = ncp - 1; k >= 0; --k) {
+    const int n0 = k * every, len = (nsteps - n0 < every) ? nsteps - n0 : every;
+    CK(cudaMemcpyAsync(seg, cp + (size_t)k * sb3, sb3, cudaMemcpyDeviceToDevice, c->stream));
+    for (int j = 1; j < len; ++j) {
+      CK(cudaMemcpyAsync(seg + (size_t)j * sb3, seg + (size_t)(j - 1) * sb3, sb3, cudaMemcpyDeviceToDevice,
+                         c->stream));
+      RET(dnsbox_step(c, seg + (size_t)j * sb3, 1, nullptr));
+    }
+    for (int j = len - 1; j >= 0; --j) {
+      RET(step_vjp_impl<T>(c, seg + (size_t)j * sb3, ga, gb, dt));
+      char *t = ga;
+      ga = gb;
+      gb = t;
+    }
+  }
+  CK(cudaMemcpyAsync(g0, ga, sb3, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DNSBOX_OK;
+}
+
+// J = 1/2 s^2 sum_half W |u(T) - u0|^2 and, when grad != null, (Phi'^T - I)(s^2 W r).
+template <typename T>
+int orbit_impl(dnsbox_ctx *c, const void *u0, int nsteps, int every, void *grad, double *J) {
+  using C = typename CT<T>::type;
+  const size_t sb = c->nh * sizeof(C);
+  char *P = nullptr, *S = nullptr;
+  RET(ensure_adj(c, 9, 39, &P, &S));
+  char *uT = S + 33 * sb, *gc = S + 36 * sb;
+  const Grid3 gr = grid3(c);
+  const long long nh = (long long)c->nh;
+  const double s = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz);
+  CK(cudaMemcpyAsync(uT, u0, 3 * sb, cudaMemcpyDeviceToDevice, c->stream));
+  RET(dnsbox_step(c, uT, nsteps, nullptr));
+  RET(ensure_red(c, kRedBlocks + 1));
+  k_orbit_res<C><<<kRedBlocks, 256, 0, c->stream>>>(reinterpret_cast<const C *>(uT), reinterpret_cast<const C *>(u0),
+                                                     reinterpret_cast<C *>(gc), nh, gr, s * s, c->red);
+  CK(cudaGetLastError());
+  RET(sum_to_host(c, kRedBlocks, J));
+  if (grad) {
+    RET(steps_vjp_impl<T>(c, u0, nsteps, every, gc, grad, nullptr));
+    k_accum<C><<<grid_for(3 * nh), 256, 0, c->stream>>>(reinterpret_cast<C *>(grad), reinterpret_cast<const C *>(gc),
+                                                         3 * nh, -1.0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return DNSBOX_OK;
+}
+
 }  // namespace
+
+extern "C" int dnsbox_heun_step_vjp(dnsbox_ctx *ctx, const void *uh, const void *g, void *out) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!uh || !g || !out) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  if (out == uh || out == g) return set_err(DNSBOX_ERR_ARG, "output may not alias an input");
+  RET(step_vjp_ok(ctx));
+  double dt = 0.0;
+  RET(dnsbox_get_dt(ctx, &dt));
+  return ctx->fp64 ? step_vjp_impl<double>(ctx, uh, g, out, dt) : step_vjp_impl<float>(ctx, uh, g, out, dt);
+}
+
+extern "C" int dnsbox_heun_steps_vjp(dnsbox_ctx *ctx, const void *u0, int nsteps, int every, const void *gT,
+                                     void *g0, void *uT) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!u0 || !gT || !g0) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  if (nsteps < 1 || every < 1) return set_err(DNSBOX_ERR_ARG, "nsteps and every must be positive");
+  RET(step_vjp_ok(ctx));
+  return ctx->fp64 ? steps_vjp_impl<double>(ctx, u0, nsteps, every, gT, g0, uT)
+                   : steps_vjp_impl<float>(ctx, u0, nsteps, every, gT, g0, uT);
+}
+
+extern "C" int dnsbox_orbit_residual(dnsbox_ctx *ctx, const void *u0, int nsteps, int every, void *grad,
+                                     double *J) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!u0 || !J) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  if (nsteps < 1 || every < 1) return set_err(DNSBOX_ERR_ARG, "nsteps and every must be positive");
+  if (grad == u0) return set_err(DNSBOX_ERR_ARG, "output may not alias the input");
+  RET(step_vjp_ok(ctx));
+  return ctx->fp64 ? orbit_impl<double>(ctx, u0, nsteps, every, grad, J)
+                   : orbit_impl<float>(ctx, u0, nsteps, every, grad, J);
+}
 
 extern "C" int dnsbox_rhs_nonlinear_vjp(dnsbox_ctx *ctx, const void *uh, const void *g, void *out) {
   if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");

@@ -609,6 +609,7 @@ static void free_ctx(dnsbox_ctx *c) {
   cudaFree(c->band);
   cudaFree(c->ddiag);
   cudaFree(c->adj);
+  cudaFree(c->orbit);
   cudaFree(c->d_nu);
   if (c->hstage) cudaFreeHost(c->hstage);
   delete c;

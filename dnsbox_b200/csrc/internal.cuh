@@ -70,6 +70,8 @@ struct dnsbox_ctx {
   int tc_ctas = 0;                       // persistent grid of the tensor-core passes
   char *adj = nullptr;                   // adjoint arena
   size_t adj_bytes = 0;
+  char *orbit = nullptr;                 // checkpoints and segment states of the step-transpose chain
+  size_t orbit_bytes = 0;
   // measurement
   int prof_on = 0;
   std::vector<cudaEvent_t> ev_pool;      // pairs

@@ -287,6 +287,41 @@ class Box:
                                                     hist.ctypes.data_as(_lib._DP), ctypes.byref(a)))
         return hist, a.value
 
+    # ------------------------------------------------------- time-horizon gradients
+    def heun_step_vjp(self, uh, g):
+        """Transpose of one fixed-dt IF-Heun step linearised at uh, applied to g."""
+        self._check_state(uh)
+        g = g.contiguous()
+        self._check_state(g, "g")
+        out = torch.empty_like(uh)
+        self._sync_stream()
+        _lib.check(self._lib.dnsbox_heun_step_vjp(self._h, _ptr(uh), _ptr(g), _ptr(out)))
+        return out
+
+    def heun_steps_vjp(self, u0, nsteps, gT, every=32, want_uT=False):
+        """Transpose of nsteps fixed-dt IF-Heun steps from u0 applied to gT, with
+        checkpoints every `every` steps; returns g0 (and u(T) when want_uT)."""
+        self._check_state(u0)
+        gT = gT.contiguous()
+        self._check_state(gT, "gT")
+        g0 = torch.empty_like(u0)
+        uT = torch.empty_like(u0) if want_uT else None
+        self._sync_stream()
+        _lib.check(self._lib.dnsbox_heun_steps_vjp(self._h, _ptr(u0), int(nsteps), int(every), _ptr(gT),
+                                                   _ptr(g0), _ptr(uT) if uT is not None else None))
+        return (g0, uT) if want_uT else g0
+
+    def orbit_residual(self, u0, nsteps, every=32, grad=True):
+        """Periodic-orbit residual J = 1/2 <|u(T) - u0|^2> (T = nsteps dt) and,
+        with grad, its gradient; returns J or (J, grad)."""
+        self._check_state(u0)
+        gr = torch.empty_like(u0) if grad else None
+        self._sync_stream()
+        v = ctypes.c_double()
+        _lib.check(self._lib.dnsbox_orbit_residual(self._h, _ptr(u0), int(nsteps), int(every),
+                                                   _ptr(gr) if gr is not None else None, ctypes.byref(v)))
+        return (v.value, gr) if grad else v.value
+
     # ---------------------------------------------------------------- transforms
     def c2r(self, spec: torch.Tensor) -> torch.Tensor:
         """Unnormalised 3D C2R of one spectral field (nz, ny, nxh)."""

@@ -213,6 +213,26 @@ int dnsbox_residual_grad(dnsbox_ctx *ctx, const void *uhat3_dev, void *grad3_dev
  * step length) may be NULL. */
 int dnsbox_adjoint_descent(dnsbox_ctx *ctx, void *uhat3_dev, int niter, double *J_host, double *alpha_io);
 
+/* ---- time-horizon gradients (the periodic-orbit variant of the adjoint
+ *      configuration; no reference counterpart: the reference's adjoint
+ *      (dnsboxAdj.f90) descends on the instantaneous residual only).  All
+ *      three need one box, the Heun stepper and a fixed time step (tstep_fix);
+ *      they advance states with dnsbox_step, so the context's clock moves. -- */
+/* out = S'(u)^T g for one IF-Heun step S of the current dt (dnsboxheun.f90:85-126
+ * linearised at uhat), Euclidean on Re/Im of the half spectrum; out may not
+ * alias an input. */
+int dnsbox_heun_step_vjp(dnsbox_ctx *ctx, const void *uhat3_dev, const void *g3_dev, void *out3_dev);
+/* g0 = (S^nsteps)'(u0)^T gT, with the states recomputed per segment from
+ * checkpoints taken every `every` steps (device memory: nsteps/every + every + 2
+ * states, held by the context).  uT3_dev (may be NULL) receives u(T). */
+int dnsbox_heun_steps_vjp(dnsbox_ctx *ctx, const void *u0_3_dev, int nsteps, int every, const void *gT3_dev,
+                          void *g0_3_dev, void *uT3_dev);
+/* J = 1/2 <|u(T) - u0|^2> (mean square over the physical grid, FP64) with
+ * T = nsteps dt, and, when grad3_dev is not NULL, its gradient
+ * ((S^nsteps)'^T - I)(s^2 W r), checkpointed every `every` steps. */
+int dnsbox_orbit_residual(dnsbox_ctx *ctx, const void *u0_3_dev, int nsteps, int every, void *grad3_dev,
+                          double *J);
+
 /* ---- batched boxes and ensembles (SURVEY config 2: independent boxes of
  *      mixed N and nu; no reference counterpart -- the reference runs one box
  *      per MPI job).  A context created with nbatch > 1 holds nbatch boxes of

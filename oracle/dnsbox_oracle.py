@@ -220,13 +220,19 @@ def rhs_nonlinear(g: Grid, uh, return_eband=False):
 
 
 # ================================================================ steppers
-def heun_step(g: Grid, uh, dt):
-    """dnsboxheun.f90:85-126: IF predictor-corrector (Heun)."""
+def heun_step(g: Grid, uh, dt, force=None):
+    """dnsboxheun.f90:85-126: IF predictor-corrector (Heun).  ``force`` is an
+    optional fixed spectral forcing added to N (the Kolmogorov forcing of the
+    adjoint configuration; not in the reference)."""
     IF = rhs_int_fact(g, dt)
     n1 = rhs_nonlinear(g, uh)                               # :85
+    if force is not None:
+        n1 = n1 + force
     ut = IF * (uh + dt * n1)                                # :91-92
     un = IF * (uh + dt * n1 * 0.5)                          # :95-96
     n2 = rhs_nonlinear(g, ut)                               # :117
+    if force is not None:
+        n2 = n2 + force
     return un + dt * n2 * 0.5                               # :122-124
 
 
@@ -508,6 +514,42 @@ def rhs_nonlinear_vjp(g: Grid, uh, gout):
     curl_t = np.stack([k[1] * psi[2] - k[2] * psi[1], k[2] * psi[0] - k[0] * psi[2],
                        k[0] * psi[1] - k[1] * psi[0]])
     return curl_t + grad_u
+
+
+def heun_step_vjp(g: Grid, uh, dt, gout, force=None):
+    """Transpose of the linearised IF-Heun step (heun_step at fixed dt, bandlim
+    off) at uh applied to gout, Euclidean on (Re, Im) of the half spectrum.
+    With S(u) = IF u + dt/2 IF N(u) + dt/2 N(u*), u* = IF (u + dt N(u)) and IF
+    real and diagonal:
+        a = N'(u*)^T (dt/2 gout),
+        S'(u)^T gout = IF (gout + a) + N'(u)^T (IF (dt/2 gout + dt a))."""
+    IF = rhs_int_fact(g, dt)
+    n1 = rhs_nonlinear(g, uh)
+    if force is not None:
+        n1 = n1 + force
+    ut = IF * (uh + dt * n1)
+    a = rhs_nonlinear_vjp(g, ut, 0.5 * dt * gout)
+    return IF * (gout + a) + rhs_nonlinear_vjp(g, uh, IF * (0.5 * dt * gout + dt * a))
+
+
+def orbit_residual_grad(g: Grid, u0, dt, nsteps, force=None):
+    """Periodic-orbit residual J(u0) = 1/2 <(u(T) - u0)^2> (mean square over
+    the physical grid, = 1/2 s^2 sum_half W |r|^2 with r = u(T) - u0 and T =
+    nsteps dt of fixed-dt IF-Heun) and its gradient (Euclidean on Re/Im of the
+    half spectrum): grad = (Phi'^T - I) (s^2 W r), Phi' backpropagated through
+    the stored states."""
+    s2 = g.scalemodes ** 2
+    W = half_weight(g)
+    states = [u0]
+    for _ in range(nsteps):
+        states.append(heun_step(g, states[-1], dt, force))
+    r = states[-1] - u0
+    J = 0.5 * s2 * float(np.sum(W * np.abs(r) ** 2))
+    gc = s2 * W * r
+    gb = gc
+    for n in range(nsteps - 1, -1, -1):
+        gb = heun_step_vjp(g, states[n], dt, gb, force)
+    return J, gb - gc
 
 
 # ================================================================ drivers
