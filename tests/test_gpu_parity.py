@@ -365,3 +365,42 @@ def test_axes_of_1024(prec, shape):
     uh = O.state_dealias(g, O.state_project(g, O.state_u2uhat(g, rng.standard_normal((3, nz, ny, nx)))))
     got, _ = b.rhs_nonlinear(b.from_numpy(uh))
     assert rel(got.cpu().numpy(), O.rhs_nonlinear(g, uh)) < tol("fp64" if prec == "fp64" else "fp32")
+
+
+def test_config1_500_steps_fp64_and_fp32():
+    """Config 1 as specified: 256^3 forced turbulence (k0 = 3, band forcing
+    0 < |k| <= 2.5 with Pin = 0.1, nu = 2e-3, Courant 0.5), 500 steps in the
+    FP64 and the FP32 forms from the same seeded field.  Both close the energy
+    budget dE/dt = Pin - D (trapezoidal D) to 1e-3 on every step after the
+    first and hold the Courant number at 0.5; the reported production is the
+    injected power Pin.  The two forms' dissipation series agree to 1e-3 and
+    the final E(k) to 1e-2 on shells holding at least 1e-9 of the energy (the
+    flow is chaotic over 500 steps, so FP32 round-off grows; the velocity
+    difference is printed)."""
+    n, ns = 256, 500
+    kw = dict(nu=2e-3, kCutOff=2.5, Pin=0.1, courant_min=0.5, courant_max=0.5)
+    uh = ic.random_field(n, seed=0, k0=3.0)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        b = box(n, prec, **kw)
+        u = b.from_numpy(uh)
+        e0 = b.kinetic(u)
+        recs = b.step(u, ns)
+        es, *_ = b.spectrum(u)
+        E = [e0] + [r["ekin"] for r in recs]
+        resid = max(abs((E[i + 1] - E[i]) / recs[i]["dt"]
+                        - (0.1 - 0.5 * (recs[i - 1]["dissipation"] + recs[i]["dissipation"])))
+                    for i in range(1, ns))
+        assert resid < 1e-3, (prec, resid)
+        assert all(abs(r["courant"] - 0.5) < 1e-6 for r in recs[1:])
+        assert all(abs(r["injected_power"] - 0.1) < 1e-12 for r in recs)
+        out[prec] = (u.to(torch.complex128).cpu(), np.array([r["dissipation"] for r in recs]), es, resid)
+        b.close()
+    (u64, d64, e64, r64), (u32, d32, e32, r32) = out["fp64"], out["fp32"]
+    dd = float(np.max(np.abs(d32 - d64) / d64))
+    live = e64 >= 1e-9 * e64.sum()
+    ek = float(np.max(np.abs(e32[live] - e64[live]) / e64[live]))
+    ev = float((u32 - u64).abs().norm() / u64.abs().norm())
+    print(f"config 1, 500 steps: budget residual fp64 {r64:.2e} fp32 {r32:.2e}; fp32 vs fp64: D {dd:.2e}, "
+          f"E(k) {ek:.2e}, velocity {ev:.2e}")
+    assert dd < 1e-3 and ek < 1e-2
