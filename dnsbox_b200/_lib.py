@@ -32,7 +32,8 @@ class Params(ctypes.Structure):
         ("precision", ctypes.c_int32), ("stepper", ctypes.c_int32), ("ab2_mode", ctypes.c_int32),
         ("bandlim", ctypes.c_int32), ("spherical", ctypes.c_int32), ("tstep_fix", ctypes.c_int32),
         ("hminone", ctypes.c_int32), ("spectrum_mode", ctypes.c_int32), ("adj_phat", ctypes.c_int32),
-        ("device", ctypes.c_int32), ("nbatch", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 2),
+        ("device", ctypes.c_int32), ("nbatch", ctypes.c_int32), ("no_prune", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 1),
         ("alpha_x", ctypes.c_double), ("alpha_y", ctypes.c_double), ("alpha_z", ctypes.c_double),
         ("nu", ctypes.c_double), ("Q", ctypes.c_double), ("kCutOff", ctypes.c_double),
         ("Pin", ctypes.c_double), ("Deltak", ctypes.c_double),
@@ -106,6 +107,7 @@ SIGNATURES = {
     "dnsbox_residual_grad": (ctypes.c_int, [_VP, _VP, _VP, _DP]),
     "dnsbox_adjoint_descent": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _DP, _DP]),
     "dnsbox_heun_step_vjp": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "dnsbox_step_pruned": (ctypes.c_int, [_VP]),
     "dnsbox_heun_steps_vjp": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
     "dnsbox_orbit_residual": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _DP]),
     "dnsbox_batch_size": (ctypes.c_int, [_VP]),

@@ -341,6 +341,25 @@ __global__ void k_convert(const A *src, B *dst, long long n) {
     dst[i] = (B)src[i];
 }
 
+// Sets *flag when any component of a state (3 fields nh apart) is nonzero
+// (or not a number) at a mode outside the kept set of the pruning rule.
+template <typename C>
+__global__ void k_cut_check(const C *u, long long nh, int nxh, int ny, AxisKeep kx, AxisKeep ky, AxisKeep kz,
+                            int *flag) {
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(m % nxh), iy = (int)((m / nxh) % ny), iz = (int)(m / ((long long)nxh * ny));
+    if (kx.keep(ix) && ky.keep(iy) && kz.keep(iz)) continue;
+    for (int c = 0; c < 3; ++c) {
+      const C v = u[c * nh + m];
+      if (!(v.x == 0 && v.y == 0)) {
+        *flag = 1;
+        return;
+      }
+    }
+  }
+}
+
 template <typename T> static FinishArgs<T> finish_base(const dnsbox_ctx *c) {
   FinishArgs<T> f;
   memset(&f, 0, sizeof(f));
@@ -374,7 +393,7 @@ template <typename T> static FinishArgs<T> finish_base(const dnsbox_ctx *c) {
 // One right-hand side: passes A-E.  cfl: 0 none, 1 record (+control).
 template <typename T>
 static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *state, void *nold,
-                   bool partials, int cfl, dnsbox_diag *drec) {
+                   bool partials, int cfl, dnsbox_diag *drec, bool pruned = false) {
   using C = typename CT<T>::type;
   const dnsbox_params &p = c->p;
   const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
@@ -397,6 +416,11 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   set_job<T>(a, 2, cfield(u, c, 2), field(c->W1, c, 2));
   set_job<T>(a, 3, cfield(u, c, 1), field(c->W1, c, 3), 0.0, -s, 1);   // -dz v
   set_job<T>(a, 4, cfield(u, c, 0), field(c->W1, c, 4), 0.0, s, 1);    //  dz u
+  if (pruned) {   // input zero outside kept (kz rows, ky, kx); outputs there stay unwritten (zero)
+    a.kcol = c->keep[0];
+    a.koth = c->keep[1];
+    a.krin = c->keep[2];
+  }
   RET(run_strided<T>(c, 2, true, a, DNSBOX_PASS_Z_INV));
   // pass B: inverse y
   StridedArgs<T> b = strided_base<T>(c, 1);
@@ -408,6 +432,10 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   set_job<T>(b, 3, field(c->W1, c, 2), field(c->W2, c, 3), 0.0, s, 1, field(c->W1, c, 3));
   set_job<T>(b, 4, field(c->W1, c, 4), field(c->W2, c, 4), 1.0, 0.0, 0, field(c->W1, c, 2), 0.0, -s, 0);
   set_job<T>(b, 5, field(c->W1, c, 0), field(c->W2, c, 5), 0.0, -s, 1, field(c->W1, c, 1), 0.0, s, 0);
+  if (pruned) {   // pass-A outputs exist only on kept (ky, kx)
+    b.kcol = c->keep[0];
+    b.krin = c->keep[1];
+  }
   RET(run_strided<T>(c, 1, true, b, DNSBOX_PASS_Y_INV));
   // pass C: fused x pass
   XlineNLArgs<T> x;
@@ -428,6 +456,7 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   x.nxh = c->nxh;
   x.alpha_x = p.alpha_x;
   x.s = s;
+  if (pruned) x.kxa = c->keep[0].a;   // read only kept kx; write only kx the finish keeps
   {
     Prof pr(c, DNSBOX_PASS_X_NL);
     CK(Ops<T>::xline_nl(p.nx, x, c->stream));
@@ -446,6 +475,10 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   StridedArgs<T> d = strided_base<T>(c, 1);
   d.njobs = 3;
   for (int f = 0; f < 3; ++f) set_job<T>(d, f, field(c->W1, c, f), field(c->W2, c, f));
+  if (pruned) {   // only kept kx columns; ky rows outside the kept set are masked by the finish
+    d.kcol = c->keep[0];
+    d.krout = c->keep[1];
+  }
   RET(run_strided<T>(c, 1, false, d, DNSBOX_PASS_Y_FWD));
   // pass E: forward z + spectral finish
   FinishArgs<T> e = finish_base<T>(c);
@@ -460,6 +493,10 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   e.nh = (long long)c->fstride;
   e.bstride = (long long)c->nh;
   e.mode = mode;
+  if (pruned) {
+    e.kx = c->keep[0];
+    e.ky = c->keep[1];
+  }
   const int ztc = Ops<T>::zfinish_cols(p.nz);
   const int ntx = (c->nxh + ztc - 1) / ztc;
   Prof pr(c, DNSBOX_PASS_Z_FIN);
@@ -506,12 +543,12 @@ template <typename T> static int step_once(dnsbox_ctx *c, void *uh) {
   if (pc) {
     // dnsboxheun.f90:85-126 (and dnsbox.f90:87-141 for the AB2 first step)
     RET(run_rhs<T>(c, uh, FIN_PRED, c->ustar, nullptr, p.stepper == DNSBOX_AB2 ? c->nold : nullptr, false, 1,
-                   nullptr));
-    RET(run_rhs<T>(c, c->ustar, FIN_CORR, nullptr, uh, nullptr, true, 0, nullptr));
+                   nullptr, c->prune_now));
+    RET(run_rhs<T>(c, c->ustar, FIN_CORR, nullptr, uh, nullptr, true, 0, nullptr, c->prune_now));
     if (p.stepper == DNSBOX_AB2) c->ab2_started = 1;
   } else {
     // dnsbox.f90:143-191
-    RET(run_rhs<T>(c, uh, FIN_AB2, nullptr, uh, c->nold, true, 1, nullptr));
+    RET(run_rhs<T>(c, uh, FIN_AB2, nullptr, uh, c->nold, true, 1, nullptr, c->prune_now));
   }
   const int ztc = Ops<T>::zfinish_cols(p.nz);
   const int ntx = (c->nxh + ztc - 1) / ztc;
@@ -523,7 +560,26 @@ template <typename T> static int step_once(dnsbox_ctx *c, void *uh) {
   return DNSBOX_OK;
 }
 
+// Decides whether this call may use the pruned passes: the state must vanish
+// exactly on the 2/3-rule cut set (the stepper then keeps it so).
+template <typename T> static int prune_decide(dnsbox_ctx *c, const void *uh) {
+  using C = typename CT<T>::type;
+  c->prune_now = 0;
+  if (!c->prune_ok || c->p.no_prune || c->nbatch > 1) return DNSBOX_OK;
+  CK(cudaMemsetAsync(c->cut_flag, 0, sizeof(int), c->stream));
+  k_cut_check<C><<<grid_for((long long)c->nh), 256, 0, c->stream>>>(reinterpret_cast<const C *>(uh), (long long)c->nh,
+                                                                     c->nxh, c->p.ny, c->keep[0], c->keep[1],
+                                                                     c->keep[2], c->cut_flag);
+  CK(cudaGetLastError());
+  int *flag = reinterpret_cast<int *>(c->hstage + 62);
+  CK(cudaMemcpyAsync(flag, c->cut_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->prune_now = *flag == 0;
+  return DNSBOX_OK;
+}
+
 template <typename T> static int step_impl(dnsbox_ctx *c, void *uh, int nsteps, dnsbox_diag *dh) {
+  RET(prune_decide<T>(c, uh));
   long long chunk_first = c->host_step;
   for (int n = 0; n < nsteps; ++n) {
     RET(step_once<T>(c, uh));
@@ -597,6 +653,7 @@ static void free_ctx(dnsbox_ctx *c) {
   if (!c) return;
   cudaFree(c->adft);
   cudaFree(c->tc_status);
+  cudaFree(c->cut_flag);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   cudaFree(c->W1);
   cudaFree(c->W2);
@@ -662,6 +719,38 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
   if (p->precision == DNSBOX_TC_SPLIT) {
     c->tc = 1;
     if ((rc = alloc_dft64(c))) return fail(rc);
+  }
+  // pruning rule per axis, derived from the dealiasing mask and checked against it
+  {
+    const int ns[3] = {p->nx, p->ny, p->nz};
+    const double al[3] = {p->alpha_x, p->alpha_y, p->alpha_z};
+    bool ok = true;
+    for (int ax = 0; ax < 3; ++ax) {
+      const int n = ns[ax];
+      const bool full = ax > 0;
+      const double cut = (n / 2.0) * (2.0 * al[ax] / 3.0);
+      auto kk = [&](int i) { return full ? k_full(i, n, al[ax]) : k_half(i, n, al[ax]); };
+      int a = 0;
+      for (int i = 1; i < n / 2; ++i)
+        if (fabs(kk(i)) >= cut) {
+          a = i;
+          break;
+        }
+      c->keep[ax] = AxisKeep{a, n, full ? 1 : 0};
+      const int m = full ? n : n / 2 + 1;
+      for (int i = 0; i < m; ++i)
+        if (c->keep[ax].keep(i) != !(fabs(kk(i)) >= cut)) ok = false;
+      if (a == 0) ok = false;
+    }
+    c->prune_ok = ok;
+    if (!ok)
+      for (int ax = 0; ax < 3; ++ax) c->keep[ax].a = 0;
+    if ((e = cudaMalloc(&c->cut_flag, sizeof(int))) != cudaSuccess)
+      return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed"));
+    // pruned steps leave the cut set of these buffers untouched: start at zero
+    if ((e = cudaMemset(c->ustar, 0, 3 * fb)) != cudaSuccess ||
+        (c->nold && (e = cudaMemset(c->nold, 0, 3 * fb)) != cudaSuccess))
+      return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
   }
   {
     const int ztc = c->fp64 ? Ops<double>::zfinish_cols(p->nz) : Ops<float>::zfinish_cols(p->nz);
@@ -750,6 +839,8 @@ extern "C" int dnsbox_field_bytes(const dnsbox_ctx *ctx, size_t *sb, size_t *pb)
 }
 
 extern "C" int dnsbox_nspec(const dnsbox_ctx *ctx) { return ctx ? ctx->nspec : -1; }
+
+extern "C" int dnsbox_step_pruned(const dnsbox_ctx *ctx) { return ctx ? ctx->prune_now : -1; }
 
 #define BEGIN(ctx)                                              \
   if (!(ctx)) return set_err(DNSBOX_ERR_ARG, "null context");   \
@@ -1255,7 +1346,10 @@ extern "C" int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *stat
   if ((err = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking)) != cudaSuccess) return fail(err, "stream");
   if ((err = cudaEventCreateWithFlags(&e->in, cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
   if ((err = cudaEventCreateWithFlags(&e->out, cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
-  for (auto *c : e->ctxs) c->stream = e->user;
+  for (auto *c : e->ctxs) {
+    c->stream = e->user;
+    c->prune_now = 0;   // the captured step uses the full passes (no per-call state check inside a graph)
+  }
   // one eager step on the contexts' stream, so the captured step is a steady
   // one (the first step's forced dt update and the AB2 start-up are host-side
   // decisions)

@@ -64,6 +64,10 @@ struct dnsbox_ctx {
   int ring_cap = 0;                      // device ring of step records: ring_cap steps x nbatch
   long long host_step = 0;               // steps issued so far (ring position)
   const void *force = nullptr;           // fixed spectral forcing (3 fields) or null
+  AxisKeep keep[3];                      // pruning rule per axis (x half, y full, z full); a = 0: none
+  int prune_ok = 0;                      // the rule prunes something on this grid
+  int prune_now = 0;                     // the step in flight uses the pruned passes
+  int *cut_flag = nullptr;               // device: the state is nonzero on the cut set
   int tc = 0;                            // DNSBOX_TC_SPLIT: tensor-core strided passes
   void *adft = nullptr;                  // device DFT-64 operands (forward hi, lo, inverse hi, lo)
   int *tc_status = nullptr;              // device flag: an MMA completion wait gave up
@@ -274,18 +278,30 @@ static void set_job(StridedArgs<T> &a, int j, const void *in1, void *out, double
   a.job[j].ks2 = ks2;
 }
 
+// Launches a strided pass.  The column-tile grid follows the kernel's tile
+// width: all ceil(nxh / width) tiles, or, when a.kcol prunes, the tiles below
+// the cut and the one holding the Nyquist column; a.koth prunes the other axis.
 template <typename T>
-static int run_strided(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<T> &a,
-                       int kind = DNSBOX_PASS_OTHER) {
-  const int ntx = (c->nxh + TileCols<T>::v - 1) / TileCols<T>::v;
-  const int nother = axis == 2 ? c->p.ny : c->p.nz;
+static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int kind = DNSBOX_PASS_OTHER) {
   const int n = axis == 2 ? c->p.nz : c->p.ny;
+  const bool tc = c->tc && Ops<T>::has_tc(n);
+  const int width = tc ? 4096 / n : TileCols<T>::v;
+  if (a.kcol.a) {
+    a.ntx_lo = (a.kcol.a + width - 1) / width;
+    const int nt = (c->p.nx / 2) / width;
+    a.nyq_tile = nt < a.ntx_lo ? -1 : nt;
+  } else {
+    a.ntx_lo = (c->nxh + width - 1) / width;
+    a.nyq_tile = -1;
+  }
+  const int nother = a.koth.a ? a.koth.count() : (axis == 2 ? c->p.ny : c->p.nz);
+  const int ntiles = (a.ntx_lo + (a.nyq_tile >= 0 ? 1 : 0)) * nother;
   Prof pr(c, kind);
-  if (c->tc && Ops<T>::has_tc(n)) {
+  if (tc) {
     CK(Ops<T>::strided_tc(n, a, inv, nother, c->adft, c->tc_status, c->tc_ctas, c->stream));
     return DNSBOX_OK;
   }
-  CK(Ops<T>::strided(n, a, inv, ntx * nother, c->stream));
+  CK(Ops<T>::strided(n, a, inv, ntiles, c->stream));
   return DNSBOX_OK;
 }
 

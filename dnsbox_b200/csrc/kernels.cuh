@@ -41,6 +41,24 @@ struct StepState {
   double pad[6];
 };
 
+// Pruning of the 2/3-rule zeros.  On an axis of length n the dealiasing mask
+// (rhs.f90:74-88) keeps index i when |k_i| < (n/2)(2/3) alpha, i.e. i < a, the
+// Nyquist index n/2 (whose wavenumber is 0) and, on full axes, i > n - a.  A
+// state that vanishes outside the kept set keeps doing so under the stepper,
+// so the transforms may skip loading those zeros, skip outputs the mask
+// discards, and skip whole tiles; results are bit-identical.  a = 0: no pruning.
+struct AxisKeep {
+  int a, n, full;
+  __host__ __device__ __forceinline__ bool keep(int i) const {
+    return a == 0 || i < a || i == (n >> 1) || (full && i > n - a);
+  }
+  // kept indices of a full axis in order: [0, a), n/2, (n - a, n)
+  __host__ __device__ __forceinline__ int count() const { return a == 0 ? n : 2 * a; }
+  __host__ __device__ __forceinline__ int map(int o) const {
+    return (a == 0 || o < a) ? o : (o == a ? (n >> 1) : n - 2 * a + o);
+  }
+};
+
 // Tile width (kx columns) of the strided passes: 128 B per row segment.
 template <typename T> struct TileCols;
 template <> struct TileCols<double> { static constexpr int v = 8; };
@@ -75,7 +93,21 @@ template <typename T> struct StridedArgs {
   int nbatch;              // boxes (blockIdx.y), each job pointer advanced by bstride per box
   double alpha_other;
   long long bstride;
+  // pruning (all a = 0 when off): kept kx columns, kept other-axis indices (the
+  // tile grid covers only these), kept input rows (others read as 0) and kept
+  // output rows (others not stored).  Column tiles: [0, ntx_lo) then nyq_tile.
+  AxisKeep kcol, koth, krin, krout;
+  int ntx_lo, nyq_tile;
 };
+
+// Column origin and other-axis index of tile t of the (possibly pruned) grid.
+template <typename T>
+__device__ __forceinline__ void strided_tile(const StridedArgs<T> &a, int tile, int tcw, int &kx0, int &other) {
+  const int ntk = a.ntx_lo + (a.nyq_tile >= 0 ? 1 : 0);
+  const int o = tile / ntk, kt = tile - o * ntk;
+  kx0 = (kt < a.ntx_lo ? kt : a.nyq_tile) * tcw;
+  other = a.koth.map(o);
+}
 
 template <typename T, typename C>
 __device__ __forceinline__ C apply_mult(C v, double a, double b, double k) {
@@ -96,21 +128,21 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
   C *s = reinterpret_cast<C *>(smem_raw);
   const int job = blockIdx.x % a.njobs;
   const int tile = blockIdx.x / a.njobs;
-  const int ntx = (a.ncols + TC - 1) / TC;
-  const int other = tile / ntx;
-  const int kx0 = (tile - other * ntx) * TC;
+  int kx0, other;
+  strided_tile(a, tile, TC, kx0, other);
   const StridedJob<T> &J = a.job[job];
   const bool act = threadIdx.x < NF;
   const int col = threadIdx.x % TC, p = threadIdx.x / TC;
   const int kx = kx0 + col;
-  const bool valid = act && kx < a.ncols;
+  const bool valid = act && kx < a.ncols && a.kcol.keep(kx);
   const long long base = (long long)other * a.otherstride + kx + (long long)blockIdx.y * a.bstride;
   C v[E];
   if (valid) {
     // all E loads of the first stage are independent and issued together
     const C *in1 = J.in1 + base;
 #pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = in1[(long long)EN::in_row(p, i) * a.rowstride];
+    for (int i = 0; i < E; ++i)
+      v[i] = a.krin.keep(EN::in_row(p, i)) ? in1[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
     // wavenumber of the column (0) or of the tile's other-axis index (2)
     const double kcol = k_half(kx, a.nx, a.alpha_x);
     const double koth = a.n_other ? k_full(other, a.n_other, a.alpha_other) : 0.0;
@@ -125,7 +157,7 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
       const double kc = J.ks2 == 2 ? koth : kcol;
 #pragma unroll
       for (int i = 0; i < E; ++i) {
-        const C w = in2[(long long)EN::in_row(p, i) * a.rowstride];
+        const C w = a.krin.keep(EN::in_row(p, i)) ? in2[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
         v[i] = cadd(v[i], apply_mult<T>(w, J.a2, J.b2, J.ks2 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc));
       }
     }
@@ -137,7 +169,8 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
   if (valid) {
     C *out = J.out + base;
 #pragma unroll
-    for (int i = 0; i < E; ++i) out[(long long)EN::out_row(p, i) * a.rowstride] = v[i];
+    for (int i = 0; i < E; ++i)
+      if (a.krout.keep(EN::out_row(p, i))) out[(long long)EN::out_row(p, i) * a.rowstride] = v[i];
   }
 }
 
@@ -150,10 +183,13 @@ template <typename T> struct XlineNLArgs {
   StepState *st;                       // per-box step state: umax[3] gets max |u_i| (true scale)
   int nlines, nxh;
   int lines_per_box;                   // ny * nz
-  int pad0;
+  int kxa;                             // pruning: only kx < kxa and kx = N/2 are read and written (0: all)
   double alpha_x;
   double s;                            // scalemodes
 };
+
+// kept half-axis index under the x-line pruning rule
+__device__ __forceinline__ bool xkeep(int kxa, int k, int n) { return kxa == 0 || k < kxa || k == (n >> 1); }
 
 // Lines per CTA of the fused x pass (even; 3B columns in shared memory).
 template <typename T, int N> struct XlineB {
@@ -216,8 +252,9 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
     for (int i = 0; i < E; ++i) {
       const int n = EN::in_row(p, i);
       const int kk = n <= N / 2 ? n : N - n;
-      const C X1 = v1 ? r1[kk] : mkc<C>(0, 0);
-      const C X2 = v2 ? r2[kk] : mkc<C>(0, 0);
+      const bool kp = xkeep(a.kxa, kk, N);
+      const C X1 = (v1 && kp) ? r1[kk] : mkc<C>(0, 0);
+      const C X2 = (v2 && kp) ? r2[kk] : mkc<C>(0, 0);
       v[i] = pack_pair<C, N>(n, X1, X2);
     }
     fft_regs<C, N, true>(v, s, LD, col, p, act, a.tw);
@@ -278,6 +315,7 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
     const C X1 = mkc<C>(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
     const C X2 = mkc<C>(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
     const int la = line0 + 2 * j, lb = la + 1;
+    if (!xkeep(a.kxa, k, N)) continue;
     if (c == 0) {
       if (la < a.nlines) {
         a.NX[(long long)la * a.nxh + k] = X1;
@@ -359,8 +397,9 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
   for (int i = 0; i < E; ++i) {
     const int n = EN::in_row(lane, i);
     const int kk = n <= N / 2 ? n : N - n;
-    x1[i] = f1s[0][l1s[0] * a.nxh + kk];
-    x2[i] = f2s[0][l2s[0] * a.nxh + kk];
+    const bool kp = xkeep(a.kxa, kk, N);
+    x1[i] = kp ? f1s[0][l1s[0] * a.nxh + kk] : mkc<C>(0, 0);
+    x2[i] = kp ? f2s[0][l2s[0] * a.nxh + kk] : mkc<C>(0, 0);
   }
 #pragma unroll 1
   for (int q = 0; q < 6; ++q) {
@@ -373,8 +412,9 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
       for (int i = 0; i < E; ++i) {
         const int n = EN::in_row(lane, i);
         const int kk = n <= N / 2 ? n : N - n;
-        x1[i] = g1[kk];
-        x2[i] = g2[kk];
+        const bool kp = xkeep(a.kxa, kk, N);
+        x1[i] = kp ? g1[kk] : mkc<C>(0, 0);
+        x2[i] = kp ? g2[kk] : mkc<C>(0, 0);
       }
     }
     fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, lane, true, a.tw);
@@ -419,6 +459,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
   __syncwarp();
   // unpack two real transforms per sequence and store
   for (int k = lane; k < H; k += 32) {
+    if (!xkeep(a.kxa, k, N)) continue;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const C zk = s[AD::at(k, q, LDC)], zn = s[AD::at((N - k) % N, q, LDC)];
@@ -578,6 +619,7 @@ template <typename T> struct FinishArgs {
   double cutx, cuty, cutz, sph2;
   int bandlim, spherical, mode, ab2_standard;
   double s;                // scalemodes
+  AxisKeep kx, ky;         // pruning: column tiles outside the kept set are skipped (zero partials)
 };
 
 template <typename T, int N>
@@ -600,9 +642,18 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
   const bool act = threadIdx.x < NF;
   const int col = threadIdx.x % TC, p = threadIdx.x / TC;
   const int kx = kx0 + col;
-  const bool valid = act && kx < a.nxh;
+  const bool valid = act && kx < a.nxh && a.kx.keep(kx);
   const int box = blockIdx.y;
   const long long base = (long long)ky * a.nxh + kx + (long long)box * a.bstride;
+  // pruned column tile: every mode is masked and the state there is zero
+  if (!a.ky.keep(ky) || !(a.kx.a == 0 || kx0 < a.kx.a || (kx0 <= (a.nx >> 1) && (a.nx >> 1) < kx0 + TC))) {
+    if (a.partials && threadIdx.x == 0) {
+      double *pp = a.partials + 2 * ((long long)box * gridDim.x + blockIdx.x);
+      pp[0] = 0.0;
+      pp[1] = 0.0;
+    }
+    return;
+  }
   // forward z transforms of the three components, each using its own tile as
   // scratch; fields 0 and 1 park their outputs in this thread's own slots of
   // tiles 0 and 1, field 2 stays in v

@@ -105,8 +105,8 @@ struct FastDiv {
 };
 
 struct TcArgs {
-  int ntx;          // tiles across the kx columns
-  int nother;       // tiles along the other axis
+  int ntx;          // kept tiles across the kx columns (all when not pruning)
+  int nother;       // kept indices of the other axis
   int total;        // work items: boxes x tiles x jobs (< 2^31)
   FastDiv per_box;  // njobs * ntx * nother
   FastDiv njobs;
@@ -134,8 +134,10 @@ __device__ __forceinline__ TcItem tc_item(const StridedArgs<float> &a, const TcA
   const unsigned tile = g.njobs.div(rw);
   TcItem it;
   it.job = (int)(rw - tile * g.njobs.d);
-  it.other = (int)g.ntxd.div(tile);
-  it.kx0 = (int)(tile - (unsigned)it.other * g.ntxd.d) * TCW;
+  const int o = (int)g.ntxd.div(tile);
+  const int kt = (int)(tile - (unsigned)o * g.ntxd.d);
+  it.other = a.koth.map(o);
+  it.kx0 = (kt < a.ntx_lo ? kt : a.nyq_tile) * TCW;
   it.base0 = (long long)box * a.bstride + (long long)it.other * a.otherstride + it.kx0;
   return it;
 }
@@ -204,16 +206,18 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
     for (int h = 0; h < RUNS; ++h) {
       const int u = t + NT * h;
       const int c = u % TCW, n2 = (u / TCW) % N2, q = u / 64;
-      const bool valid = it.kx0 + c < a.ncols;
+      const bool valid = it.kx0 + c < a.ncols && a.kcol.keep(it.kx0 + c);
       const long long off = it.base0 + c + (long long)(N2 * 8 * q + n2) * a.rowstride;
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
-        cp_async8(ring + (8 * h + i) * NT + t, J.in1 + (valid ? off + (long long)(N2 * i) * a.rowstride : 0),
-                  valid);
+      for (int i = 0; i < 8; ++i) {
+        const bool vi = valid && a.krin.keep(N2 * (8 * q + i) + n2);
+        cp_async8(ring + (8 * h + i) * NT + t, J.in1 + (vi ? off + (long long)(N2 * i) * a.rowstride : 0), vi);
+      }
       if (J.in2) {
 #pragma unroll
         for (int i = 0; i < 8; ++i)
-          y[h][i] = valid ? J.in2[off + (long long)(N2 * i) * a.rowstride] : mkc<C>(0.f, 0.f);
+          y[h][i] = (valid && a.krin.keep(N2 * (8 * q + i) + n2)) ? J.in2[off + (long long)(N2 * i) * a.rowstride]
+                                                                    : mkc<C>(0.f, 0.f);
       }
     }
     cp_async_commit();
@@ -367,10 +371,11 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
         z[m2] = yy;
       }
       dft<N2, C, INV>(z);
-      if (it.kx0 + cc < a.ncols) {
+      if (it.kx0 + cc < a.ncols && a.kcol.keep(it.kx0 + cc)) {
         C *out = J.out + it.base0 + cc;
 #pragma unroll
-        for (int k2 = 0; k2 < N2; ++k2) out[(long long)(k1 + 64 * k2) * a.rowstride] = z[k2];
+        for (int k2 = 0; k2 < N2; ++k2)
+          if (a.krout.keep(k1 + 64 * k2)) out[(long long)(k1 + 64 * k2) * a.rowstride] = z[k2];
       }
     }
     __syncthreads();

@@ -51,7 +51,7 @@ class Box:
                  ab2="reference", nu=0.005, Q=0.0, kCutOff=2.0, Pin=0.1, Deltak=1.0,
                  courant_min=0.15, courant_max=0.2, dt_max=1.0e-2, dt=1.0e-3, bandlim=True,
                  spherical=False, tstep_fix=False, hminone=True, spectrum_mode="mpi",
-                 adj_phat="intent", alpha=(1.0, 1.0, 1.0), device=None, nbatch=1):
+                 adj_phat="intent", alpha=(1.0, 1.0, 1.0), device=None, nbatch=1, prune=True):
         if not torch.cuda.is_available():
             raise RuntimeError("dnsbox_b200 needs a CUDA device (there is no CPU path)")
         lib = _lib.load()
@@ -72,6 +72,7 @@ class Box:
         p.adj_phat = ADJ_PHAT[adj_phat]
         p.device = device
         p.nbatch = int(nbatch)
+        p.no_prune = 0 if prune else 1
         p.alpha_x, p.alpha_y, p.alpha_z = alpha
         p.nu, p.Q, p.kCutOff, p.Pin, p.Deltak = nu, Q, kCutOff, Pin, Deltak
         p.courant_min, p.courant_max, p.dt_max, p.dt = courant_min, courant_max, dt_max, dt
@@ -286,6 +287,10 @@ class Box:
         _lib.check(self._lib.dnsbox_adjoint_descent(self._h, _ptr(uh), int(niter),
                                                     hist.ctypes.data_as(_lib._DP), ctypes.byref(a)))
         return hist, a.value
+
+    def step_pruned(self) -> bool:
+        """Whether the last step call ran the pruned (2/3-rule) passes."""
+        return self._lib.dnsbox_step_pruned(self._h) == 1
 
     # ------------------------------------------------------- time-horizon gradients
     def heun_step_vjp(self, uh, g):

@@ -67,7 +67,9 @@ typedef struct dnsbox_params {
   int32_t adj_phat;              /* enum dnsbox_adj_phat                     */
   int32_t device;                /* CUDA device ordinal                      */
   int32_t nbatch;                /* boxes of this size advanced together (0 or 1: one box) */
-  int32_t reserved_i[2];
+  int32_t no_prune;              /* 1: dnsbox_step never prunes the 2/3-rule zeros (default 0: it
+                                    prunes when the state vanishes on the cut set; bit-identical) */
+  int32_t reserved_i[1];
   double alpha_x, alpha_y, alpha_z; /* parameters.f90:18-20                  */
   double nu;                     /* parameters.f90:21                        */
   double Q;                      /* parameters.f90:22                        */
@@ -132,6 +134,11 @@ int dnsbox_rhs_nonlinear(dnsbox_ctx *ctx, const void *uhat3_dev, void *nonlin3_d
  * tstep_fix.  diag_host (nsteps records) may be NULL; when given, the call
  * synchronises the stream before returning. */
 int dnsbox_step(dnsbox_ctx *ctx, void *uhat3_dev, int nsteps, dnsbox_diag *diag_host);
+/* 1 if the last dnsbox_step call ran the pruned passes (the state vanished on
+ * the 2/3-rule cut set, so loads of those zeros and transforms of modes the
+ * mask discards were skipped, bit-identically), 0 if it ran the full passes,
+ * -1 for a null context.  No reference counterpart. */
+int dnsbox_step_pruned(const dnsbox_ctx *ctx);
 /* state_project, state.f90:120-179 (in place) */
 int dnsbox_project(dnsbox_ctx *ctx, void *uhat3_dev);
 /* state_dealias, state.f90:181-209 (in place) */
