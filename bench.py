@@ -45,6 +45,18 @@ PASS_FIELDS_HEUN = {"z_inv": [8, 8], "y_inv": [11, 11], "x_nl": [9, 9], "y_fwd":
                     "z_fin": [9, 12]}
 
 
+def pruned_pass_fields(n):
+    """The same for the pruned passes of a cubic n^3 box: only the kept fraction
+    of each axis (kx < a plus the Nyquist column; |ky|, |kz| < a plus Nyquist,
+    a = ceil(n/3)) is read or written where the pass skips the 2/3-rule zeros."""
+    a = -(-n // 3)
+    fx = (a + 1) / (n // 2 + 1)
+    fy = fz = 2 * a / n
+    fxy = fx * fy
+    return {"z_inv": [3 * fxy * fz + 5 * fxy] * 2, "y_inv": [5 * fxy + 6 * fx] * 2, "x_nl": [9 * fx] * 2,
+            "y_fwd": [3 * fx + 3 * fxy] * 2, "z_fin": [9 * fxy, 12 * fxy]}
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -353,16 +365,18 @@ def ensemble_rate(steps=50):
             "graph": "one CUDA-graph replay per ensemble step (3 batched size groups)"}
 
 
-def read_traffic(prec, n):
-    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+def read_traffic(prec, n, pruned):
+    """DRAM bytes per launch from a committed ncu summary, if one exists
+    (columns: pass precision n pruned bytes)."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     out = {}
     if not os.path.exists(path):
         return out
     for line in open(path):
         parts = line.split()
-        if len(parts) == 4 and not line.startswith("#") and parts[1] == prec and int(parts[2]) == n:
-            out[parts[0]] = float(parts[3])
+        if (len(parts) == 5 and not line.startswith("#") and parts[1] == prec and int(parts[2]) == n
+                and int(parts[3]) == int(bool(pruned))):
+            out[parts[0]] = float(parts[4])
     return out
 
 
@@ -388,10 +402,12 @@ def run_ours(args, rank, world, dist_on):
         with sampler:
             ms = timed_steps(box, u, args.steps, dist_on)
         launches = box.profile_read(reset=True)["total_launches"]
+        pruned = box.step_pruned()
         if rank == 0 and prec in ("fp64", "tc_split", "fp32"):
             final[prec] = u.to(torch.complex128).cpu()   # after W + K steps from the same field
         pr = profile_passes(box, u, args.steps)
-        res = {"ms": ms, "launches": launches, "profile": pr, "clocks": sampler.summary()}
+        res = {"ms": ms, "launches": launches, "profile": pr, "clocks": sampler.summary(), "pruned": pruned,
+               "pass_fields": pruned_pass_fields(n) if pruned else PASS_FIELDS_HEUN}
         if prec == args.precisions[0] and rank == 0:
             res["e2e"] = measure_e2e(box, uh_np, max(3, min(args.steps, 20)))
         fb = box.nz * box.ny * box.nxh * (16 if prec == "fp64" else 8)
@@ -408,7 +424,7 @@ def run_ours(args, rank, world, dist_on):
     # dominant kernel roofline
     pr = r["profile"]
     per_pass = {}
-    for name, fields in PASS_FIELDS_HEUN.items():
+    for name, fields in r["pass_fields"].items():
         ms = pr["ms"][name]
         nl = pr["launches"][name]
         if nl == 0 or ms <= 0:
@@ -419,7 +435,7 @@ def run_ours(args, rank, world, dist_on):
                           "gbs": nbytes / (ms / 1e3) / 1e9, "bytes_per_launch": nbytes / nl}
     dom = max(per_pass, key=lambda k: per_pass[k]["ms_total"])
     d = per_pass[dom]
-    traffic = read_traffic(main, n).get(dom)
+    traffic = read_traffic(main, n, r["pruned"]).get(dom)
     gp = float(n) ** 3
     model_bytes = 72 * (8 if main == "fp64" else 4) * gp
     step_time = r["ms"] / args.steps / 1e3
@@ -432,7 +448,8 @@ def run_ours(args, rank, world, dist_on):
         "config": {"workload": f"forced isotropic turbulence {n}^3, IF-Heun, CFL 0.5, band forcing Pin 0.1, "
                                f"nu 2e-3, k0 3 (independent box per GPU)",
                    "n": n, "precision": main, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (3 x %.0f MB state, 12-field workspace)" % (r["field_bytes"] / 1e6)},
+                   "l2": "inputs larger than L2 (3 x %.0f MB state, 12-field workspace)" % (r["field_bytes"] / 1e6),
+                   "pruned_transforms": r["pruned"]},
         "grid_point_steps_per_s": steps_s * gp,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": hbm_peak, "unit": "GB/s",
                      "frac": d["gbs"] / hbm_peak, "traffic": traffic,
@@ -440,7 +457,10 @@ def run_ours(args, rank, world, dist_on):
                      "peak_source": peak_src},
         "step_roofline": {"model_bytes_per_gp_step": 72 * (8 if main == "fp64" else 4),
                           "achieved": model_bytes / step_time / 1e9, "peak": hbm_peak,
-                          "frac": model_bytes / step_time / 1e9 / hbm_peak},
+                          "frac": model_bytes / step_time / 1e9 / hbm_peak,
+                          "algorithmic_fields_per_step": sum(sum(v) for v in r["pass_fields"].values()),
+                          "algorithmic_achieved": sum(sum(v) for v in r["pass_fields"].values()) * r["field_bytes"]
+                          / step_time / 1e9},
         "passes": {k: {kk: round(vv, 3) for kk, vv in v.items()} for k, v in per_pass.items()},
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
@@ -465,7 +485,8 @@ def run_ours(args, rank, world, dist_on):
             "passes": {k: {"avg_us": round(1e3 * prr["ms"][k] / prr["launches"][k], 2),
                            "gbs": round(sum(f[i % len(f)] for i in range(prr["launches"][k])) * rr["field_bytes"]
                                         / (prr["ms"][k] / 1e3) / 1e9, 1)}
-                       for k, f in PASS_FIELDS_HEUN.items() if prr["launches"][k]}}
+                       for k, f in rr["pass_fields"].items() if prr["launches"][k]},
+            "pruned": rr["pruned"]}
     if world == 1 and not args.no_extra:
         line["extra"] = extra_sizes(args)
         line["extra"]["tc_split_1024"] = tc_1024_rate(args)
