@@ -289,13 +289,13 @@ static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int 
   if (a.kcol.a) {
     a.ntx_lo = (a.kcol.a + width - 1) / width;
     const int nt = (c->p.nx / 2) / width;
-    a.nyq_tile = nt < a.ntx_lo ? -1 : nt;
+    a.nyq_tile = nt < a.ntx_lo ? 0 : nt;   // > 0: the Nyquist column's tile follows the low tiles
   } else {
-    a.ntx_lo = (c->nxh + width - 1) / width;
-    a.nyq_tile = -1;
+    a.ntx_lo = 0;   // full grid
+    a.nyq_tile = 0;
   }
   const int nother = a.koth.a ? a.koth.count() : (axis == 2 ? c->p.ny : c->p.nz);
-  const int ntiles = (a.ntx_lo + (a.nyq_tile >= 0 ? 1 : 0)) * nother;
+  const int ntiles = strided_ntx(a, width) * nother;
   Prof pr(c, kind);
   if (tc) {
     CK(Ops<T>::strided_tc(n, a, inv, nother, c->adft, c->tc_status, c->tc_ctas, c->stream));

@@ -93,19 +93,27 @@ template <typename T> struct StridedArgs {
   int nbatch;              // boxes (blockIdx.y), each job pointer advanced by bstride per box
   double alpha_other;
   long long bstride;
-  // pruning (all a = 0 when off): kept kx columns, kept other-axis indices (the
-  // tile grid covers only these), kept input rows (others read as 0) and kept
-  // output rows (others not stored).  Column tiles: [0, ntx_lo) then nyq_tile.
+  // pruning (all zero when off, so zero-initialised arguments run the full
+  // grid): kept kx columns, kept other-axis indices (the tile grid covers only
+  // these), kept input rows (others read as 0) and kept output rows (others
+  // not stored).  Column tiles: all ceil(ncols / width) when ntx_lo = 0, else
+  // [0, ntx_lo) followed by tile nyq_tile when nyq_tile > 0.
   AxisKeep kcol, koth, krin, krout;
   int ntx_lo, nyq_tile;
 };
 
+// Column tiles of the grid of a strided launch with tile width tcw.
+template <typename T>
+__host__ __device__ __forceinline__ int strided_ntx(const StridedArgs<T> &a, int tcw) {
+  return a.ntx_lo ? a.ntx_lo + (a.nyq_tile > 0 ? 1 : 0) : (a.ncols + tcw - 1) / tcw;
+}
+
 // Column origin and other-axis index of tile t of the (possibly pruned) grid.
 template <typename T>
 __device__ __forceinline__ void strided_tile(const StridedArgs<T> &a, int tile, int tcw, int &kx0, int &other) {
-  const int ntk = a.ntx_lo + (a.nyq_tile >= 0 ? 1 : 0);
+  const int ntk = strided_ntx(a, tcw);
   const int o = tile / ntk, kt = tile - o * ntk;
-  kx0 = (kt < a.ntx_lo ? kt : a.nyq_tile) * tcw;
+  kx0 = (a.ntx_lo == 0 || kt < a.ntx_lo ? kt : a.nyq_tile) * tcw;
   other = a.koth.map(o);
 }
 

@@ -137,7 +137,7 @@ __device__ __forceinline__ TcItem tc_item(const StridedArgs<float> &a, const TcA
   const int o = (int)g.ntxd.div(tile);
   const int kt = (int)(tile - (unsigned)o * g.ntxd.d);
   it.other = a.koth.map(o);
-  it.kx0 = (kt < a.ntx_lo ? kt : a.nyq_tile) * TCW;
+  it.kx0 = (a.ntx_lo == 0 || kt < a.ntx_lo ? kt : a.nyq_tile) * TCW;
   it.base0 = (long long)box * a.bstride + (long long)it.other * a.otherstride + it.kx0;
   return it;
 }

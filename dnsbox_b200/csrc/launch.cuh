@@ -73,7 +73,7 @@ cudaError_t Launcher<T, N>::strided_tc(const StridedArgs<T> &a, bool inv, int no
   if constexpr (std::is_same<T, float>::value && TcPlan<N>::on) {
     using PL = TcPlan<N>;
     TcArgs g;
-    g.ntx = a.ntx_lo + (a.nyq_tile >= 0 ? 1 : 0);   // column tiles of the (possibly pruned) grid
+    g.ntx = strided_ntx(a, PL::TCW);   // column tiles of the (possibly pruned) grid
     g.nother = nother;
     const long long total = (long long)a.njobs * g.ntx * nother * (a.nbatch > 0 ? a.nbatch : 1);
     if (total == 0) return cudaSuccess;
