@@ -685,7 +685,7 @@ int steps_vjp_impl(dnsbox_ctx *c, const void *u0, int nsteps, int every, const v
   CK(cudaMemcpyAsync(seg, u0, sb3, cudaMemcpyDeviceToDevice, c->stream));
   for (int n = 0; n < nsteps; ++n) {
     if (n % every == 0) CK(cudaMemcpyAsync(cp + (size_t)(n / every) * sb3, seg, sb3, cudaMemcpyDeviceToDevice, c->stream));
-    RET(dnsbox_step(c, seg, 1, nullptr));
+    RET(step_advance_decided(c, seg, 1, n == 0));   // pruning decided once for the trajectory
   }
   if (uT_out) CK(cudaMemcpyAsync(uT_out, seg, sb3, cudaMemcpyDeviceToDevice, c->stream));
   // backward sweep, one segment at a time
@@ -696,7 +696,7 @@ int steps_vjp_impl(dnsbox_ctx *c, const void *u0, int nsteps, int every, const v
     for (int j = 1; j < len; ++j) {
       CK(cudaMemcpyAsync(seg + (size_t)j * sb3, seg + (size_t)(j - 1) * sb3, sb3, cudaMemcpyDeviceToDevice,
                          c->stream));
-      RET(dnsbox_step(c, seg + (size_t)j * sb3, 1, nullptr));
+      RET(step_advance_decided(c, seg + (size_t)j * sb3, 1, false));
     }
     for (int j = len - 1; j >= 0; --j) {
       RET(step_vjp_impl<T>(c, seg + (size_t)j * sb3, ga, gb, dt));

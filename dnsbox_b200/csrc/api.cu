@@ -910,6 +910,15 @@ extern "C" int dnsbox_rhs_nonlinear(dnsbox_ctx *ctx, const void *uh, void *out, 
   return DNSBOX_OK;
 }
 
+// Internal: decide pruning for state uh, then advance nsteps without further
+// checks or diagnostics read-back (the trajectory of a state that vanishes on
+// the cut set keeps vanishing there).  Used by the step-transpose chains.
+int step_advance_decided(dnsbox_ctx *c, void *uh, int nsteps, bool decide) {
+  if (decide) RET(c->fp64 ? prune_decide<double>(c, uh) : prune_decide<float>(c, uh));
+  for (int n = 0; n < nsteps; ++n) RET(c->fp64 ? step_once<double>(c, uh) : step_once<float>(c, uh));
+  return DNSBOX_OK;
+}
+
 extern "C" int dnsbox_step(dnsbox_ctx *ctx, void *uh, int nsteps, dnsbox_diag *diag) {
   BEGIN(ctx);
   if (!uh || nsteps < 0) return set_err(DNSBOX_ERR_ARG, "invalid argument");

@@ -34,6 +34,11 @@ int set_err(int code, const char *fmt, ...);
     if (r_ != DNSBOX_OK) return r_;   \
   } while (0)
 
+struct dnsbox_ctx;
+// Advances nsteps with the fused step; with `decide`, first chooses pruned or
+// full passes for this state (api.cu).  No diagnostics are read back.
+int step_advance_decided(dnsbox_ctx *c, void *uh, int nsteps, bool decide);
+
 // ------------------------------------------------------------------ context
 struct dnsbox_ctx {
   dnsbox_params p;
