@@ -66,7 +66,7 @@ template <> struct TileCols<float> { static constexpr int v = 16; };
 // Tile width of the fused z finish, which holds three N-row tiles in shared
 // memory (halved at N = 1024 to stay within 227 KB per CTA).
 template <typename T, int N> struct FinishCols {
-  static constexpr int v = N >= 1024 ? TileCols<T>::v / 2 : TileCols<T>::v;
+  static constexpr int v = (N >= 1024 || (N >= 512 && sizeof(T) == 4)) ? TileCols<T>::v / 2 : TileCols<T>::v;
 };
 
 template <typename T> struct StridedJob {
@@ -639,7 +639,9 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
   constexpr int TC = FinishCols<T, N>::v;
   constexpr int E = EN::E;
   constexpr int NF = TC * (N / E);
-  constexpr int CH = 2;                 // modes per batch of global loads (E is even)
+  // modes per batch of global loads (E is even); one for FP64 at N >= 512,
+  // whose 512-thread blocks have 128 registers a thread
+  constexpr int CH = (sizeof(T) == 8 && N >= 512) ? 1 : 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s = reinterpret_cast<C *>(smem_raw);   // three N x TC tiles, one per component
   __shared__ double red[2 * 32];
