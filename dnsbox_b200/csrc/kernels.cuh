@@ -15,6 +15,8 @@
 // (k_zfinish).
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -372,20 +374,26 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
 // __syncwarp, so the SM overlaps one warp's memory phases with another's
 // transforms (the block-wide barriers of k_xline_nl serialise them).  Columns
 // of a warp's tile are the six sequences of k_xline_nl, stored column-major
-// with the row / R0 skew (conflict-free for the 32-threads-per-sequence plan).
+// with the row / R0 skew (conflict-free for both plans below).  At N = 256 a
+// sequence runs the two-stage radix-16 plan on 16 threads, so a warp
+// transforms two sequences at once with one shared-memory exchange each; at
+// N = 512 a sequence runs the three-stage plan on all 32 threads.
 template <typename T, int N> struct XlineWarp {
   static constexpr bool on = N == 256 || N == 512;
   static constexpr int wpb = sizeof(T) == 8 ? (N >= 512 ? 1 : 2) : (N >= 1024 ? 1 : (N >= 512 ? 2 : 4));
+  using Plan = typename std::conditional<N == 256, FftPlan<256>, WarpPlan<N>>::type;
 };
 
 template <typename T, int N>
 __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
     k_xline_nl_w(const __grid_constant__ XlineNLArgs<T> a) {
   using C = typename CT<T>::type;
-  using PL = WarpPlan<N>;
+  using PL = typename XlineWarp<T, N>::Plan;
   using EN = FftEndsP<PL>;
   using AD = AddrSkew<PL::R[0]>;
   constexpr int E = PL::E;
+  constexpr int P = N / E;                // threads per sequence
+  constexpr int SPW = 32 / P;             // sequences a warp transforms at once
   constexpr int H = N / 2 + 1;
   constexpr int LDC = N + N / PL::R[0];   // column length with the skew
   constexpr int WPB = XlineWarp<T, N>::wpb;
@@ -399,35 +407,39 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
   const C *f2s[6] = {a.V, a.V, a.W, a.OY, a.OY, a.OZ};
   const long long l1s[6] = {la, lb, la, la, lb, la};
   const long long l2s[6] = {la, lb, lb, la, lb, lb};
-  // inverse transforms, loads of sequence q+1 issued before the transform of q
+  const int p = lane % P, h = lane / P;   // position in the sequence, sequence slot
+  // inverse transforms: round r transforms sequences SPW r + h; the loads of
+  // the next round are issued before this round's transform
   C x1[E], x2[E];
 #pragma unroll
   for (int i = 0; i < E; ++i) {
-    const int n = EN::in_row(lane, i);
+    const int n = EN::in_row(p, i);
     const int kk = n <= N / 2 ? n : N - n;
     const bool kp = xkeep(a.kxa, kk, N);
-    x1[i] = kp ? f1s[0][l1s[0] * a.nxh + kk] : mkc<C>(0, 0);
-    x2[i] = kp ? f2s[0][l2s[0] * a.nxh + kk] : mkc<C>(0, 0);
+    x1[i] = kp ? f1s[h][l1s[h] * a.nxh + kk] : mkc<C>(0, 0);
+    x2[i] = kp ? f2s[h][l2s[h] * a.nxh + kk] : mkc<C>(0, 0);
   }
 #pragma unroll 1
-  for (int q = 0; q < 6; ++q) {
+  for (int r = 0; r < 6 / SPW; ++r) {
+    const int q = SPW * r + h;
     C v[E];
 #pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = pack_pair<C, N>(EN::in_row(lane, i), x1[i], x2[i]);
-    if (q < 5) {
-      const C *g1 = f1s[q + 1] + l1s[q + 1] * a.nxh, *g2 = f2s[q + 1] + l2s[q + 1] * a.nxh;
+    for (int i = 0; i < E; ++i) v[i] = pack_pair<C, N>(EN::in_row(p, i), x1[i], x2[i]);
+    if (r + 1 < 6 / SPW) {
+      const int qn = q + SPW;
+      const C *g1 = f1s[qn] + l1s[qn] * a.nxh, *g2 = f2s[qn] + l2s[qn] * a.nxh;
 #pragma unroll
       for (int i = 0; i < E; ++i) {
-        const int n = EN::in_row(lane, i);
+        const int n = EN::in_row(p, i);
         const int kk = n <= N / 2 ? n : N - n;
         const bool kp = xkeep(a.kxa, kk, N);
         x1[i] = kp ? g1[kk] : mkc<C>(0, 0);
         x2[i] = kp ? g2[kk] : mkc<C>(0, 0);
       }
     }
-    fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, lane, true, a.tw);
+    fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, p, true, a.tw);
 #pragma unroll
-    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(lane, i), q, LDC)] = v[i];
+    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
   }
   __syncwarp();
   // (omega x u) * s, written back as (px_a,py_a) (pz_a,pz_b) (px_b,py_b) in columns 0..2
@@ -453,16 +465,23 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
     s[AD::at(n, 2, LDC)] = mkc<C>(px[1], py[1]);
   }
   __syncwarp();
-  // forward transforms of the three product sequences
+  // forward transforms of the three product sequences (SPW at a time)
 #pragma unroll 1
-  for (int q = 0; q < 3; ++q) {
+  for (int r = 0; r < (3 + SPW - 1) / SPW; ++r) {
+    const int q = SPW * r + h;
+    const bool act = q < 3;
+    const int qc = act ? q : 0;
     C v[E];
+    if (act) {
 #pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = s[AD::at(EN::in_row(lane, i), q, LDC)];
+      for (int i = 0; i < E; ++i) v[i] = s[AD::at(EN::in_row(p, i), qc, LDC)];
+    }
     __syncwarp();
-    fft_regs_p<C, PL, false, true, AD>(v, s, LDC, q, lane, true, a.tw);
+    fft_regs_p<C, PL, false, true, AD>(v, s, LDC, qc, p, act, a.tw);
+    if (act) {
 #pragma unroll
-    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(lane, i), q, LDC)] = v[i];
+      for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), qc, LDC)] = v[i];
+    }
   }
   __syncwarp();
   // unpack two real transforms per sequence and store

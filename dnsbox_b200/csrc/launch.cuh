@@ -109,7 +109,7 @@ cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, cudaStream_t st) {
   if constexpr (XlineWarp<T, N>::on) {
     // warp-granular kernel: one warp per line pair
     constexpr int WPB = XlineWarp<T, N>::wpb;
-    constexpr int LDC = N + N / WarpPlan<N>::R[0];
+    constexpr int LDC = N + N / XlineWarp<T, N>::Plan::R[0];
     const size_t smem = (size_t)WPB * 6 * LDC * sizeof(C);
     cudaError_t e;
     if ((e = set_smem(k_xline_nl_w<T, N>, smem)) != cudaSuccess) return e;
