@@ -496,6 +496,7 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   if (pruned) {
     e.kx = c->keep[0];
     e.ky = c->keep[1];
+    e.kz = c->keep[2];
   }
   const int ztc = Ops<T>::zfinish_cols(p.nz);
   const int ntx = (c->nxh + ztc - 1) / ztc;

@@ -285,7 +285,9 @@ static void set_job(StridedArgs<T> &a, int j, const void *in1, void *out, double
 
 // Launches a strided pass.  The column-tile grid follows the kernel's tile
 // width: all ceil(nxh / width) tiles, or, when a.kcol prunes, the tiles below
-// the cut and the one holding the Nyquist column; a.koth prunes the other axis.
+// the cut with the Nyquist column in the first free slot past the cut (or in
+// a tile of its own when the cut fills the last low tile); a.koth prunes the
+// other axis.
 template <typename T>
 static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int kind = DNSBOX_PASS_OTHER) {
   const int n = axis == 2 ? c->p.nz : c->p.ny;
@@ -294,7 +296,9 @@ static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int 
   if (a.kcol.a) {
     a.ntx_lo = (a.kcol.a + width - 1) / width;
     const int nt = (c->p.nx / 2) / width;
-    a.nyq_tile = nt < a.ntx_lo ? 0 : nt;   // > 0: the Nyquist column's tile follows the low tiles
+    // 0: the Nyquist column lies in the low tiles; < 0: it takes the free slot
+    // kx = kcol.a of the last low tile; > 0: its own tile follows the low tiles
+    a.nyq_tile = nt < a.ntx_lo ? 0 : (a.kcol.a % width ? -1 : nt);
   } else {
     a.ntx_lo = 0;   // full grid
     a.nyq_tile = 0;

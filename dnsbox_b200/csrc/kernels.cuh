@@ -99,7 +99,9 @@ template <typename T> struct StridedArgs {
   // grid): kept kx columns, kept other-axis indices (the tile grid covers only
   // these), kept input rows (others read as 0) and kept output rows (others
   // not stored).  Column tiles: all ceil(ncols / width) when ntx_lo = 0, else
-  // [0, ntx_lo) followed by tile nyq_tile when nyq_tile > 0.
+  // [0, ntx_lo) followed by tile nyq_tile when nyq_tile > 0; nyq_tile < 0
+  // places the Nyquist column in the free slot kx = kcol.a of the last low
+  // tile (see strided_col).
   AxisKeep kcol, koth, krin, krout;
   int ntx_lo, nyq_tile;
 };
@@ -108,6 +110,14 @@ template <typename T> struct StridedArgs {
 template <typename T>
 __host__ __device__ __forceinline__ int strided_ntx(const StridedArgs<T> &a, int tcw) {
   return a.ntx_lo ? a.ntx_lo + (a.nyq_tile > 0 ? 1 : 0) : (a.ncols + tcw - 1) / tcw;
+}
+
+// Half-axis index held by tile column kx0 + c: the identity, except in the
+// merged layout (nyq_tile < 0), where the first column past the cut holds the
+// Nyquist column kcol.n / 2.
+template <typename T>
+__host__ __device__ __forceinline__ int strided_col(const StridedArgs<T> &a, int kx) {
+  return (a.nyq_tile < 0 && kx == a.kcol.a) ? (a.kcol.n >> 1) : kx;
 }
 
 // Column origin and other-axis index of tile t of the (possibly pruned) grid.
@@ -143,7 +153,7 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
   const StridedJob<T> &J = a.job[job];
   const bool act = threadIdx.x < NF;
   const int col = threadIdx.x % TC, p = threadIdx.x / TC;
-  const int kx = kx0 + col;
+  const int kx = strided_col(a, kx0 + col);
   const bool valid = act && kx < a.ncols && a.kcol.keep(kx);
   const long long base = (long long)other * a.otherstride + kx + (long long)blockIdx.y * a.bstride;
   C v[E];
@@ -647,6 +657,7 @@ template <typename T> struct FinishArgs {
   int bandlim, spherical, mode, ab2_standard;
   double s;                // scalemodes
   AxisKeep kx, ky;         // pruning: column tiles outside the kept set are skipped (zero partials)
+  AxisKeep kz;             // pruning: cut kz rows are neither read nor written (their modes stay zero)
 };
 
 template <typename T, int N>
@@ -722,24 +733,32 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
   double esum = 0.0, dsum = 0.0;
   if (valid) {
     const bool need_u = a.bandlim || a.mode != FIN_RHS;
+    unsigned kzkeep = 0;   // bit i: output row i of this thread is a kept kz
+#pragma unroll
+    for (int i = 0; i < E; ++i) kzkeep |= (a.kz.keep(EN::out_row(p, i)) ? 1u : 0u) << i;
 #pragma unroll
     for (int i0 = 0; i0 < E; i0 += CH) {
       // batch the global operands of CH modes before any store
       C uu[CH][3], ss[CH][3], no[CH][3];
 #pragma unroll
       for (int h = 0; h < CH; ++h) {
-        const long long idx = (long long)EN::out_row(p, i0 + h) * rowstride + base;
+        const int kz = EN::out_row(p, i0 + h);
+        const long long idx = (long long)kz * rowstride + base;
+        const bool kept = (kzkeep >> (i0 + h)) & 1u;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          uu[h][c] = need_u ? a.uin[c * a.nh + idx] : mkc<C>(0, 0);
-          ss[h][c] = a.mode == FIN_CORR ? a.state[c * a.nh + idx] : mkc<C>(0, 0);
-          no[h][c] = a.mode == FIN_AB2 ? a.nold[c * a.nh + idx] : mkc<C>(0, 0);
+          uu[h][c] = need_u && kept ? a.uin[c * a.nh + idx] : mkc<C>(0, 0);
+          ss[h][c] = a.mode == FIN_CORR && kept ? a.state[c * a.nh + idx] : mkc<C>(0, 0);
+          no[h][c] = a.mode == FIN_AB2 && kept ? a.nold[c * a.nh + idx] : mkc<C>(0, 0);
         }
       }
 #pragma unroll
       for (int h = 0; h < CH; ++h) {
         const int i = i0 + h;
         const int kz = EN::out_row(p, i);
+        // pruned: a cut kz row (operands read as zero above) has N = 0 and a
+        // zero update, which adds nothing to E and D and is not stored
+        const bool kept = (kzkeep >> i) & 1u;
         const long long idx = (long long)kz * rowstride + base;
         const double kzr = k_full(kz, N, a.az);
         const double k2 = kxr * kxr + kyr * kyr + kzr * kzr;
@@ -775,7 +794,8 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
         }
         if (a.mode == FIN_RHS) {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) a.out[c * a.nh + idx] = Nc[c];
+          for (int c = 0; c < 3; ++c)
+            if (kept) a.out[c * a.nh + idx] = Nc[c];
           continue;
         }
         const T IF = T(exp((a.Q - nu * k2) * dt));
@@ -784,8 +804,8 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             const C u = uu[h][c];
-            a.out[c * a.nh + idx] = mkc<C>((u.x + tdt * Nc[c].x) * IF, (u.y + tdt * Nc[c].y) * IF);
-            if (a.nold) a.nold[c * a.nh + idx] = Nc[c];
+            if (kept) a.out[c * a.nh + idx] = mkc<C>((u.x + tdt * Nc[c].x) * IF, (u.y + tdt * Nc[c].y) * IF);
+            if (a.nold && kept) a.nold[c * a.nh + idx] = Nc[c];
           }
           continue;
         }
@@ -796,7 +816,7 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
           for (int c = 0; c < 3; ++c) {
             const C u = ss[h][c], us = uu[h][c];
             un[c] = mkc<C>(hf * (IF * u.x + us.x) + hdt * Nc[c].x, hf * (IF * u.y + us.y) + hdt * Nc[c].y);
-            a.state[c * a.nh + idx] = un[c];
+            if (kept) a.state[c * a.nh + idx] = un[c];
           }
         } else {  // FIN_AB2
           const T e1c1 = T(c1) * IF;
@@ -805,8 +825,10 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
           for (int c = 0; c < 3; ++c) {
             const C u = uu[h][c], o = no[h][c];
             un[c] = mkc<C>(IF * u.x + e1c1 * Nc[c].x + e2c2 * o.x, IF * u.y + e1c1 * Nc[c].y + e2c2 * o.y);
-            a.state[c * a.nh + idx] = un[c];
-            a.nold[c * a.nh + idx] = Nc[c];
+            if (kept) {
+              a.state[c * a.nh + idx] = un[c];
+              a.nold[c * a.nh + idx] = Nc[c];
+            }
           }
         }
         double e2 = 0;

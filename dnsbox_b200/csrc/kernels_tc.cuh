@@ -198,6 +198,27 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
   // while the current tile is processed.
   C y[RUNS][8];
   TcItem nxt;   // decoded work item of the tile being fetched
+  // Row offsets within one field fit in 32 bits (the launcher checks
+  // N * rowstride < 2^31); the 64-bit part is the per-tile base.
+  const int rs = (int)a.rowstride;
+  // Kept-row masks, fixed per thread for the whole launch: bit 8 h + i for
+  // input row N2 (8 q + i) + n2 of run h, bit N2 r + k2 for output row
+  // k1 + 64 k2 of stage-2 item r.
+  constexpr int R2 = (64 * TCW + NT - 1) / NT;   // stage-2 items per thread
+  unsigned inmask = 0, outmask = 0;
+#pragma unroll
+  for (int h = 0; h < RUNS; ++h) {
+    const int u = t + NT * h;
+    const int n2 = (u / TCW) % N2, q = u / 64;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) inmask |= (a.krin.keep(N2 * (8 * q + i) + n2) ? 1u : 0u) << (8 * h + i);
+  }
+#pragma unroll
+  for (int r = 0; r < R2; ++r) {
+    const int k1 = (t + NT * r) / TCW;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) outmask |= (a.krout.keep(k1 + 64 * k2) ? 1u : 0u) << (N2 * r + k2);
+  }
   auto fetch = [&](unsigned w) {
     nxt = tc_item<TCW>(a, g, w);
     const TcItem &it = nxt;
@@ -206,18 +227,20 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
     for (int h = 0; h < RUNS; ++h) {
       const int u = t + NT * h;
       const int c = u % TCW, n2 = (u / TCW) % N2, q = u / 64;
-      const bool valid = it.kx0 + c < a.ncols && a.kcol.keep(it.kx0 + c);
-      const long long off = it.base0 + c + (long long)(N2 * 8 * q + n2) * a.rowstride;
+      const int dc = strided_col(a, it.kx0 + c) - it.kx0;   // column offset from the tile origin
+      const bool valid = it.kx0 + dc < a.ncols && a.kcol.keep(it.kx0 + dc);
+      const int roff = (N2 * 8 * q + n2) * rs;
+      const C *src1 = J.in1 + (it.base0 + dc);
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const bool vi = valid && a.krin.keep(N2 * (8 * q + i) + n2);
-        cp_async8(ring + (8 * h + i) * NT + t, J.in1 + (vi ? off + (long long)(N2 * i) * a.rowstride : 0), vi);
+        const bool vi = valid && ((inmask >> (8 * h + i)) & 1u);
+        cp_async8(ring + (8 * h + i) * NT + t, vi ? src1 + (roff + N2 * i * rs) : J.in1, vi);
       }
       if (J.in2) {
+        const C *src2 = J.in2 + (it.base0 + dc);
 #pragma unroll
         for (int i = 0; i < 8; ++i)
-          y[h][i] = (valid && a.krin.keep(N2 * (8 * q + i) + n2)) ? J.in2[off + (long long)(N2 * i) * a.rowstride]
-                                                                    : mkc<C>(0.f, 0.f);
+          y[h][i] = (valid && ((inmask >> (8 * h + i)) & 1u)) ? src2[roff + N2 * i * rs] : mkc<C>(0.f, 0.f);
       }
     }
     cp_async_commit();
@@ -242,7 +265,7 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
       for (int h = 0; h < RUNS; ++h) {
         const int u = t + NT * h;
         const int c = u % TCW, n2 = (u / TCW) % N2, q = u / 64;
-        const float kcol = (float)k_half(it.kx0 + c, a.nx, a.alpha_x);
+        const float kcol = (float)k_half(strided_col(a, it.kx0 + c), a.nx, a.alpha_x);
         const float kc1 = J.ks1 == 2 ? koth : kcol, kc2 = J.ks2 == 2 ? koth : kcol;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -355,7 +378,9 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
     __syncthreads();
     // 5. unscale, twiddle, N2-point DFT, store; item (k1, c), c fastest
 #pragma unroll
-    for (int idx = t; idx < 64 * TCW; idx += NT) {
+    for (int r = 0; r < R2; ++r) {
+      const int idx = t + NT * r;
+      if ((64 * TCW) % NT != 0 && idx >= 64 * TCW) break;
       const int cc = idx % TCW, k1 = idx / TCW;
       const int sw = tc_swz<LG_R>(k1), swi = sw ^ XIM;
       C z[N2];
@@ -371,11 +396,12 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
         z[m2] = yy;
       }
       dft<N2, C, INV>(z);
-      if (it.kx0 + cc < a.ncols && a.kcol.keep(it.kx0 + cc)) {
-        C *out = J.out + it.base0 + cc;
+      const int dc = strided_col(a, it.kx0 + cc) - it.kx0;
+      if (it.kx0 + dc < a.ncols && a.kcol.keep(it.kx0 + dc)) {
+        C *out = J.out + (it.base0 + dc);
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2)
-          if (a.krout.keep(k1 + 64 * k2)) out[(long long)(k1 + 64 * k2) * a.rowstride] = z[k2];
+          if ((outmask >> (N2 * r + k2)) & 1u) out[(k1 + 64 * k2) * rs] = z[k2];
       }
     }
     __syncthreads();

@@ -78,6 +78,7 @@ cudaError_t Launcher<T, N>::strided_tc(const StridedArgs<T> &a, bool inv, int no
     const long long total = (long long)a.njobs * g.ntx * nother * (a.nbatch > 0 ? a.nbatch : 1);
     if (total == 0) return cudaSuccess;
     if (total + 2LL * nctas >= (1LL << 31)) return cudaErrorInvalidValue;
+    if ((long long)N * a.rowstride >= (1LL << 31)) return cudaErrorInvalidValue;   // 32-bit row offsets
     g.total = (int)total;
     g.per_box.init((unsigned)(a.njobs * g.ntx * nother));
     g.njobs.init((unsigned)a.njobs);
