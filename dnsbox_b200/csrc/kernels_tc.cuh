@@ -164,8 +164,10 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
   __shared__ float usc[64];            // this tile's per-pencil unscale factors 2^e
   __shared__ float krow[N];            // wavenumber of each row index along the transformed axis
   __shared__ StridedJob<float> sjob[6];   // the job table (read with a per-tile index)
+  __shared__ C tws[(N2 - 1) * 64];        // stage-2 twiddles W_N^(m2 k1), m2 = 1 .. N2-1
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   if (t < a.njobs) sjob[t] = a.job[t];
+  for (int i = t; i < (N2 - 1) * 64; i += NT) tws[i] = a.tw[(i / 64 + 1) * (i % 64)];
   for (int n = t; n < N; n += NT) krow[n] = (float)k_full(n, N, a.alpha_row);
   {
     const uint4 *src = reinterpret_cast<const uint4 *>(Adft);
@@ -390,7 +392,7 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
         const float us = usc[jj];
         C yy = mkc<C>(sD[k1 * 64 + (jj ^ sw)] * us, sD[(64 + k1) * 64 + (jj ^ swi)] * us);
         if (m2) {
-          const C tw = __ldg(&a.tw[m2 * k1]);
+          const C tw = tws[(m2 - 1) * 64 + k1];
           yy = INV ? cmulc(yy, tw) : cmul(yy, tw);
         }
         z[m2] = yy;
