@@ -42,7 +42,7 @@ WORKLOAD = dict(n=256, k0=3.0, nu=2e-3, kCutOff=2.5, Pin=0.1, courant=0.5, dt_ma
 # Algorithmic HBM traffic per launch of each pass, in spectral-field units
 # (one field = nz*ny*(nx/2+1) complex values): reads + writes, each field once.
 PASS_FIELDS_HEUN = {"z_inv": [8, 8], "y_inv": [11, 11], "x_nl": [9, 9], "y_fwd": [6, 6],
-                    "z_fin": [9, 12]}
+                    "z_fwd": [6, 6], "z_fin": [9, 12]}
 
 
 def pruned_pass_fields(n):
@@ -53,8 +53,9 @@ def pruned_pass_fields(n):
     fx = (a + 1) / (n // 2 + 1)
     fy = fz = 2 * a / n
     fxy = fx * fy
-    return {"z_inv": [3 * fxy * fz + 5 * fxy] * 2, "y_inv": [5 * fxy + 6 * fx] * 2, "x_nl": [9 * fx] * 2,
-            "y_fwd": [3 * fx + 3 * fxy] * 2, "z_fin": [9 * fxy, 12 * fxy]}
+    fxyz = fxy * fz
+    return {"z_inv": [3 * fxyz + 5 * fxy] * 2, "y_inv": [5 * fxy + 6 * fx] * 2, "x_nl": [9 * fx] * 2,
+            "y_fwd": [3 * fx + 3 * fxy] * 2, "z_fwd": [3 * fxy + 3 * fxyz] * 2, "z_fin": [9 * fxyz, 12 * fxyz]}
 
 
 def log(*a):

@@ -54,7 +54,7 @@ class Diag(ctypes.Structure):
 
 
 NPASS = 8
-PASS_NAMES = ["z_inv", "y_inv", "x_nl", "y_fwd", "z_fin", "small", "other", "reserved"]
+PASS_NAMES = ["z_inv", "y_inv", "x_nl", "y_fwd", "z_fin", "small", "other", "z_fwd"]
 
 
 class Profile(ctypes.Structure):

@@ -322,7 +322,7 @@ __global__ void k_axpy(const C *x, const C *d, C *y, long long n, double alpha) 
   }
 }
 
-// out = IF (u + dt n), IF = exp((Q - nu |k|^2) dt): the FIN_PRED arithmetic of k_zfinish
+// out = IF (u + dt n), IF = exp((Q - nu |k|^2) dt): the FIN_PRED arithmetic of k_finish_rows
 template <typename C>
 __global__ void k_if_pred(const C *u, const C *n, C *out, long long nh, Grid3 gr, double nu, double Q, double dt) {
   using T = decltype(C{}.x);

@@ -90,7 +90,30 @@ __global__ void k_cfl(StepState *sts, int nbatch, double dx, double dy, double d
 
 // Sums the finish-kernel partials (fixed order), writes the step record and
 // advances the clock.
-// one block per box
+// Per-plane sums of the spectral finish's row partials: block (kz, box) adds
+// the (E, D) pairs of the ny rows of plane kz in a fixed order.  Rows and
+// planes outside the kept ky / kz sets of a pruned step were not visited and
+// count as zero.
+__global__ void k_plane_sums(const double *rows, double *planes, int nz, int ny, AxisKeep ky, AxisKeep kz) {
+  __shared__ double red[2 * 32];
+  const int iz = blockIdx.x, box = blockIdx.y;
+  const double *r = rows + 2 * ((long long)box * nz + iz) * ny;
+  double e = 0.0, d = 0.0;
+  if (kz.keep(iz))
+    for (int j = threadIdx.x; j < ny; j += blockDim.x)
+      if (ky.keep(j)) {
+        e += r[2 * j];
+        d += r[2 * j + 1];
+      }
+  double v[2] = {e, d};
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    planes[2 * ((long long)box * nz + iz)] = v[0];
+    planes[2 * ((long long)box * nz + iz) + 1] = v[1];
+  }
+}
+
+// one block per box; partials: np (E, D) pairs per box (the plane sums)
 __global__ void k_finalize(StepState *sts, const double *partials, int np, double s2, double nu,
                            const double *nu_box, double Q, double Pin, int bandlim, dnsbox_diag *ring,
                            int ring_cap) {
@@ -480,7 +503,18 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
     d.krout = c->keep[1];
   }
   RET(run_strided<T>(c, 1, false, d, DNSBOX_PASS_Y_FWD));
-  // pass E: forward z + spectral finish
+  // pass E1: forward z of the three components, in place (the SIMT kernel in
+  // every form); pruned: kept kx columns and ky tiles, kept kz rows written
+  StridedArgs<T> z = strided_base<T>(c, 2);
+  z.njobs = 3;
+  for (int f = 0; f < 3; ++f) set_job<T>(z, f, field(c->W2, c, f), field(c->W2, c, f));
+  if (pruned) {
+    z.kcol = c->keep[0];
+    z.koth = c->keep[1];
+    z.krout = c->keep[2];
+  }
+  RET(run_strided<T>(c, 2, false, z, DNSBOX_PASS_Z_FWD, false));
+  // pass E2: spectral finish, one warp per (kz, ky) row
   FinishArgs<T> e = finish_base<T>(c);
   e.n3 = reinterpret_cast<const C *>(c->W2);
   e.uin = reinterpret_cast<const C *>(uin);
@@ -493,15 +527,19 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   e.nh = (long long)c->fstride;
   e.bstride = (long long)c->nh;
   e.mode = mode;
-  if (pruned) {
-    e.kx = c->keep[0];
-    e.ky = c->keep[1];
-    e.kz = c->keep[2];
-  }
-  const int ztc = Ops<T>::zfinish_cols(p.nz);
-  const int ntx = (c->nxh + ztc - 1) / ztc;
+  e.kx = pruned ? c->keep[0] : AxisKeep{0, p.nx, 0};
+  e.ky = pruned ? c->keep[1] : AxisKeep{0, p.ny, 1};
+  e.kz = pruned ? c->keep[2] : AxisKeep{0, p.nz, 1};
+  const int nrows = e.kz.count() * e.ky.count();
   Prof pr(c, DNSBOX_PASS_Z_FIN);
-  CK(Ops<T>::zfinish(p.nz, e, ntx * p.ny, c->nbatch, c->stream));
+  const dim3 grid((unsigned)((nrows + 7) / 8), (unsigned)c->nbatch);
+  switch (mode) {
+    case FIN_RHS: k_finish_rows<T, FIN_RHS><<<grid, 256, 0, c->stream>>>(e, nrows); break;
+    case FIN_PRED: k_finish_rows<T, FIN_PRED><<<grid, 256, 0, c->stream>>>(e, nrows); break;
+    case FIN_CORR: k_finish_rows<T, FIN_CORR><<<grid, 256, 0, c->stream>>>(e, nrows); break;
+    default: k_finish_rows<T, FIN_AB2><<<grid, 256, 0, c->stream>>>(e, nrows); break;
+  }
+  CK(cudaGetLastError());
   return DNSBOX_OK;
 }
 
@@ -551,11 +589,15 @@ template <typename T> static int step_once(dnsbox_ctx *c, void *uh) {
     // dnsbox.f90:143-191
     RET(run_rhs<T>(c, uh, FIN_AB2, nullptr, uh, c->nold, true, 1, nullptr, c->prune_now));
   }
-  const int ztc = Ops<T>::zfinish_cols(p.nz);
-  const int ntx = (c->nxh + ztc - 1) / ztc;
-  Prof pr(c, DNSBOX_PASS_SMALL);
-  k_finalize<<<c->nbatch, 1024, 0, c->stream>>>(c->st, c->partials, ntx * p.ny, s * s, p.nu, c->d_nu, p.Q, p.Pin,
-                                                 p.bandlim, c->ddiag, c->ring_cap);
+  const AxisKeep ky = c->prune_now ? c->keep[1] : AxisKeep{0, p.ny, 1};
+  const AxisKeep kz = c->prune_now ? c->keep[2] : AxisKeep{0, p.nz, 1};
+  double *planes = c->partials + 2 * (size_t)c->npartials * c->nbatch;
+  Prof pr(c, DNSBOX_PASS_SMALL, 2);
+  k_plane_sums<<<dim3((unsigned)p.nz, (unsigned)c->nbatch), 256, 0, c->stream>>>(c->partials, planes, p.nz, p.ny, ky,
+                                                                                 kz);
+  CK(cudaGetLastError());
+  k_finalize<<<c->nbatch, 1024, 0, c->stream>>>(c->st, planes, p.nz, s * s, p.nu, c->d_nu, p.Q, p.Pin, p.bandlim,
+                                                 c->ddiag, c->ring_cap);
   CK(cudaGetLastError());
   c->host_step += 1;
   return DNSBOX_OK;
@@ -753,11 +795,8 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
         (c->nold && (e = cudaMemset(c->nold, 0, 3 * fb)) != cudaSuccess))
       return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
   }
-  {
-    const int ztc = c->fp64 ? Ops<double>::zfinish_cols(p->nz) : Ops<float>::zfinish_cols(p->nz);
-    c->npartials = ((c->nxh + ztc - 1) / ztc) * p->ny;
-  }
-  if ((e = cudaMalloc(&c->partials, 2 * (size_t)c->npartials * c->nbatch * sizeof(double))) != cudaSuccess)
+  c->npartials = p->nz * p->ny;   // one (E, D) pair per (kz, ky) row, then one per kz plane
+  if ((e = cudaMalloc(&c->partials, 2 * (size_t)(c->npartials + p->nz) * c->nbatch * sizeof(double))) != cudaSuccess)
     return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed"));
   // band modes |k| <= kCutOff (rhs.f90:145-149), stored as (offset lo, offset hi, kx)
   std::vector<int> band;

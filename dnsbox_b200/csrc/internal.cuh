@@ -197,18 +197,6 @@ template <typename T> struct Ops {
     switch (n) { DNSBOX_SIZES(DNSBOX_CASE_R2C) }
     return cudaErrorInvalidValue;
   }
-#define DNSBOX_CASE_FINC(NN) \
-  case NN: return Launcher<T, NN>::zfinish_cols();
-  static int zfinish_cols(int n) {
-    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_FINC) }
-    return 1;
-  }
-#define DNSBOX_CASE_FIN(NN) \
-  case NN: return Launcher<T, NN>::zfinish(a, nb, nbatch, st);
-  static cudaError_t zfinish(int n, const FinishArgs<T> &a, int nb, int nbatch, cudaStream_t st) {
-    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_FIN) }
-    return cudaErrorInvalidValue;
-  }
 };
 
 // ---------------------------------------------------------------- helpers
@@ -289,9 +277,10 @@ static void set_job(StridedArgs<T> &a, int j, const void *in1, void *out, double
 // a tile of its own when the cut fills the last low tile); a.koth prunes the
 // other axis.
 template <typename T>
-static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int kind = DNSBOX_PASS_OTHER) {
+static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int kind = DNSBOX_PASS_OTHER,
+                       bool allow_tc = true) {
   const int n = axis == 2 ? c->p.nz : c->p.ny;
-  const bool tc = c->tc && Ops<T>::has_tc(n);
+  const bool tc = allow_tc && c->tc && Ops<T>::has_tc(n);
   const int width = tc ? 4096 / n : TileCols<T>::v;
   if (a.kcol.a) {
     a.ntx_lo = (a.kcol.a + width - 1) / width;

@@ -9,10 +9,10 @@
 //             curl into the inverse transforms;
 //   x       : k_xline_*  -- whole lines along x, two real lines per complex FFT.
 // The nonlinear term fuses the last inverse x pass, the u x omega product, the
-// max|u_i| (CFL) reduction and the first forward x pass (k_xline_nl); the last
-// forward z pass is fused with dealiasing, pressure projection, band forcing,
-// the integrating-factor stepper and the energy/dissipation reductions
-// (k_zfinish).
+// max|u_i| (CFL) reduction and the first forward x pass (k_xline_nl); after
+// the last forward z pass (k_strided, in place) one streaming kernel applies
+// dealiasing, pressure projection, band forcing, the integrating-factor
+// stepper and the energy/dissipation row sums (k_finish_rows).
 #pragma once
 
 #include <type_traits>
@@ -65,11 +65,6 @@ struct AxisKeep {
 template <typename T> struct TileCols;
 template <> struct TileCols<double> { static constexpr int v = 8; };
 template <> struct TileCols<float> { static constexpr int v = 16; };
-// Tile width of the fused z finish, which holds three N-row tiles in shared
-// memory (halved at N = 1024 to stay within 227 KB per CTA).
-template <typename T, int N> struct FinishCols {
-  static constexpr int v = (N >= 1024 || (N >= 512 && sizeof(T) == 4)) ? TileCols<T>::v / 2 : TileCols<T>::v;
-};
 
 template <typename T> struct StridedJob {
   using C = typename CT<T>::type;
@@ -638,7 +633,7 @@ enum FinishMode : int {
 
 template <typename T> struct FinishArgs {
   using C = typename CT<T>::type;
-  const C *n3;             // 3 fields (kx, ky, z) after the forward y pass
+  const C *n3;             // 3 fields (kx, ky, kz): the nonlinear term after the forward z pass
   const C *uin;            // 3 fields, RHS input (forcing)
   C *out;                  // FIN_RHS / FIN_PRED output (3 fields)
   C *state;                // FIN_CORR state (3 fields)
@@ -656,66 +651,37 @@ template <typename T> struct FinishArgs {
   double cutx, cuty, cutz, sph2;
   int bandlim, spherical, mode, ab2_standard;
   double s;                // scalemodes
-  AxisKeep kx, ky;         // pruning: column tiles outside the kept set are skipped (zero partials)
-  AxisKeep kz;             // pruning: cut kz rows are neither read nor written (their modes stay zero)
+  AxisKeep kx, ky, kz;     // pruning: only kept (kz, ky) rows and kept kx modes are visited
 };
 
-template <typename T, int N>
-__global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::E)),
-                                  min_ctas(round32(FinishCols<T, N>::v *(N / FftPlan<N>::E)), 2))
-    k_zfinish(const __grid_constant__ FinishArgs<T> a) {
+// Spectral finish after the forward z transform (the second half of one
+// right-hand side's pass E): per mode the 2/3 mask, the pressure projection,
+// band or fixed forcing and the integrating-factor update, one warp per
+// (kz, ky) row of kx modes.  n3 holds the z-transformed nonlinear term.  Rows
+// run over the kept kz and ky indices (every row when not pruning) and cut kx
+// modes are skipped; the row's E and D sums (fixed lane order) go to
+// partials[kz ny + ky] of the box, and the finalize reads the rows a pruned
+// launch does not visit as zero.  Each lane batches the global operands of
+// two modes before any store.  MODE (a FinishMode) is a template parameter so
+// that only the operands of the update in use occupy registers.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_finish_rows(const __grid_constant__ FinishArgs<T> a, int nrows) {
   using C = typename CT<T>::type;
-  using EN = FftEnds<N>;
-  constexpr int TC = FinishCols<T, N>::v;
-  constexpr int E = EN::E;
-  constexpr int NF = TC * (N / E);
-  // modes per batch of global loads (E is even); one for FP64 at N >= 512,
-  // whose 512-thread blocks have 128 registers a thread
-  constexpr int CH = (sizeof(T) == 8 && N >= 512) ? 1 : 2;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *s = reinterpret_cast<C *>(smem_raw);   // three N x TC tiles, one per component
-  __shared__ double red[2 * 32];
-  const int ntx = (a.nxh + TC - 1) / TC;
-  const int ky = blockIdx.x / ntx;
-  const int kx0 = (blockIdx.x - ky * ntx) * TC;
-  const long long rowstride = (long long)a.ny * a.nxh;
-  const bool act = threadIdx.x < NF;
-  const int col = threadIdx.x % TC, p = threadIdx.x / TC;
-  const int kx = kx0 + col;
-  const bool valid = act && kx < a.nxh && a.kx.keep(kx);
+  constexpr int CH = 2;
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= nrows) return;   // whole warps: no block-level synchronisation below
+  const int nky = a.ky.count();
+  const int oz = w / nky;
+  const int kz = a.kz.map(oz), ky = a.ky.map(w - oz * nky);
   const int box = blockIdx.y;
-  const long long base = (long long)ky * a.nxh + kx + (long long)box * a.bstride;
-  // pruned column tile: every mode is masked and the state there is zero
-  if (!a.ky.keep(ky) || !(a.kx.a == 0 || kx0 < a.kx.a || (kx0 <= (a.nx >> 1) && (a.nx >> 1) < kx0 + TC))) {
-    if (a.partials && threadIdx.x == 0) {
-      double *pp = a.partials + 2 * ((long long)box * gridDim.x + blockIdx.x);
-      pp[0] = 0.0;
-      pp[1] = 0.0;
-    }
-    return;
-  }
-  // forward z transforms of the three components, each using its own tile as
-  // scratch; fields 0 and 1 park their outputs in this thread's own slots of
-  // tiles 0 and 1, field 2 stays in v
-  C v[E];
-  for (int f = 0; f < 3; ++f) {
-    const C *src = a.n3 + f * a.nh + base;
-#pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = valid ? src[(long long)EN::in_row(p, i) * rowstride] : mkc<C>(0, 0);
-    C *tile = s + f * N * TC;
-    fft_regs<C, N, false>(v, tile, TC, col, p, act, a.tw);
-    if (f < 2 && act) {
-#pragma unroll
-      for (int i = 0; i < E; ++i) tile[EN::out_row(p, i) * TC + col] = v[i];
-    }
-  }
-
+  const long long rowbase = ((long long)kz * a.ny + ky) * a.nxh + (long long)box * a.bstride;
   const StepState *st = a.st + box;
   const double nu = a.nu_box ? a.nu_box[box] : a.nu;
   const double dt = st->dt;
   const double fc = a.bandlim ? a.Pin / (2.0 * st->eband) : 0.0;
   double c1 = 0, c2 = 0, tau2 = 0;
-  if (a.mode == FIN_AB2) {
+  if (MODE == FIN_AB2) {
     const double tn = st->t, tm = st->t_prev;
     if (a.ab2_standard) {
       const double h = tn - tm;
@@ -728,126 +694,115 @@ __global__ void __launch_bounds__(round32(FinishCols<T, N>::v *(N / FftPlan<N>::
     tau2 = dt + tn - tm;
   }
   const double kyr = k_full(ky, a.ny, a.ay);
-  const double kxr = k_half(kx, a.nx, a.ax);
-  const double wk = (kxr == 0.0) ? 0.5 : 1.0;   // state.f90:436-440
+  const double kzr = k_full(kz, a.nz, a.az);
+  const bool need_u = a.bandlim || MODE != FIN_RHS;
   double esum = 0.0, dsum = 0.0;
-  if (valid) {
-    const bool need_u = a.bandlim || a.mode != FIN_RHS;
-    unsigned kzkeep = 0;   // bit i: output row i of this thread is a kept kz
+  for (int kx0 = lane; kx0 < a.nxh; kx0 += 32 * CH) {
+    C nn[CH][3], uu[CH][3], ss[CH][3], no[CH][3];
+    bool ok[CH];
 #pragma unroll
-    for (int i = 0; i < E; ++i) kzkeep |= (a.kz.keep(EN::out_row(p, i)) ? 1u : 0u) << i;
+    for (int h = 0; h < CH; ++h) {
+      const int kx = kx0 + 32 * h;
+      ok[h] = kx < a.nxh && a.kx.keep(kx);
+      const long long idx = rowbase + kx;
 #pragma unroll
-    for (int i0 = 0; i0 < E; i0 += CH) {
-      // batch the global operands of CH modes before any store
-      C uu[CH][3], ss[CH][3], no[CH][3];
+      for (int c = 0; c < 3; ++c) {
+        nn[h][c] = ok[h] ? a.n3[c * a.nh + idx] : mkc<C>(0, 0);
+        uu[h][c] = ok[h] && need_u ? a.uin[c * a.nh + idx] : mkc<C>(0, 0);
+        ss[h][c] = ok[h] && MODE == FIN_CORR ? a.state[c * a.nh + idx] : mkc<C>(0, 0);
+        no[h][c] = ok[h] && MODE == FIN_AB2 ? a.nold[c * a.nh + idx] : mkc<C>(0, 0);
+      }
+    }
 #pragma unroll
-      for (int h = 0; h < CH; ++h) {
-        const int kz = EN::out_row(p, i0 + h);
-        const long long idx = (long long)kz * rowstride + base;
-        const bool kept = (kzkeep >> (i0 + h)) & 1u;
+    for (int h = 0; h < CH; ++h) {
+      if (!ok[h]) continue;
+      const int kx = kx0 + 32 * h;
+      const long long idx = rowbase + kx;
+      const double kxr = k_half(kx, a.nx, a.ax);
+      const double wk = (kxr == 0.0) ? 0.5 : 1.0;   // state.f90:436-440
+      const double k2 = kxr * kxr + kyr * kyr + kzr * kzr;
+      const bool zero = (kxr == 0.0) && (kyr == 0.0) && (kzr == 0.0);
+      const bool cut = (a.spherical && k2 >= a.sph2) || fabs(kxr) >= a.cutx || fabs(kyr) >= a.cuty ||
+                       fabs(kzr) >= a.cutz || zero;
+      C Nc[3];
+      if (cut) {
+        Nc[0] = Nc[1] = Nc[2] = mkc<C>(0, 0);
+      } else {
+        // phat = -(i k . n) / (-(k.k))  (rhs.f90:101-106)
+        const double knre = kxr * (double)nn[h][0].x + kyr * (double)nn[h][1].x + kzr * (double)nn[h][2].x;
+        const double knim = kxr * (double)nn[h][0].y + kyr * (double)nn[h][1].y + kzr * (double)nn[h][2].y;
+        const double pre = -knim / k2, pim = knre / k2;
+        const double kr[3] = {kxr, kyr, kzr};
+        const bool forced = a.bandlim && sqrt(k2) <= a.kcut;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          uu[h][c] = need_u && kept ? a.uin[c * a.nh + idx] : mkc<C>(0, 0);
-          ss[h][c] = a.mode == FIN_CORR && kept ? a.state[c * a.nh + idx] : mkc<C>(0, 0);
-          no[h][c] = a.mode == FIN_AB2 && kept ? a.nold[c * a.nh + idx] : mkc<C>(0, 0);
+          double re = -(double)nn[h][c].x + kr[c] * pim;
+          double im = -(double)nn[h][c].y - kr[c] * pre;
+          if (forced) {
+            re += fc * (double)uu[h][c].x;
+            im += fc * (double)uu[h][c].y;
+          }
+          if (a.force) {
+            const C q = a.force[c * a.nh + idx];
+            re += (double)q.x;
+            im += (double)q.y;
+          }
+          Nc[c] = mkc<C>(T(re), T(im));
         }
       }
+      if (MODE == FIN_RHS) {
 #pragma unroll
-      for (int h = 0; h < CH; ++h) {
-        const int i = i0 + h;
-        const int kz = EN::out_row(p, i);
-        // pruned: a cut kz row (operands read as zero above) has N = 0 and a
-        // zero update, which adds nothing to E and D and is not stored
-        const bool kept = (kzkeep >> i) & 1u;
-        const long long idx = (long long)kz * rowstride + base;
-        const double kzr = k_full(kz, N, a.az);
-        const double k2 = kxr * kxr + kyr * kyr + kzr * kzr;
-        const bool zero = (kxr == 0.0) && (kyr == 0.0) && (kzr == 0.0);
-        const bool cut = (a.spherical && k2 >= a.sph2) || fabs(kxr) >= a.cutx || fabs(kyr) >= a.cuty ||
-                         fabs(kzr) >= a.cutz || zero;
-        C Nc[3];
-        if (cut) {
-          Nc[0] = Nc[1] = Nc[2] = mkc<C>(0, 0);
-        } else {
-          const C nn[3] = {s[kz * TC + col], s[N * TC + kz * TC + col], v[i]};
-          // phat = -(i k . n) / (-(k.k))  (rhs.f90:101-106)
-          const double knre = kxr * (double)nn[0].x + kyr * (double)nn[1].x + kzr * (double)nn[2].x;
-          const double knim = kxr * (double)nn[0].y + kyr * (double)nn[1].y + kzr * (double)nn[2].y;
-          const double pre = -knim / k2, pim = knre / k2;
-          const double kr[3] = {kxr, kyr, kzr};
-          const bool forced = a.bandlim && sqrt(k2) <= a.kcut;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            double re = -(double)nn[c].x + kr[c] * pim;
-            double im = -(double)nn[c].y - kr[c] * pre;
-            if (forced) {
-              re += fc * (double)uu[h][c].x;
-              im += fc * (double)uu[h][c].y;
-            }
-            if (a.force) {
-              const C q = a.force[c * a.nh + (long long)kz * rowstride + base];
-              re += (double)q.x;
-              im += (double)q.y;
-            }
-            Nc[c] = mkc<C>(T(re), T(im));
-          }
-        }
-        if (a.mode == FIN_RHS) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            if (kept) a.out[c * a.nh + idx] = Nc[c];
-          continue;
-        }
-        const T IF = T(exp((a.Q - nu * k2) * dt));
-        const T tdt = T(dt);
-        if (a.mode == FIN_PRED) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const C u = uu[h][c];
-            if (kept) a.out[c * a.nh + idx] = mkc<C>((u.x + tdt * Nc[c].x) * IF, (u.y + tdt * Nc[c].y) * IF);
-            if (a.nold && kept) a.nold[c * a.nh + idx] = Nc[c];
-          }
-          continue;
-        }
-        C un[3];
-        if (a.mode == FIN_CORR) {
-          const T hf = T(0.5), hdt = T(0.5 * dt);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const C u = ss[h][c], us = uu[h][c];
-            un[c] = mkc<C>(hf * (IF * u.x + us.x) + hdt * Nc[c].x, hf * (IF * u.y + us.y) + hdt * Nc[c].y);
-            if (kept) a.state[c * a.nh + idx] = un[c];
-          }
-        } else {  // FIN_AB2
-          const T e1c1 = T(c1) * IF;
-          const T e2c2 = T(c2 * exp((a.Q - nu * k2) * tau2));
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const C u = uu[h][c], o = no[h][c];
-            un[c] = mkc<C>(IF * u.x + e1c1 * Nc[c].x + e2c2 * o.x, IF * u.y + e1c1 * Nc[c].y + e2c2 * o.y);
-            if (kept) {
-              a.state[c * a.nh + idx] = un[c];
-              a.nold[c * a.nh + idx] = Nc[c];
-            }
-          }
-        }
-        double e2 = 0;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) e2 += (double)un[c].x * un[c].x + (double)un[c].y * un[c].y;
-        esum += wk * e2;
-        dsum += 2.0 * wk * k2 * e2;
+        for (int c = 0; c < 3; ++c) a.out[c * a.nh + idx] = Nc[c];
+        continue;
       }
+      const T IF = T(exp((a.Q - nu * k2) * dt));
+      const T tdt = T(dt);
+      if (MODE == FIN_PRED) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const C u = uu[h][c];
+          a.out[c * a.nh + idx] = mkc<C>((u.x + tdt * Nc[c].x) * IF, (u.y + tdt * Nc[c].y) * IF);
+          if (a.nold) a.nold[c * a.nh + idx] = Nc[c];
+        }
+        continue;
+      }
+      C un[3];
+      if (MODE == FIN_CORR) {
+        const T hf = T(0.5), hdt = T(0.5 * dt);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const C u = ss[h][c], us = uu[h][c];
+          un[c] = mkc<C>(hf * (IF * u.x + us.x) + hdt * Nc[c].x, hf * (IF * u.y + us.y) + hdt * Nc[c].y);
+          a.state[c * a.nh + idx] = un[c];
+        }
+      } else {  // FIN_AB2
+        const T e1c1 = T(c1) * IF;
+        const T e2c2 = T(c2 * exp((a.Q - nu * k2) * tau2));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const C u = uu[h][c], o = no[h][c];
+          un[c] = mkc<C>(IF * u.x + e1c1 * Nc[c].x + e2c2 * o.x, IF * u.y + e1c1 * Nc[c].y + e2c2 * o.y);
+          a.state[c * a.nh + idx] = un[c];
+          a.nold[c * a.nh + idx] = Nc[c];
+        }
+      }
+      double e2 = 0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) e2 += (double)un[c].x * un[c].x + (double)un[c].y * un[c].y;
+      esum += wk * e2;
+      dsum += 2.0 * wk * k2 * e2;
     }
   }
   if (a.partials) {
-    double r2[2] = {esum, dsum};
-    block_sum<2>(r2, red);
-    if (threadIdx.x == 0) {
-      double *pp = a.partials + 2 * ((long long)box * gridDim.x + blockIdx.x);
-      pp[0] = r2[0];
-      pp[1] = r2[1];
+    esum = warp_sum(esum);
+    dsum = warp_sum(dsum);
+    if (lane == 0) {
+      double *pp = a.partials + 2 * ((long long)box * a.nz * a.ny + (long long)kz * a.ny + ky);
+      pp[0] = esum;
+      pp[1] = dsum;
     }
   }
 }
+
 
 }  // namespace dnsbox

@@ -20,10 +20,7 @@ template <typename T, int N> struct Launcher {
   static cudaError_t xline_nl(const XlineNLArgs<T> &a, cudaStream_t st);
   static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);
   static cudaError_t xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_t st);
-  static cudaError_t zfinish(const FinishArgs<T> &a, int nblocks, int nbatch, cudaStream_t st);
   static int strided_threads();
-  static int zfinish_threads();
-  static int zfinish_cols();
 };
 
 #define DNSBOX_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512) X(1024)
@@ -41,10 +38,6 @@ static cudaError_t set_smem(K kernel, size_t bytes) {
 template <typename T, int N> int Launcher<T, N>::strided_threads() {
   return round32(TileCols<T>::v * (N / FftPlan<N>::E));
 }
-template <typename T, int N> int Launcher<T, N>::zfinish_threads() {
-  return round32(FinishCols<T, N>::v * (N / FftPlan<N>::E));
-}
-template <typename T, int N> int Launcher<T, N>::zfinish_cols() { return FinishCols<T, N>::v; }
 
 template <typename T, int N>
 cudaError_t Launcher<T, N>::strided(const StridedArgs<T> &a, bool inv, int ntiles, cudaStream_t st) {
@@ -155,16 +148,6 @@ cudaError_t Launcher<T, N>::xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_
   return cudaGetLastError();
 }
 
-template <typename T, int N>
-cudaError_t Launcher<T, N>::zfinish(const FinishArgs<T> &a, int nblocks, int nbatch, cudaStream_t st) {
-  using C = typename CT<T>::type;
-  const size_t smem = (size_t)3 * N * FinishCols<T, N>::v * sizeof(C);
-  const int nt = zfinish_threads();
-  cudaError_t e;
-  if ((e = set_smem(k_zfinish<T, N>, smem)) != cudaSuccess) return e;
-  k_zfinish<T, N><<<dim3((unsigned)nblocks, (unsigned)nbatch), nt, smem, st>>>(a);
-  return cudaGetLastError();
-}
 #endif
 
 }  // namespace dnsbox

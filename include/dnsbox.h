@@ -272,9 +272,10 @@ enum dnsbox_pass {
   DNSBOX_PASS_Y_INV = 1,     /* pass B: inverse y FFT, vorticity assembly    */
   DNSBOX_PASS_X_NL = 2,      /* pass C: C2R x, u x omega, CFL max, R2C x     */
   DNSBOX_PASS_Y_FWD = 3,     /* pass D: forward y FFT                        */
-  DNSBOX_PASS_Z_FIN = 4,     /* pass E: forward z FFT + projection + stepper */
+  DNSBOX_PASS_Z_FIN = 4,     /* pass E2: projection, forcing, stepper, E/D   */
   DNSBOX_PASS_SMALL = 5,     /* band energy, CFL, step bookkeeping           */
   DNSBOX_PASS_OTHER = 6,     /* standalone transforms and diagnostics        */
+  DNSBOX_PASS_Z_FWD = 7,     /* pass E1: forward z FFT of the nonlinear term */
   DNSBOX_NPASS = 8
 };
 typedef struct dnsbox_profile {
