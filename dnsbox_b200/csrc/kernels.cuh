@@ -115,6 +115,16 @@ __host__ __device__ __forceinline__ int strided_col(const StridedArgs<T> &a, int
   return (a.nyq_tile < 0 && kx == a.kcol.a) ? (a.kcol.n >> 1) : kx;
 }
 
+// Resident CTAs of a strided launch to ask the register allocator for: FP32
+// blocks of up to 256 threads whose plans hold at most 16 values a thread
+// are held to 64 registers a thread (the load-latency-bound passes gain more
+// from the extra warps than they lose to the tighter allocation); 0 leaves
+// the choice to the compiler.
+template <typename T, int N> struct StridedMinCtas {
+  static constexpr int NT = round32(TileCols<T>::v * (N / FftPlan<N>::E));
+  static constexpr int v = (sizeof(T) == 4 && NT <= 256 && FftPlan<N>::E <= 16) ? 1024 / NT : 0;
+};
+
 // Column origin and other-axis index of tile t of the (possibly pruned) grid.
 template <typename T>
 __device__ __forceinline__ void strided_tile(const StridedArgs<T> &a, int tile, int tcw, int &kx0, int &other) {
@@ -132,7 +142,7 @@ __device__ __forceinline__ C apply_mult(C v, double a, double b, double k) {
 }
 
 template <typename T, int N, bool INV>
-__global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)))
+__global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), StridedMinCtas<T, N>::v)
     k_strided(const __grid_constant__ StridedArgs<T> a) {
   using C = typename CT<T>::type;
   using EN = FftEnds<N>;
