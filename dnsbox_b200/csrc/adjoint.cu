@@ -442,6 +442,20 @@ int sum_to_host(dnsbox_ctx *c, int nblk, double *out) {
   return DNSBOX_OK;
 }
 
+// The sums of two partial arrays of nblk doubles each, red[0, nblk) and
+// red[nblk, 2 nblk), read back with one synchronisation (red must hold
+// 2 nblk + 2 doubles).
+int sum2_to_host(dnsbox_ctx *c, int nblk, double *a, double *b) {
+  k_sum_scalar<256><<<1, 256, 0, c->stream>>>(c->red, nblk, c->red + 2 * nblk);
+  k_sum_scalar<256><<<1, 256, 0, c->stream>>>(c->red + nblk, nblk, c->red + 2 * nblk + 1);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->hstage, c->red + 2 * nblk, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *a = c->hstage[0];
+  *b = c->hstage[1];
+  return DNSBOX_OK;
+}
+
 template <typename T>
 int vjp_impl(dnsbox_ctx *c, const void *uh, const void *g, void *out) {
   using C = typename CT<T>::type;
@@ -542,10 +556,12 @@ int rhs_adj_impl(dnsbox_ctx *c, const void *uh, void *rt, void *rhsadj) {
   return DNSBOX_OK;
 }
 
-// J (and, when grad != null, its Euclidean gradient) at uh.  Uses arena
-// spectral slots 6-8 for N and 9-11 for gE (slots 0-5 belong to the VJP).
+// Forward half of the residual: N(u) and the per-block partials of J into
+// `partials` (kRedBlocks doubles), and, when `weighted` is set, the weighted
+// residual that the gradient half transposes (arena slots 6-11).  No
+// synchronisation.
 template <typename T>
-int residual_impl(dnsbox_ctx *c, const void *uh, void *grad, double *J) {
+int residual_fwd(dnsbox_ctx *c, const void *uh, bool weighted, double *partials) {
   using C = typename CT<T>::type;
   const dnsbox_params &p = c->p;
   const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
@@ -557,19 +573,40 @@ int residual_impl(dnsbox_ctx *c, const void *uh, void *grad, double *J) {
     const int rc = dnsbox_rhs_nonlinear(c, uh, Nb, nullptr);
     if (rc != DNSBOX_OK) return rc;
   }
-  RET(ensure_red(c, kRedBlocks + 1));
   const Grid3 gr = grid3(c);
   k_residual<C><<<kRedBlocks, 256, 0, c->stream>>>(
-      reinterpret_cast<const C *>(uh), reinterpret_cast<const C *>(Nb), grad ? reinterpret_cast<C *>(gE) : nullptr,
-      (long long)c->nh, gr, p.nu, p.Q, p.hminone, s * s, c->red);
+      reinterpret_cast<const C *>(uh), reinterpret_cast<const C *>(Nb), weighted ? reinterpret_cast<C *>(gE) : nullptr,
+      (long long)c->nh, gr, p.nu, p.Q, p.hminone, s * s, partials);
   CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+// Gradient half: grad = (L + N'(u))^T applied to the weighted residual that
+// the last residual_fwd(uh, weighted) left in the arena.
+template <typename T>
+int residual_bwd(dnsbox_ctx *c, const void *uh, void *grad) {
+  using C = typename CT<T>::type;
+  const dnsbox_params &p = c->p;
+  const size_t sb = c->nh * sizeof(C);
+  char *P = nullptr, *S = nullptr;
+  RET(ensure_adj(c, 9, 12, &P, &S));
+  char *gE = S + 9 * sb;
+  const Grid3 gr = grid3(c);
+  RET(vjp_impl<T>(c, uh, gE, grad));
+  k_add_linear<C><<<grid_for((long long)c->nh), 256, 0, c->stream>>>(
+      reinterpret_cast<C *>(grad), reinterpret_cast<const C *>(gE), (long long)c->nh, gr, p.nu, p.Q);
+  CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+// J (and, when grad != null, its Euclidean gradient) at uh.  Uses arena
+// spectral slots 6-8 for N and 9-11 for gE (slots 0-5 belong to the VJP).
+template <typename T>
+int residual_impl(dnsbox_ctx *c, const void *uh, void *grad, double *J) {
+  RET(ensure_red(c, 2 * kRedBlocks + 2));
+  RET(residual_fwd<T>(c, uh, grad != nullptr, c->red));
   RET(sum_to_host(c, kRedBlocks, J));
-  if (grad) {
-    RET(vjp_impl<T>(c, uh, gE, grad));
-    k_add_linear<C><<<grid_for((long long)c->nh), 256, 0, c->stream>>>(
-        reinterpret_cast<C *>(grad), reinterpret_cast<const C *>(gE), (long long)c->nh, gr, p.nu, p.Q);
-    CK(cudaGetLastError());
-  }
+  if (grad) RET(residual_bwd<T>(c, uh, grad));
   return DNSBOX_OK;
 }
 
@@ -586,32 +623,50 @@ int descent_impl(dnsbox_ctx *c, void *uh, int niter, double *Jhist, double *alph
   double J = 0.0;
   RET(residual_impl<T>(c, uh, grad, &J));
   if (Jhist) Jhist[0] = J;
+  // The current state alternates between uh and the trial slot: an accepted
+  // trial's forward half (J and the weighted residual) is kept, so only the
+  // gradient half runs at the new point, and the slope <grad, d> is read back
+  // together with the first trial's J.
+  char *cur = reinterpret_cast<char *>(uh), *nxt = trial;
+  const double s = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz);
+  RET(ensure_red(c, 2 * kRedBlocks + 2));
   for (int it = 0; it < niter; ++it) {
-    RET(ensure_red(c, kRedBlocks + 1));
-    const double s = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz);
     k_descent_dir<C><<<kRedBlocks, 256, 0, c->stream>>>(reinterpret_cast<const C *>(grad), reinterpret_cast<C *>(dir),
                                                         (long long)c->nh, gr, s * s, c->red);
     CK(cudaGetLastError());
-    double slope;
-    RET(sum_to_host(c, kRedBlocks, &slope));   // <grad, d> < 0
-    if (!(slope < 0.0)) break;                    // stationary (or non-finite)
     // Armijo backtracking in FP64: J(u + a d) <= J + 1e-4 a <grad, d>
-    double Jt = 0.0;
+    double slope = 0.0, Jt = 0.0;
     int tries = 0;
+    bool stationary = false;
     for (;;) {
-      k_axpy<C><<<grid_for(n3), 256, 0, c->stream>>>(reinterpret_cast<const C *>(uh), reinterpret_cast<const C *>(dir),
-                                                     reinterpret_cast<C *>(trial), n3, alpha);
+      k_axpy<C><<<grid_for(n3), 256, 0, c->stream>>>(reinterpret_cast<const C *>(cur), reinterpret_cast<const C *>(dir),
+                                                     reinterpret_cast<C *>(nxt), n3, alpha);
       CK(cudaGetLastError());
-      RET(residual_impl<T>(c, trial, nullptr, &Jt));
+      RET(residual_fwd<T>(c, nxt, true, c->red + kRedBlocks));
+      if (tries == 0) {
+        RET(sum2_to_host(c, kRedBlocks, &slope, &Jt));
+        if (!(slope < 0.0)) {   // stationary (or non-finite)
+          stationary = true;
+          break;
+        }
+      } else {
+        k_sum_scalar<256><<<1, 256, 0, c->stream>>>(c->red + kRedBlocks, kRedBlocks, c->red + 2 * kRedBlocks + 1);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->hstage, c->red + 2 * kRedBlocks + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        Jt = c->hstage[0];
+      }
       if ((isfinite(Jt) && Jt <= J + 1e-4 * alpha * slope) || ++tries >= 30) break;
       alpha *= 0.5;
     }
-    if (!(isfinite(Jt) && Jt <= J)) break;
-    CK(cudaMemcpyAsync(uh, trial, 3 * sb, cudaMemcpyDeviceToDevice, c->stream));
-    RET(residual_impl<T>(c, uh, grad, &J));
+    if (stationary || !(isfinite(Jt) && Jt <= J)) break;
+    RET(residual_bwd<T>(c, nxt, grad));
+    std::swap(cur, nxt);   // the accepted trial becomes the state; the old state's buffer the next trial
+    J = Jt;
     if (Jhist) Jhist[it + 1] = J;
     if (tries == 0) alpha *= 2.0;
   }
+  if (cur != reinterpret_cast<char *>(uh)) CK(cudaMemcpyAsync(uh, cur, 3 * sb, cudaMemcpyDeviceToDevice, c->stream));
   if (alpha_io) *alpha_io = alpha;
   return DNSBOX_OK;
 }
