@@ -28,6 +28,8 @@
 //
 // W is the half-spectrum multiplicity (1 on the kx = 0 and Nyquist planes, 2
 // elsewhere); L = Q - nu |k|^2 (the reference's nu (k.k) + Q with imaginary k).
+#include <memory>
+
 #include "internal.cuh"
 
 namespace {
@@ -442,20 +444,6 @@ int sum_to_host(dnsbox_ctx *c, int nblk, double *out) {
   return DNSBOX_OK;
 }
 
-// The sums of two partial arrays of nblk doubles each, red[0, nblk) and
-// red[nblk, 2 nblk), read back with one synchronisation (red must hold
-// 2 nblk + 2 doubles).
-int sum2_to_host(dnsbox_ctx *c, int nblk, double *a, double *b) {
-  k_sum_scalar<256><<<1, 256, 0, c->stream>>>(c->red, nblk, c->red + 2 * nblk);
-  k_sum_scalar<256><<<1, 256, 0, c->stream>>>(c->red + nblk, nblk, c->red + 2 * nblk + 1);
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c->hstage, c->red + 2 * nblk, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  *a = c->hstage[0];
-  *b = c->hstage[1];
-  return DNSBOX_OK;
-}
-
 template <typename T>
 int vjp_impl(dnsbox_ctx *c, const void *uh, const void *g, void *out) {
   using C = typename CT<T>::type;
@@ -569,10 +557,7 @@ int residual_fwd(dnsbox_ctx *c, const void *uh, bool weighted, double *partials)
   char *P = nullptr, *S = nullptr;
   RET(ensure_adj(c, 9, 12, &P, &S));
   char *Nb = S + 6 * sb, *gE = S + 9 * sb;
-  {
-    const int rc = dnsbox_rhs_nonlinear(c, uh, Nb, nullptr);
-    if (rc != DNSBOX_OK) return rc;
-  }
+  RET(rhs_nonlinear_impl(c, uh, Nb));
   const Grid3 gr = grid3(c);
   k_residual<C><<<kRedBlocks, 256, 0, c->stream>>>(
       reinterpret_cast<const C *>(uh), reinterpret_cast<const C *>(Nb), weighted ? reinterpret_cast<C *>(gE) : nullptr,
@@ -610,6 +595,87 @@ int residual_impl(dnsbox_ctx *c, const void *uh, void *grad, double *J) {
   return DNSBOX_OK;
 }
 
+// y = x + alpha d with alpha read from device memory (the launch is part of a
+// captured graph whose step length changes between launches)
+template <typename C>
+__global__ void k_axpy_dev(const C *x, const C *d, C *y, long long n, const double *alpha_p) {
+  using T = decltype(C{}.x);
+  const double alpha = *alpha_p;
+  GRID_LOOP(i, n) {
+    const C a = x[i], b = d[i];
+    y[i] = mkc<C>(T(a.x + alpha * b.x), T(a.y + alpha * b.y));
+  }
+}
+
+}  // namespace
+
+// The adjoint descent's fixed launch sequences as CUDA graphs, on a private
+// stream: the descent direction with the slope sum; per buffer parity p (state
+// in buffer p, trial in buffer 1 - p) the trial (axpy with the device step
+// length, forward residual, J sum, read-back of slope and J into pinned host
+// memory) and the gradient half at the trial.  Valid while the state pointer
+// and the scratch buffers they were captured with are unchanged.
+struct DescentGraphs {
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev = nullptr;
+  cudaGraphExec_t dir = nullptr, tryg[2] = {nullptr, nullptr}, bwd[2] = {nullptr, nullptr};
+  const void *uh = nullptr;
+  const char *adj = nullptr;
+  const double *red = nullptr;
+  int fp64 = -1;
+};
+
+static void graphs_destroy(DescentGraphs *g) {
+  if (!g) return;
+  if (g->dir) cudaGraphExecDestroy(g->dir);
+  for (int i = 0; i < 2; ++i) {
+    if (g->tryg[i]) cudaGraphExecDestroy(g->tryg[i]);
+    if (g->bwd[i]) cudaGraphExecDestroy(g->bwd[i]);
+  }
+  if (g->ev) cudaEventDestroy(g->ev);
+  if (g->s) cudaStreamDestroy(g->s);
+  delete g;
+}
+
+void descent_graphs_free(dnsbox_ctx *c) {
+  graphs_destroy(c->descent);
+  c->descent = nullptr;
+}
+
+namespace {
+
+// Captures the launches f() makes on the context's stream (redirected to s)
+// into an executable graph.  Pass-event profiling is off during the capture.
+template <typename F>
+static int capture_graph(dnsbox_ctx *c, cudaStream_t s, F &&f, cudaGraphExec_t *out) {
+  cudaStream_t saved = c->stream;
+  const int prof = c->prof_on;
+  c->stream = s;
+  c->prof_on = 0;
+  const cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  const int rc = e == cudaSuccess ? f() : DNSBOX_OK;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(s, &graph) : e;
+  c->stream = saved;
+  c->prof_on = prof;
+  if (e != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(e));
+  if (rc != DNSBOX_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e2 != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e2));
+  const cudaError_t e3 = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e3 != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e3));
+  return DNSBOX_OK;
+}
+
+// Steepest descent on J with an FP64 Armijo line search.  The state alternates
+// between uh and the trial slot: an accepted trial's forward half (J and the
+// weighted residual) is kept, so only the gradient half runs at the new
+// point, and the slope <grad, d> is read back together with the first trial's
+// J (one synchronisation per trial).  After the first residual (which grows
+// every scratch buffer) the iterations run as graph launches.
 template <typename T>
 int descent_impl(dnsbox_ctx *c, void *uh, int niter, double *Jhist, double *alpha_io) {
   using C = typename CT<T>::type;
@@ -621,52 +687,90 @@ int descent_impl(dnsbox_ctx *c, void *uh, int niter, double *Jhist, double *alph
   const long long n3 = 3 * (long long)c->nh;
   double alpha = (alpha_io && *alpha_io > 0) ? *alpha_io : 1.0;
   double J = 0.0;
+  RET(ensure_red(c, 2 * kRedBlocks + 4));
   RET(residual_impl<T>(c, uh, grad, &J));
   if (Jhist) Jhist[0] = J;
-  // The current state alternates between uh and the trial slot: an accepted
-  // trial's forward half (J and the weighted residual) is kept, so only the
-  // gradient half runs at the new point, and the slope <grad, d> is read back
-  // together with the first trial's J.
-  char *cur = reinterpret_cast<char *>(uh), *nxt = trial;
-  const double s = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz);
-  RET(ensure_red(c, 2 * kRedBlocks + 2));
+  if (niter <= 0) {
+    if (alpha_io) *alpha_io = alpha;
+    return DNSBOX_OK;
+  }
+  double *red = c->red, *d_alpha = c->red + 2 * kRedBlocks + 2;
+  double *h_alpha = c->hstage + 40, *h_res = c->hstage + 41;   // pinned: step length out, (slope, J) in
+  const double s = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz), s2 = s * s;
+  char *buf[2] = {reinterpret_cast<char *>(uh), trial};
+  DescentGraphs *g = c->descent;
+  if (g && (g->uh != uh || g->adj != c->adj || g->red != c->red || g->fp64 != c->fp64)) {
+    descent_graphs_free(c);
+    g = nullptr;
+  }
+  if (!g) {
+    // built aside and kept only when every capture succeeded
+    std::unique_ptr<DescentGraphs, void (*)(DescentGraphs *)> ng(new DescentGraphs(), graphs_destroy);
+    g = ng.get();
+    g->uh = uh;
+    g->adj = c->adj;
+    g->red = c->red;
+    g->fp64 = c->fp64;
+    CK(cudaStreamCreateWithFlags(&g->s, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming));
+    RET(capture_graph(c, g->s, [&]() -> int {
+      k_descent_dir<C><<<kRedBlocks, 256, 0, c->stream>>>(reinterpret_cast<const C *>(grad), reinterpret_cast<C *>(dir),
+                                                          (long long)c->nh, gr, s2, red);
+      k_sum_scalar<256><<<1, 256, 0, c->stream>>>(red, kRedBlocks, red + 2 * kRedBlocks);
+      CK(cudaGetLastError());
+      return DNSBOX_OK;
+    }, &g->dir));
+    for (int p = 0; p < 2; ++p) {
+      char *cur = buf[p], *nxt = buf[1 - p];
+      RET(capture_graph(c, g->s, [&]() -> int {
+        k_axpy_dev<C><<<grid_for(n3), 256, 0, c->stream>>>(reinterpret_cast<const C *>(cur),
+                                                           reinterpret_cast<const C *>(dir), reinterpret_cast<C *>(nxt),
+                                                           n3, d_alpha);
+        CK(cudaGetLastError());
+        RET(residual_fwd<T>(c, nxt, true, red + kRedBlocks));
+        k_sum_scalar<256><<<1, 256, 0, c->stream>>>(red + kRedBlocks, kRedBlocks, red + 2 * kRedBlocks + 1);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h_res, red + 2 * kRedBlocks, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        return DNSBOX_OK;
+      }, &g->tryg[p]));
+      RET(capture_graph(c, g->s, [&]() -> int { return residual_bwd<T>(c, nxt, grad); }, &g->bwd[p]));
+    }
+    c->descent = ng.release();
+  }
+  // the graphs run on g->s after the work queued so far on the context's stream
+  CK(cudaEventRecord(g->ev, c->stream));
+  CK(cudaStreamWaitEvent(g->s, g->ev, 0));
+  int p = 0;   // the state is in buf[p]
   for (int it = 0; it < niter; ++it) {
-    k_descent_dir<C><<<kRedBlocks, 256, 0, c->stream>>>(reinterpret_cast<const C *>(grad), reinterpret_cast<C *>(dir),
-                                                        (long long)c->nh, gr, s * s, c->red);
-    CK(cudaGetLastError());
+    CK(cudaGraphLaunch(g->dir, g->s));
     // Armijo backtracking in FP64: J(u + a d) <= J + 1e-4 a <grad, d>
     double slope = 0.0, Jt = 0.0;
     int tries = 0;
     bool stationary = false;
     for (;;) {
-      k_axpy<C><<<grid_for(n3), 256, 0, c->stream>>>(reinterpret_cast<const C *>(cur), reinterpret_cast<const C *>(dir),
-                                                     reinterpret_cast<C *>(nxt), n3, alpha);
-      CK(cudaGetLastError());
-      RET(residual_fwd<T>(c, nxt, true, c->red + kRedBlocks));
-      if (tries == 0) {
-        RET(sum2_to_host(c, kRedBlocks, &slope, &Jt));
-        if (!(slope < 0.0)) {   // stationary (or non-finite)
-          stationary = true;
-          break;
-        }
-      } else {
-        k_sum_scalar<256><<<1, 256, 0, c->stream>>>(c->red + kRedBlocks, kRedBlocks, c->red + 2 * kRedBlocks + 1);
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(c->hstage, c->red + 2 * kRedBlocks + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        Jt = c->hstage[0];
+      *h_alpha = alpha;   // the previous copy of this slot has completed (synchronised below)
+      CK(cudaMemcpyAsync(d_alpha, h_alpha, sizeof(double), cudaMemcpyHostToDevice, g->s));
+      CK(cudaGraphLaunch(g->tryg[p], g->s));
+      CK(cudaStreamSynchronize(g->s));
+      slope = h_res[0];
+      Jt = h_res[1];
+      if (!(slope < 0.0)) {   // stationary (or non-finite)
+        stationary = true;
+        break;
       }
       if ((isfinite(Jt) && Jt <= J + 1e-4 * alpha * slope) || ++tries >= 30) break;
       alpha *= 0.5;
     }
     if (stationary || !(isfinite(Jt) && Jt <= J)) break;
-    RET(residual_bwd<T>(c, nxt, grad));
-    std::swap(cur, nxt);   // the accepted trial becomes the state; the old state's buffer the next trial
+    CK(cudaGraphLaunch(g->bwd[p], g->s));
+    p ^= 1;   // the accepted trial becomes the state; the old state's buffer the next trial
     J = Jt;
     if (Jhist) Jhist[it + 1] = J;
     if (tries == 0) alpha *= 2.0;
   }
-  if (cur != reinterpret_cast<char *>(uh)) CK(cudaMemcpyAsync(uh, cur, 3 * sb, cudaMemcpyDeviceToDevice, c->stream));
+  if (p) CK(cudaMemcpyAsync(uh, buf[1], 3 * sb, cudaMemcpyDeviceToDevice, g->s));
+  CK(cudaEventRecord(g->ev, g->s));
+  CK(cudaStreamWaitEvent(c->stream, g->ev, 0));
   if (alpha_io) *alpha_io = alpha;
   return DNSBOX_OK;
 }

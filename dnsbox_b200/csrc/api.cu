@@ -708,6 +708,7 @@ static void free_ctx(dnsbox_ctx *c) {
   cudaFree(c->red);
   cudaFree(c->band);
   cudaFree(c->ddiag);
+  descent_graphs_free(c);
   cudaFree(c->adj);
   cudaFree(c->orbit);
   cudaFree(c->d_nu);
@@ -933,6 +934,13 @@ extern "C" int dnsbox_reset_history(dnsbox_ctx *ctx) {
   ctx->ab2_started = 0;
   ctx->cfl_first = 1;
   return DNSBOX_OK;
+}
+
+// Internal: N(u) into out on the context's stream, with no device selection
+// or host synchronisation (usable inside stream capture).
+int rhs_nonlinear_impl(dnsbox_ctx *ctx, const void *uh, void *out) {
+  return ctx->fp64 ? run_rhs<double>(ctx, uh, FIN_RHS, out, nullptr, nullptr, false, 0, nullptr)
+                   : run_rhs<float>(ctx, uh, FIN_RHS, out, nullptr, nullptr, false, 0, nullptr);
 }
 
 extern "C" int dnsbox_rhs_nonlinear(dnsbox_ctx *ctx, const void *uh, void *out, double *eband) {

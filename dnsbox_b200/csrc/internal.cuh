@@ -35,9 +35,15 @@ int set_err(int code, const char *fmt, ...);
   } while (0)
 
 struct dnsbox_ctx;
+struct DescentGraphs;
 // Advances nsteps with the fused step; with `decide`, first chooses pruned or
 // full passes for this state (api.cu).  No diagnostics are read back.
 int step_advance_decided(dnsbox_ctx *c, void *uh, int nsteps, bool decide);
+// N(u) into out on the context's stream, without device selection or host
+// synchronisation (api.cu).
+int rhs_nonlinear_impl(dnsbox_ctx *ctx, const void *uh, void *out);
+// Releases the adjoint descent's captured graphs and stream (adjoint.cu).
+void descent_graphs_free(dnsbox_ctx *c);
 
 // ------------------------------------------------------------------ context
 struct dnsbox_ctx {
@@ -81,6 +87,7 @@ struct dnsbox_ctx {
   size_t adj_bytes = 0;
   char *orbit = nullptr;                 // checkpoints and segment states of the step-transpose chain
   size_t orbit_bytes = 0;
+  DescentGraphs *descent = nullptr;      // adjoint descent: captured launch sequences (adjoint.cu)
   // measurement
   int prof_on = 0;
   std::vector<cudaEvent_t> ev_pool;      // pairs
