@@ -457,8 +457,9 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
     for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
   }
   __syncwarp();
-  // (omega x u) * s, written back as (px_a,py_a) (pz_a,pz_b) (px_b,py_b) in columns 0..2
-  double m0 = 0, m1 = 0, m2 = 0;
+  // (omega x u) * s, written back as (px_a,py_a) (pz_a,pz_b) (px_b,py_b) in
+  // columns 0..2; the CFL maxima are taken in T (exact) and widened at the end
+  T m0 = 0, m1 = 0, m2 = 0;
 #pragma unroll 4
   for (int n = lane; n < N; n += 32) {
     const C c0 = s[AD::at(n, 0, LDC)], c1 = s[AD::at(n, 1, LDC)], c2 = s[AD::at(n, 2, LDC)];
@@ -471,18 +472,23 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
       px[h] = (oy[h] * ww[h] - oz[h] * vv[h]) * sc;
       py[h] = (oz[h] * uu[h] - ox[h] * ww[h]) * sc;
       pz[h] = (ox[h] * vv[h] - oy[h] * uu[h]) * sc;
-      m0 = fmax(m0, fabs((double)uu[h]));
-      m1 = fmax(m1, fabs((double)vv[h]));
-      m2 = fmax(m2, fabs((double)ww[h]));
+      m0 = fmax(m0, fabs(uu[h]));
+      m1 = fmax(m1, fabs(vv[h]));
+      m2 = fmax(m2, fabs(ww[h]));
     }
     s[AD::at(n, 0, LDC)] = mkc<C>(px[0], py[0]);
     s[AD::at(n, 1, LDC)] = mkc<C>(pz[0], pz[1]);
     s[AD::at(n, 2, LDC)] = mkc<C>(px[1], py[1]);
   }
   __syncwarp();
-  // forward transforms of the three product sequences (SPW at a time)
+  // forward transforms of the three product sequences, SPW at a time.  In
+  // FP32 with two per warp, sequence 2 runs on all 32 lanes with the 32-thread
+  // plan (same column, skew and twiddle table) instead of on one half-warp
+  // (in FP64 that form measured slower)
+  constexpr bool FULL3 = SPW == 2 && sizeof(T) == 4;
+  constexpr int RF = FULL3 ? 1 : (3 + SPW - 1) / SPW;
 #pragma unroll 1
-  for (int r = 0; r < (3 + SPW - 1) / SPW; ++r) {
+  for (int r = 0; r < RF; ++r) {
     const int q = SPW * r + h;
     const bool act = q < 3;
     const int qc = act ? q : 0;
@@ -497,6 +503,18 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
 #pragma unroll
       for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), qc, LDC)] = v[i];
     }
+  }
+  if constexpr (FULL3) {
+    using WP = WarpPlan<N>;
+    using EW = FftEndsP<WP>;
+    static_assert(N + (N - 1) / PL::R[0] < LDC, "the 32-thread plan stays inside its column");
+    C w[WP::E];
+#pragma unroll
+    for (int i = 0; i < WP::E; ++i) w[i] = s[AD::at(EW::in_row(lane, i), 2, LDC)];
+    __syncwarp();
+    fft_regs_p<C, WP, false, true, AD>(w, s, LDC, 2, lane, true, a.tw);
+#pragma unroll
+    for (int i = 0; i < WP::E; ++i) s[AD::at(EW::out_row(lane, i), 2, LDC)] = w[i];
   }
   __syncwarp();
   // unpack two real transforms per sequence and store
@@ -525,9 +543,9 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
   m2 = warp_max(m2);
   if (lane == 0 && a.st) {
     double *um = a.st[la / a.lines_per_box].umax;
-    atomic_max_nonneg(um + 0, m0 * a.s);
-    atomic_max_nonneg(um + 1, m1 * a.s);
-    atomic_max_nonneg(um + 2, m2 * a.s);
+    atomic_max_nonneg(um + 0, (double)m0 * a.s);
+    atomic_max_nonneg(um + 1, (double)m1 * a.s);
+    atomic_max_nonneg(um + 2, (double)m2 * a.s);
   }
 }
 
