@@ -117,3 +117,31 @@ def test_config2_96_boxes_300_steps_against_fp64():
     ens.close()
     print("config 2, 96 boxes x 300 steps, FP32 ensemble vs FP64 singles:", worst)
     assert worst["vel"] < 1e-5 and worst["ekin"] < 1e-5 and worst["diss"] < 1e-5
+
+
+def test_sharded_config2_equals_unsharded():
+    """The config-2 ensemble split as over two ranks (each share run here in
+    turn on one GPU, in its own captured graph) advances every box exactly as
+    the whole 96-box ensemble does, bit for bit: sharding changes which boxes
+    share a launch, not the per-box arithmetic."""
+    from dnsbox_b200.ensemble import Ensemble, config2_local
+    ns = 3
+    whole = config2_local(0, 1)
+    ens = Ensemble([bu for _, _, bu in whole])
+    ens.run(ns)
+    torch.cuda.synchronize()
+    ref = {gi: u[:, j].cpu() for _, idx, (_, u) in whole for j, gi in enumerate(idx)}
+    ens.close()
+    seen = set()
+    for rank in range(2):
+        part = config2_local(rank, 2)
+        e = Ensemble([bu for _, _, bu in part])
+        e.run(ns)
+        torch.cuda.synchronize()
+        for _, idx, (box, u) in part:
+            for j, gi in enumerate(idx):
+                got = (u[:, j] if box.nbatch > 1 else u).cpu()
+                assert torch.equal(got, ref[gi])
+                seen.add(gi)
+        e.close()
+    assert seen == set(range(96))
