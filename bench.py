@@ -304,7 +304,7 @@ def orbit_rate():
     box.set_forcing(f)
     u = box.from_numpy(ic.random_field(n, seed=0, k0=4.0))
     box.step(u, ns, diag=False)
-    box.orbit_residual(u, 20, every=32)   # warm-up (allocates the checkpoint arena)
+    box.orbit_residual(u, ns, every=32)   # warm-up of the same length: grows the checkpoint arena, loads the kernels
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     J, _ = box.orbit_residual(u, ns, every=32)
