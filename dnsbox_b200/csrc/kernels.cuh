@@ -232,9 +232,16 @@ __device__ __forceinline__ C pack_pair(int n, C X1, C X2) {
   return mkc<C>(X1.x + X2.y, X2.x - X1.y);   // conj(X1) + i conj(X2) at N - n
 }
 
+// Resident CTAs of the block x-line kernel to ask the register allocator
+// for: 3 for blocks of up to 256 threads; 2 for the 384-thread FP32 blocks of
+// N = 1024 (80 registers instead of 123, two CTAs per SM instead of one).
+template <typename T, int N> struct XlineMinCtas {
+  static constexpr int NT = round32(3 * XlineB<T, N>::v * (N / FftPlan<N>::E));
+  static constexpr int v = (sizeof(T) == 4 && N >= 1024) ? 2 : min_ctas(NT, 3);
+};
+
 template <typename T, int N>
-__global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::E)),
-                                  min_ctas(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::E)), 3))
+__global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::E)), XlineMinCtas<T, N>::v)
     k_xline_nl(const __grid_constant__ XlineNLArgs<T> a) {
   using C = typename CT<T>::type;
   using EN = FftEnds<N>;
