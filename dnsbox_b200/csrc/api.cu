@@ -413,7 +413,8 @@ template <typename T> static FinishArgs<T> finish_base(const dnsbox_ctx *c) {
   return f;
 }
 
-// One right-hand side: passes A-E.  cfl: 0 none, 1 record (+control).
+// One right-hand side: passes A-D, E1 (forward z) and E2 (spectral finish).
+// cfl: 0 none, 1 record (+control).
 template <typename T>
 static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *state, void *nold,
                    bool partials, int cfl, dnsbox_diag *drec, bool pruned = false) {
