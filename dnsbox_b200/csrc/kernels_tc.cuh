@@ -215,11 +215,21 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
 #pragma unroll
     for (int i = 0; i < 8; ++i) inmask |= (a.krin.keep(N2 * (8 * q + i) + n2) ? 1u : 0u) << (8 * h + i);
   }
+  // With half as many stage-2 items as threads (N2 = 16), a lane pair shares
+  // item t / 2: lane parity s takes the inputs m2 = 2 r + s and the outputs
+  // k2 = 8 s + k (bit k of outmask).
+  constexpr bool PAIR = 2 * 64 * TCW == NT;
+  if constexpr (PAIR) {
+    const int k1 = (t >> 1) / TCW, sp = t & 1;
 #pragma unroll
-  for (int r = 0; r < R2; ++r) {
-    const int k1 = (t + NT * r) / TCW;
+    for (int k = 0; k < 8; ++k) outmask |= (a.krout.keep(k1 + 64 * (8 * sp + k)) ? 1u : 0u) << k;
+  } else {
 #pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) outmask |= (a.krout.keep(k1 + 64 * k2) ? 1u : 0u) << (N2 * r + k2);
+    for (int r = 0; r < R2; ++r) {
+      const int k1 = (t + NT * r) / TCW;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) outmask |= (a.krout.keep(k1 + 64 * k2) ? 1u : 0u) << (N2 * r + k2);
+    }
   }
   auto fetch = [&](unsigned w) {
     nxt = tc_item<TCW>(a, g, w);
@@ -378,7 +388,54 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
     }
     tc::fence_before_sync();
     __syncthreads();
-    // 5. unscale, twiddle, N2-point DFT, store; item (k1, c), c fastest
+    // 5. unscale, twiddle, N2-point DFT, store; item (k1, c), c fastest.
+    //    Paired form (N2 = 16), decimation in time: lane s forms the 8-point
+    //    DFT of the inputs m2 = 2 r + s, the odd lane multiplies by W16^k, the
+    //    pair exchanges them, and X[k] = E[k] + W O[k] (even lane),
+    //    X[k + 8] = E[k] - W O[k] (odd lane).
+    if constexpr (PAIR) {
+      const int item = t >> 1, sp = t & 1;
+      const int cc = item % TCW, k1 = item / TCW;
+      const int sw = tc_swz<LG_R>(k1), swi = sw ^ XIM;
+      C z[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int m2 = 2 * r + sp;
+        const int jj = m2 * TCW + cc;
+        const float us = usc[jj];
+        C yy = mkc<C>(sD[k1 * 64 + (jj ^ sw)] * us, sD[(64 + k1) * 64 + (jj ^ swi)] * us);
+        if (m2) {
+          const C tw = tws[(m2 - 1) * 64 + k1];
+          yy = INV ? cmulc(yy, tw) : cmul(yy, tw);
+        }
+        z[r] = yy;
+      }
+      dft<8, C, INV>(z);
+      // exp(-2 pi i k / 16), k < 8
+      constexpr float kc[8] = {1.f, 0.92387953251128676f, 0.70710678118654752f, 0.38268343236508977f,
+                               0.f, -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128676f};
+      constexpr float ks[8] = {0.f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128676f,
+                               1.f, 0.92387953251128676f, 0.70710678118654752f, 0.38268343236508977f};
+      if (sp) {
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+          const C w = mkc<C>(kc[k], -ks[k]);
+          z[k] = INV ? cmulc(z[k], w) : cmul(z[k], w);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const C o = mkc<C>(__shfl_xor_sync(0xffffffffu, z[k].x, 1), __shfl_xor_sync(0xffffffffu, z[k].y, 1));
+        z[k] = sp ? csub(o, z[k]) : cadd(z[k], o);
+      }
+      const int dc = strided_col(a, it.kx0 + cc) - it.kx0;
+      if (it.kx0 + dc < a.ncols && a.kcol.keep(it.kx0 + dc)) {
+        C *out = J.out + (it.base0 + dc);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if ((outmask >> k) & 1u) out[(k1 + 64 * (8 * sp + k)) * rs] = z[k];
+      }
+    } else
 #pragma unroll
     for (int r = 0; r < R2; ++r) {
       const int idx = t + NT * r;
