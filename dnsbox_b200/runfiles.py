@@ -65,6 +65,11 @@ def fortran_i(n: int, w: int) -> str:
     return s if len(s) <= w else "*" * w
 
 
+def _single(box):
+    if getattr(box, "nbatch", 1) > 1:
+        raise ValueError("run files describe one box; take the box out of the batch first")
+
+
 # ------------------------------------------------------------------ info.dat
 def write_info(path, box, *, courant=None, isave1=1000, isave2=10, initrand=True, mode="a"):
     """Append the run parameters of ``box`` to ``path`` in the layout of
@@ -113,6 +118,7 @@ def stats_row(box, uh, t, dt):
     """The eight Ekin.dat quantities at state ``uh`` and time t (io.f90:628-661):
     time, Ekin, dissipation, input 2 Q Ekin, Courant number at step dt,
     maximum divergence, EZero (state_spectrum), Eband (rhs_Eband)."""
+    _single(box)
     ekin = box.kinetic(uh)
     disp = box.dissipation(uh)
     courant, _ = box.courant(uh, dt)
@@ -145,6 +151,7 @@ def write_spectrum(path, kspec, espec):
 
 def save_spectrum(box, uh, count, directory="."):
     """state_spectrum of ``uh`` to specNNNN.dat (NNNN = count, I4.4)."""
+    _single(box)
     es, _, _, _ = box.spectrum(uh)
     kspec = (np.arange(1, len(es) + 1) * box.params.Deltak).tolist()
     path = os.path.join(directory, f"spec{count:04d}.dat")
@@ -157,6 +164,7 @@ def save_state(box, uh, count, directory=".", time=0.0, step=0):
     """Physical u, v, w (FP64) of the spectral state ``uh`` to stateNNNN.bin
     plus the layout descriptor stateNNNN.json; returns the .bin path."""
     import torch
+    _single(box)
     s = 1.0 / (box.nx * box.ny * box.nz)
     base = os.path.join(directory, f"state{count:04d}")
     with open(base + ".bin", "wb") as f:
@@ -189,6 +197,7 @@ def load_state(box, path):
     """A state file to the spectral state of ``box``: R2C of the physical
     fields, then dealias and projection (dnsboxheun.f90:48-55)."""
     import torch
+    _single(box)
     phys, desc = read_state_file(path)
     if (desc["nx"], desc["ny"], desc["nz"]) != (box.nx, box.ny, box.nz):
         raise ValueError(f"state is {desc['nx']}x{desc['ny']}x{desc['nz']}, the box "

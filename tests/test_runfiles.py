@@ -103,3 +103,11 @@ def test_state_file_reader(tmp_path):
     u[:, :2].astype("<f8").tofile(str(base) + ".bin")
     with pytest.raises(ValueError):
         R.read_state_file(str(base) + ".bin")
+
+
+def test_batched_box_is_refused():
+    box = types.SimpleNamespace(nbatch=4, nx=8, ny=8, nz=8, params=_fake_box(True).params)
+    for fn in (lambda: R.stats_row(box, None, 0.0, 1e-3), lambda: R.save_spectrum(box, None, 1),
+               lambda: R.save_state(box, None, 1), lambda: R.load_state(box, "x.bin")):
+        with pytest.raises(ValueError):
+            fn()
