@@ -315,15 +315,6 @@ __global__ void k_descent_dir(const C *grad, C *d, long long nh, Grid3 gr, doubl
   if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
 }
 
-template <typename C>
-__global__ void k_axpy(const C *x, const C *d, C *y, long long n, double alpha) {
-  using T = decltype(C{}.x);
-  GRID_LOOP(i, n) {
-    const C a = x[i], b = d[i];
-    y[i] = mkc<C>(T(a.x + alpha * b.x), T(a.y + alpha * b.y));
-  }
-}
-
 // out = IF (u + dt n), IF = exp((Q - nu |k|^2) dt): the FIN_PRED arithmetic of k_finish_rows
 template <typename C>
 __global__ void k_if_pred(const C *u, const C *n, C *out, long long nh, Grid3 gr, double nu, double Q, double dt) {
