@@ -49,10 +49,10 @@ def test_pruned_heun_cfl_bit_identical(prec, shape):
                                                                         b["courant"])
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "tc_split"])
 @pytest.mark.parametrize("ab2", ["reference", "standard"])
 def test_pruned_ab2_bit_identical(prec, ab2):
-    n = 64
+    n = 128 if prec == "tc_split" else 64   # the tensor-core passes start at 128
     uh = ic.random_field(n, seed=2, k0=4.0)
     (up, rp, pr), (uf, rf, _) = run_pair((n, n, n), prec, 8, uh, nu=0.01, bandlim=False, stepper="ab2", ab2=ab2,
                                          tstep_fix=True, dt=2e-3)
