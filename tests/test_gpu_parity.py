@@ -404,3 +404,40 @@ def test_config1_500_steps_fp64_and_fp32():
     print(f"config 1, 500 steps: budget residual fp64 {r64:.2e} fp32 {r32:.2e}; fp32 vs fp64: D {dd:.2e}, "
           f"E(k) {ek:.2e}, velocity {ev:.2e}")
     assert dd < 1e-3 and ek < 1e-2
+
+
+# ------------------------------------------------------- spherical truncation
+@pytest.mark.parametrize("broadband", [False, True])
+def test_spherical_truncation(broadband):
+    """The spherical option (parameters.f90:48): the right-hand side masks
+    |k| >= (N/2) alpha_x / 2 as rhs.f90:74-88 does, state_dealias masks
+    |k| >= (N/2)(2/3) alpha_x as state.f90:186-199 does, and fixed-dt Heun steps
+    follow the oracle.  A dealiased field steps through the pruned passes, one
+    with broadband content through the full passes.  FP64, 1e-12."""
+    n, dt, ns = 32, 2e-3, 6
+    uh = field(n, seed=21, k0=3.0, nyquist=broadband)
+    p = O.Params(nx=n, ny=n, nz=n, nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True, spherical=True, tstep_fix=True)
+    g = O.Grid(p)
+    b = box(n, nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True, spherical=True, tstep_fix=True, dt=dt)
+    got, _ = b.rhs_nonlinear(b.from_numpy(uh))
+    assert rel(got.cpu().numpy(), O.rhs_nonlinear(g, uh)) < FP64_TOL
+    d = b.from_numpy(uh)
+    b.dealias(d)
+    assert rel(d.cpu().numpy(), O.state_dealias(g, uh)) < FP64_TOL
+    want, _ = O.drive(g, uh, ns, dt)
+    u = b.from_numpy(uh)
+    b.step(u, ns)
+    assert b.step_pruned() == (not broadband)
+    assert rel(u.cpu().numpy(), want) < FP64_TOL
+
+
+def test_spherical_truncation_tc_split():
+    """Spherical truncation with the tensor-core passes (128^3): one
+    right-hand side against the oracle, the FP32 forms' bar 2e-5."""
+    n = 128
+    uh = ic.random_field(n, seed=22, k0=3.0)
+    p = O.Params(nx=n, ny=n, nz=n, nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True, spherical=True)
+    want = O.rhs_nonlinear(O.Grid(p), uh)
+    b = box(n, "tc_split", nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True, spherical=True)
+    got, _ = b.rhs_nonlinear(b.from_numpy(uh))
+    assert rel(got.cpu().numpy(), want) < FP32_TOL
