@@ -118,6 +118,7 @@ SIGNATURES = {
     "dnsbox_ensemble_run": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dnsbox_ensemble_destroy": (ctypes.c_int, [_VP]),
     "dnsbox_profile_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "dnsbox_sync": (ctypes.c_int, [_VP]),
     "dnsbox_profile_read": (ctypes.c_int, [_VP, ctypes.POINTER(Profile), ctypes.c_int]),
 }
 

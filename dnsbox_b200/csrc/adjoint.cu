@@ -430,7 +430,7 @@ int sum_to_host(dnsbox_ctx *c, int nblk, double *out) {
   k_sum_scalar<256><<<1, 256, 0, c->stream>>>(c->red, nblk, c->red + nblk);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->hstage, c->red + nblk, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  RET(tc_check(c));
   *out = c->hstage[0];
   return DNSBOX_OK;
 }
@@ -613,6 +613,7 @@ struct DescentGraphs {
   const void *uh = nullptr;
   const char *adj = nullptr;
   const double *red = nullptr;
+  const void *force = nullptr;   // the fixed forcing the captured finish launches read
   int fp64 = -1;
 };
 
@@ -690,7 +691,7 @@ int descent_impl(dnsbox_ctx *c, void *uh, int niter, double *Jhist, double *alph
   const double s = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz), s2 = s * s;
   char *buf[2] = {reinterpret_cast<char *>(uh), trial};
   DescentGraphs *g = c->descent;
-  if (g && (g->uh != uh || g->adj != c->adj || g->red != c->red || g->fp64 != c->fp64)) {
+  if (g && (g->uh != uh || g->adj != c->adj || g->red != c->red || g->fp64 != c->fp64 || g->force != c->force)) {
     descent_graphs_free(c);
     g = nullptr;
   }
@@ -701,6 +702,7 @@ int descent_impl(dnsbox_ctx *c, void *uh, int niter, double *Jhist, double *alph
     g->uh = uh;
     g->adj = c->adj;
     g->red = c->red;
+    g->force = c->force;
     g->fp64 = c->fp64;
     CK(cudaStreamCreateWithFlags(&g->s, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming));
@@ -763,6 +765,15 @@ int descent_impl(dnsbox_ctx *c, void *uh, int niter, double *Jhist, double *alph
   CK(cudaEventRecord(g->ev, g->s));
   CK(cudaStreamWaitEvent(c->stream, g->ev, 0));
   if (alpha_io) *alpha_io = alpha;
+  RET(tc_check(c));
+  return DNSBOX_OK;
+}
+
+// The adjoint arena and the residual reductions hold one box: batched
+// contexts are refused before anything is launched.
+static int single_box(dnsbox_ctx *c) {
+  if (c->nbatch > 1)
+    return set_err(DNSBOX_ERR_UNSUPPORTED, "not available on a batched context (nbatch = %d)", c->nbatch);
   return DNSBOX_OK;
 }
 
@@ -856,7 +867,7 @@ int steps_vjp_impl(dnsbox_ctx *c, const void *u0, int nsteps, int every, const v
     }
   }
   CK(cudaMemcpyAsync(g0, ga, sb3, cudaMemcpyDeviceToDevice, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  RET(tc_check(c));
   return DNSBOX_OK;
 }
 
@@ -883,7 +894,7 @@ int orbit_impl(dnsbox_ctx *c, const void *u0, int nsteps, int every, void *grad,
     k_accum<C><<<grid_for(3 * nh), 256, 0, c->stream>>>(reinterpret_cast<C *>(grad), reinterpret_cast<const C *>(gc),
                                                          3 * nh, -1.0);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(c->stream));
+    RET(tc_check(c));
   }
   return DNSBOX_OK;
 }
@@ -926,6 +937,7 @@ extern "C" int dnsbox_orbit_residual(dnsbox_ctx *ctx, const void *u0, int nsteps
 
 extern "C" int dnsbox_rhs_nonlinear_vjp(dnsbox_ctx *ctx, const void *uh, const void *g, void *out) {
   if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  RET(single_box(ctx));
   CK(cudaSetDevice(ctx->p.device));
   if (!uh || !g || !out) return set_err(DNSBOX_ERR_ARG, "null pointer");
   if (out == uh || out == g) return set_err(DNSBOX_ERR_ARG, "output may not alias an input");
@@ -934,6 +946,7 @@ extern "C" int dnsbox_rhs_nonlinear_vjp(dnsbox_ctx *ctx, const void *uh, const v
 
 extern "C" int dnsbox_rhs_adj(dnsbox_ctx *ctx, const void *uh, void *rt, void *rhsadj) {
   if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  RET(single_box(ctx));
   CK(cudaSetDevice(ctx->p.device));
   if (!uh || !rt || !rhsadj) return set_err(DNSBOX_ERR_ARG, "null pointer");
   if (rt == uh || rhsadj == uh || rt == rhsadj) return set_err(DNSBOX_ERR_ARG, "outputs may not alias");
@@ -942,6 +955,7 @@ extern "C" int dnsbox_rhs_adj(dnsbox_ctx *ctx, const void *uh, void *rt, void *r
 
 extern "C" int dnsbox_residual(dnsbox_ctx *ctx, const void *uh, double *J) {
   if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  RET(single_box(ctx));
   CK(cudaSetDevice(ctx->p.device));
   if (!uh || !J) return set_err(DNSBOX_ERR_ARG, "null pointer");
   return ctx->fp64 ? residual_impl<double>(ctx, uh, nullptr, J) : residual_impl<float>(ctx, uh, nullptr, J);
@@ -949,6 +963,7 @@ extern "C" int dnsbox_residual(dnsbox_ctx *ctx, const void *uh, double *J) {
 
 extern "C" int dnsbox_residual_grad(dnsbox_ctx *ctx, const void *uh, void *grad, double *J) {
   if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  RET(single_box(ctx));
   CK(cudaSetDevice(ctx->p.device));
   if (!uh || !grad || !J) return set_err(DNSBOX_ERR_ARG, "null pointer");
   if (grad == uh) return set_err(DNSBOX_ERR_ARG, "output may not alias the input");
@@ -957,6 +972,7 @@ extern "C" int dnsbox_residual_grad(dnsbox_ctx *ctx, const void *uh, void *grad,
 
 extern "C" int dnsbox_adjoint_descent(dnsbox_ctx *ctx, void *uh, int niter, double *Jhist, double *alpha) {
   if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  RET(single_box(ctx));
   CK(cudaSetDevice(ctx->p.device));
   if (!uh || niter < 0) return set_err(DNSBOX_ERR_ARG, "invalid argument");
   return ctx->fp64 ? descent_impl<double>(ctx, uh, niter, Jhist, alpha)

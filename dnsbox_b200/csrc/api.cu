@@ -545,8 +545,10 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
 }
 
 // Synchronises the stream and reports a tensor-core pass whose MMA
-// completion wait gave up (the flag is cleared).
-static int tc_check(dnsbox_ctx *c) {
+// completion wait gave up (the flag is cleared).  Every entry point that
+// synchronises before returning ends with it; asynchronous entries leave the
+// flag to the next such call or to dnsbox_sync.
+int tc_check(dnsbox_ctx *c) {
   int *flag = reinterpret_cast<int *>(c->hstage + 63);
   if (c->tc) CK(cudaMemcpyAsync(flag, c->tc_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -953,7 +955,7 @@ extern "C" int dnsbox_rhs_nonlinear(dnsbox_ctx *ctx, const void *uh, void *out, 
   RET(rc);
   if (eband) {
     CK(cudaMemcpyAsync(ctx->hstage, &ctx->st->eband, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    RET(tc_check(ctx));
     *eband = ctx->p.bandlim ? ctx->hstage[0] : 0.0;
   }
   return DNSBOX_OK;
@@ -1034,7 +1036,7 @@ static int specdiag(dnsbox_ctx *ctx, const void *uh, int single, std::vector<dou
   out.resize(nv);
   CK(cudaMemcpyAsync(out.data(), ctx->red + (size_t)nblk * nv, nv * sizeof(double), cudaMemcpyDeviceToHost,
                      ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  RET(tc_check(ctx));
   return DNSBOX_OK;
 }
 
@@ -1126,7 +1128,7 @@ static int reduce_max(dnsbox_ctx *ctx, const void *f, bool fp64, long long n, in
   k_max_partials<<<1, 1024, 0, ctx->stream>>>(ctx->red, nblk, ctx->red + nblk);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(ctx->hstage, ctx->red + nblk, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  RET(tc_check(ctx));
   *host = ctx->hstage[0];
   return DNSBOX_OK;
 }
@@ -1251,7 +1253,7 @@ extern "C" int dnsbox_upload_physical(dnsbox_ctx *ctx, const double *host, void 
   }
   for (int c = 0; c < 3; ++c) out[c] = field(reinterpret_cast<char *>(uh), ctx, c);
   RET(ctx->fp64 ? r2c_fields<double>(ctx, 3, in, out) : r2c_fields<float>(ctx, 3, in, out));
-  CK(cudaStreamSynchronize(ctx->stream));
+  RET(tc_check(ctx));
   return DNSBOX_OK;
 }
 
@@ -1277,10 +1279,15 @@ extern "C" int dnsbox_download_physical(dnsbox_ctx *ctx, const void *uh, double 
                          ctx->stream));
     }
   }
-  CK(cudaStreamSynchronize(ctx->stream));
+  RET(tc_check(ctx));
   return DNSBOX_OK;
 }
 
+
+extern "C" int dnsbox_sync(dnsbox_ctx *ctx) {
+  BEGIN(ctx);
+  return tc_check(ctx);
+}
 
 extern "C" int dnsbox_profile_enable(dnsbox_ctx *ctx, int on) {
   if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");

@@ -44,6 +44,9 @@ int step_advance_decided(dnsbox_ctx *c, void *uh, int nsteps, bool decide);
 int rhs_nonlinear_impl(dnsbox_ctx *ctx, const void *uh, void *out);
 // Releases the adjoint descent's captured graphs and stream (adjoint.cu).
 void descent_graphs_free(dnsbox_ctx *c);
+// Synchronises the context's stream and returns DNSBOX_ERR_TIMEOUT (clearing
+// the flag) if a tensor-core pass gave up waiting for its MMAs (api.cu).
+int tc_check(dnsbox_ctx *c);
 
 // ------------------------------------------------------------------ context
 struct dnsbox_ctx {

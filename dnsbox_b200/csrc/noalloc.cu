@@ -13,8 +13,12 @@
 // Set-up: the first call on a device (with that device current) resolves the
 // arrays' device addresses with cudaGetSymbolAddress and fills the twiddle
 // tables; later calls on that device reuse them.  Make that first call before
-// any stream capture.  Host code never hands the arrays' names to a kernel:
-// in host code they are stand-ins, not device addresses.
+// any stream capture.  Every call resolves the scratch address again (a host
+// lookup, no allocation); when it differs from the one set up -- the module was
+// reloaded after cudaDeviceReset or a primary-context teardown -- the set-up
+// runs again, so the first call after such a reset must also come before any
+// stream capture.  Host code never hands the arrays' names to a kernel: in host
+// code they are stand-ins, not device addresses.
 //
 // Every call shares the scratch array and leaves its contents behind.  Nothing
 // in it has to start at zero: each pass writes every element the next pass
@@ -53,11 +57,17 @@ int tw_offset(int n) {
   return -1;
 }
 
-// Once per device, with the device current: resolve the symbols and fill the
-// twiddle tables exp(-2 pi i j / n).
+// Once per device (and again after the module was reloaded), with the device
+// current: resolve the symbols and fill the twiddle tables exp(-2 pi i j / n).
 int setup_device(int dev, DeviceSetup **out) {
   std::lock_guard<std::mutex> lock(g_mu);
   DeviceSetup &d = g_dev[dev];
+  if (d.done) {
+    unsigned char *now = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&now), g_scratch);
+    if (e != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    if (now != d.scratch) d.done = false;   // a new module instance: its twiddle tables are unfilled
+  }
   if (!d.done) {
     cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&d.scratch), g_scratch);
     if (e != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));

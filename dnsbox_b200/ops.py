@@ -288,6 +288,11 @@ class Box:
                                                     hist.ctypes.data_as(_lib._DP), ctypes.byref(a)))
         return hist, a.value
 
+    def sync(self):
+        """Waits for the work queued on this Box and raises if a device-side
+        wait gave up (a tensor-core pass whose output is then invalid)."""
+        _lib.check(self._lib.dnsbox_sync(self._h))
+
     def step_pruned(self) -> bool:
         """Whether the last step call ran the pruned (2/3-rule) passes."""
         return self._lib.dnsbox_step_pruned(self._h) == 1

@@ -170,8 +170,9 @@ int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec_dev, void *phys_dev);
  * DNSBOX_FP32) bytes must fit in 8 MiB (64^3 FP64, 96^3 FP32), else
  * DNSBOX_ERR_SIZE.  Runs on the current device and the given stream.  The first
  * call on a device sets that device up (resolves the arrays' addresses, fills
- * the twiddle tables): make it before any stream capture.  All calls share the
- * scratch array, so calls that overlap on the GPU race. */
+ * the twiddle tables): make it before any stream capture, and likewise the
+ * first call after a cudaDeviceReset, which repeats the set-up.  All calls
+ * share the scratch array, so calls that overlap on the GPU race. */
 int dnsbox_c2r_noalloc(int nx, int ny, int nz, int precision, const void *spec_dev, void *phys_dev,
                        void *cuda_stream);
 
@@ -196,7 +197,9 @@ int dnsbox_download_physical(dnsbox_ctx *ctx, const void *uhat3_dev, double *u3_
 int dnsbox_rhs_adj(dnsbox_ctx *ctx, const void *uhat3_dev, void *rtilde3_dev,
                    void *rhsadj3_dev);
 /* Fixed spectral forcing f (3 fields, kept by the caller; NULL clears) added to
- * the nonlinear term of rhs_nonlinear and of every step.  No reference
+ * the nonlinear term of rhs_nonlinear and of every step.  An ensemble keeps
+ * the forcing in effect when it was created; the adjoint descent recaptures
+ * its graphs when the forcing changes.  No reference
  * counterpart (the reference forces only through Q and the band term); used for
  * the Kolmogorov flow f = (F sin(4y), 0, 0). */
 int dnsbox_set_forcing(dnsbox_ctx *ctx, const void *f3_dev);
@@ -240,9 +243,9 @@ int dnsbox_heun_steps_vjp(dnsbox_ctx *ctx, const void *u0_3_dev, int nsteps, int
 int dnsbox_orbit_residual(dnsbox_ctx *ctx, const void *u0_3_dev, int nsteps, int every, void *grad3_dev,
                           double *J);
 
-/* ---- batched boxes and ensembles (SURVEY config 2: independent boxes of
- *      mixed N and nu; no reference counterpart -- the reference runs one box
- *      per MPI job).  A context created with nbatch > 1 holds nbatch boxes of
+/* ---- batched boxes and ensembles (independent boxes of mixed N and nu,
+ *      e.g. 96 boxes of 32^3, 64^3 and 96^3; no reference counterpart -- the
+ *      reference runs one box per MPI job).  A context created with nbatch > 1 holds nbatch boxes of
  *      one size; its states are component-major, [3][nbatch][nz][ny][nx/2+1],
  *      and dnsbox_step / dnsbox_rhs_nonlinear advance all boxes in the same
  *      launches (box index on the grid's y dimension), each box with its own
@@ -284,6 +287,14 @@ typedef struct dnsbox_profile {
   int64_t total_launches;           /* all kernel launches since reset       */
 } dnsbox_profile;
 int dnsbox_profile_enable(dnsbox_ctx *ctx, int on);
+/* Waits for the context's stream and reports a device-side failure of the
+ * work queued so far: DNSBOX_ERR_TIMEOUT when a tensor-core pass gave up
+ * waiting for its MMAs (its output is then invalid).  Entry points that return
+ * host values make this check themselves; asynchronous ones (transforms,
+ * rhs_nonlinear without eband, step without diagnostics, VJPs) leave it to the
+ * next such call or to this one.  No reference counterpart (the reference has
+ * no error channel). */
+int dnsbox_sync(dnsbox_ctx *ctx);
 int dnsbox_profile_read(dnsbox_ctx *ctx, dnsbox_profile *out, int reset);
 
 #ifdef __cplusplus

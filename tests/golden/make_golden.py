@@ -141,6 +141,8 @@ def make(path, n, seed, out):
 
 
 if __name__ == "__main__":
-    proto = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/python/dnsbox.py"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path to the reference's python/dnsbox.py>")
+    proto = sys.argv[1]
     make(proto, 16, 7, os.path.join(HERE, "golden_n16.npz"))
     make(proto, 12, 11, os.path.join(HERE, "golden_n12.npz"))

@@ -101,11 +101,12 @@ def _kolmogorov_box(n, precision="fp64", hminone=True):
     return b
 
 
+@pytest.mark.parametrize("n", [32, 64])
 @pytest.mark.parametrize("hminone", [True, False])
-def test_residual_gradient_finite_differences(hminone):
+def test_residual_gradient_finite_differences(n, hminone):
     """dJ along 16 seeded solenoidal directions, eps = 1e-6, FP64: the exact
-    adjoint gradient agrees with central differences to 1e-6."""
-    n = 32
+    adjoint gradient agrees with central differences to 1e-6 (64^3 is the
+    adjoint-descent configuration's grid)."""
     b = _kolmogorov_box(n, hminone=hminone)
     u = b.from_numpy(ic.random_field(n, seed=0, k0=4.0))
     J, grad = b.residual_grad(u)
@@ -215,3 +216,39 @@ def test_residual_gradient_tc_split_128():
     print(f"tc_split residual 128^3: J {abs(Jtc - J64) / J64:.2e}, gradient {eg:.2e}")
     assert abs(Jtc - J64) <= 1e-5 * J64
     assert eg < 2e-5
+
+
+def test_batched_context_refuses_residual_and_adjoint():
+    """The adjoint arena holds one box: every residual and adjoint entry
+    refuses a batched context with DNSBOX_ERR_UNSUPPORTED before launching."""
+    from dnsbox_b200._lib import DnsboxError
+    n = 16
+    b = box(n, nu=0.01, bandlim=False, tstep_fix=True, nbatch=3)
+    u = b.zeros()
+    calls = [lambda: b.residual(u), lambda: b.residual_grad(u), lambda: b.rhs_adj(u),
+             lambda: b.rhs_nonlinear_vjp(u, u), lambda: b.adjoint_descent(u, 1)]
+    for call in calls:
+        with pytest.raises(DnsboxError) as e:
+            call()
+        assert e.value.code == -8 and "batched" in str(e.value)
+    b.close()
+
+
+def test_adjoint_descent_follows_a_forcing_change():
+    """The descent graphs capture the forcing pointer: after set_forcing the
+    next descent on the same state tensor recaptures, and its J history equals
+    that of a fresh context created with the new forcing."""
+    n = 24
+    b = _kolmogorov_box(n)
+    u = b.from_numpy(ic.random_field(n, seed=5, k0=4.0))
+    b.adjoint_descent(u, 2, alpha=1.0)
+    f2 = b.from_numpy(2.0 * ic.kolmogorov_forcing(n, 1.0, 4))
+    b.set_forcing(f2)
+    u_after = u.clone()
+    h, a = b.adjoint_descent(u, 3, alpha=1.0)
+    c = _kolmogorov_box(n)
+    c.set_forcing(c.from_numpy(2.0 * ic.kolmogorov_forcing(n, 1.0, 4)))
+    v = u_after.clone()
+    hc, ac = c.adjoint_descent(v, 3, alpha=1.0)
+    assert np.array_equal(h, hc) and a == ac
+    assert torch.equal(u, v)

@@ -1,4 +1,4 @@
-"""Batched boxes and ensembles (SURVEY config 2) against single-box runs."""
+"""Batched boxes and ensembles (96 boxes of 32^3, 64^3 and 96^3 with their own seeds and viscosities) against single-box runs."""
 import numpy as np
 import pytest
 import torch

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 FP64_TOL = 1e-12
-FP32_TOL = 2e-5
+FP32_TOL = 2e-6   # one FP32 right-hand side measures 3-6e-7 against the FP64 oracle
 
 
 def rel(a, b):
@@ -55,9 +55,9 @@ def test_transforms_match_pocketfft(prec, shape):
     f = rng.standard_normal((nz, ny, nx))
     F = g.r2c(f)
     Fg = b.r2c(torch.from_numpy(f).to(b.device, b.rdtype)).cpu().numpy()
-    assert rel(Fg, F) < (1e-13 if prec == "fp64" else 2e-6)
+    assert rel(Fg, F) < (1e-13 if prec == "fp64" else 8e-7)   # FP32 measures 1-3e-7
     fg = b.c2r(torch.from_numpy(F).to(b.device, b.cdtype)).cpu().numpy()
-    assert rel(fg, g.c2r(F)) < (1e-13 if prec == "fp64" else 2e-6)
+    assert rel(fg, g.c2r(F)) < (1e-13 if prec == "fp64" else 8e-7)
 
 
 @pytest.mark.parametrize("n", [256, 512])
@@ -135,7 +135,7 @@ def test_heun_steps(prec, bandlim):
     b = box(n, prec, nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=bandlim, tstep_fix=True, dt=dt)
     u = b.from_numpy(uh)
     grec = b.step(u, ns)
-    assert rel(u.cpu().numpy(), want) < tol(prec) * (1 if prec == "fp64" else 5)
+    assert rel(u.cpu().numpy(), want) < tol(prec) * (1 if prec == "fp64" else 2)
     for a, r in zip(grec, recs):
         assert abs(a["ekin"] - r["ekin"]) < (1e-12 if prec == "fp64" else 1e-5) * r["ekin"]
         assert abs(a["dissipation"] - r["dissipation"]) < (1e-12 if prec == "fp64" else 1e-5) * r["dissipation"]
@@ -238,10 +238,10 @@ def test_host_layout_round_trips(prec):
     assert rel(back, host) < (1e-15 if prec == "fp64" else 1e-7)
     g = O.Grid(O.Params(nx=n, ny=n, nz=n))
     phys = b.download_physical(u)
-    assert rel(phys, O.state_uhat2u(g, uh)) < (1e-13 if prec == "fp64" else 1e-6)
+    assert rel(phys, O.state_uhat2u(g, uh)) < (1e-13 if prec == "fp64" else 8e-7)
     u2 = b.zeros()
     b.upload_physical(phys, u2)
-    assert rel(u2.cpu().numpy(), uh) < (1e-13 if prec == "fp64" else 1e-6)
+    assert rel(u2.cpu().numpy(), uh) < (1e-13 if prec == "fp64" else 8e-7)
 
 
 # ---------------------------------------------------------------- full size
@@ -342,7 +342,7 @@ def test_rhs_nonlinear_512_properties():
     b32.close()
     b64 = box(n, "fp64", bandlim=False)
     N64, _ = b64.rhs_nonlinear(host.to(b64.device))
-    assert float((N32.to(torch.complex128) - N64).abs().norm() / N64.abs().norm()) < 2e-5
+    assert float((N32.to(torch.complex128) - N64).abs().norm() / N64.abs().norm()) < 2e-6
 
 
 # ---------------------------------------------------------------- 1024-point axes

@@ -43,7 +43,7 @@ def test_tc_transforms_match_pocketfft(shape):
     fg = b.c2r(torch.from_numpy(F).to(b.device, b.cdtype)).cpu().numpy()
     e_c2r = rel(fg, g.c2r(F))
     print(f"tc transforms {shape}: r2c {e_r2c:.3e} c2r {e_c2r:.3e}")
-    assert e_r2c < 1e-6 and e_c2r < 1e-6   # FP32 storage: a few ulp of 2^-24 per pass
+    assert e_r2c < 8e-7 and e_c2r < 8e-7   # measured 2-3e-7: a few ulp of 2^-24 per pass
 
 
 def test_tc_path_is_taken_and_close_to_fp32():
@@ -84,7 +84,7 @@ def test_tc_rhs_nonlinear(n):
     got, ebg = b.rhs_nonlinear(b.from_numpy(uh))
     e = rel(got.cpu().numpy(), want)
     print(f"tc rhs {n}: {e:.3e}")
-    assert e < 2e-5   # same bar as the FP32 form
+    assert e < 2e-6   # same bar as the FP32 form (measured 5e-7)
     assert abs(ebg - eb) < 1e-6 * eb
 
 
@@ -129,8 +129,11 @@ def test_tc_heun_trajectory_128():
         res[prec] = _errors(*_trajectory(prec, n, u0, ns, **kw), u64, r64, e64)
         print(f"{prec} 128^3 {ns} steps: vel {res[prec][0]:.3e} E(k) {res[prec][1]:.3e} "
               f"(tail shells {res[prec][2]:.3e}) D {res[prec][3]:.3e}")
-    ev, ek, _, dd = res["tc_split"]
+    ev, ek, ek_tail, dd = res["tc_split"]
     assert ev < 1e-6 and ek < 1e-5 and dd < 1e-6
+    # tail shells (1e-14 .. 1e-9 of E): bounded, and no worse than the FP32
+    # SIMT form's by more than a small factor
+    assert ek_tail < 1e-3 and ek_tail < 4 * res["fp32"][2] + 1e-6
     # no worse than the FP32 SIMT form by more than a small factor
     assert ev < 4 * res["fp32"][0] + 1e-7
 
@@ -154,7 +157,9 @@ def test_tc_512_accuracy_against_fp64():
     """512^3 forced turbulence (nu = 8e-4, band forcing eps = 0.1, Courant 0.5),
     100 Heun steps from the seeded k0 = 3 field: TC-split against the plain
     FP64 GPU form.  Bars: velocity relative L2 <= 1e-6; E(k) <= 1e-5 on every
-    shell holding at least 1e-9 of the energy (the deeper tail is printed);
+    shell holding at least 1e-9 of the energy and <= 1e-3 on the shells between
+    1e-14 and 1e-9 of it (there the FP32 transforms' error, which is relative to
+    the whole field, dominates: the FP32 SIMT form measures the same);
     dissipation <= 1e-5 on every step."""
     from dnsbox_b200.ic import random_field_gpu
     n, ns = 512, 100
@@ -176,8 +181,9 @@ def test_tc_512_accuracy_against_fp64():
         torch.cuda.empty_cache()
         print(f"{prec} 512^3 {ns} steps: vel {res[prec][0]:.3e} E(k) {res[prec][1]:.3e} "
               f"(tail shells {res[prec][2]:.3e}) D {res[prec][3]:.3e}")
-    ev, ek, _, dd = res["tc_split"]
+    ev, ek, ek_tail, dd = res["tc_split"]
     assert ev < 1e-6 and ek < 1e-5 and dd < 1e-5
+    assert ek_tail < 1e-3 and ek_tail < 4 * res["fp32"][2] + 1e-6
 
 
 def test_tc_1024_energy_budget():
@@ -212,7 +218,7 @@ def test_tc_rhs_anisotropic_box():
     """One right-hand side on an anisotropic box, x 64, y 128, z 256 with
     alpha 1, 2, 0.5: tensor-core passes of two lengths and a 2/3 cut at a
     different index on every axis, against the FP64 oracle (the FP32 form's
-    bar, 2e-5)."""
+    bar, 2e-6)."""
     nx, ny, nz = 64, 128, 256
     alpha = (1.0, 2.0, 0.5)
     p = O.Params(nx=nx, ny=ny, nz=nz, alpha_x=alpha[0], alpha_y=alpha[1], alpha_z=alpha[2], nu=2e-3,
@@ -226,6 +232,6 @@ def test_tc_rhs_anisotropic_box():
     got, ebg = b.rhs_nonlinear(b.from_numpy(uh))
     e = rel(got.cpu().numpy(), want)
     print(f"tc rhs anisotropic {nx}x{ny}x{nz}: {e:.3e}")
-    assert e < 2e-5
+    assert e < 2e-6
     assert abs(ebg - eb) < 1e-6 * eb
     b.close()
