@@ -33,12 +33,13 @@ class Params(ctypes.Structure):
         ("bandlim", ctypes.c_int32), ("spherical", ctypes.c_int32), ("tstep_fix", ctypes.c_int32),
         ("hminone", ctypes.c_int32), ("spectrum_mode", ctypes.c_int32), ("adj_phat", ctypes.c_int32),
         ("device", ctypes.c_int32), ("nbatch", ctypes.c_int32), ("no_prune", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 1),
+        ("implicit_max_iter", ctypes.c_int32),
         ("alpha_x", ctypes.c_double), ("alpha_y", ctypes.c_double), ("alpha_z", ctypes.c_double),
         ("nu", ctypes.c_double), ("Q", ctypes.c_double), ("kCutOff", ctypes.c_double),
         ("Pin", ctypes.c_double), ("Deltak", ctypes.c_double),
         ("courant_min", ctypes.c_double), ("courant_max", ctypes.c_double),
-        ("dt_max", ctypes.c_double), ("dt", ctypes.c_double), ("reserved_d", ctypes.c_double * 4),
+        ("dt_max", ctypes.c_double), ("dt", ctypes.c_double), ("implicit_c", ctypes.c_double),
+        ("implicit_tol", ctypes.c_double), ("reserved_d", ctypes.c_double * 2),
     ]
 
 
@@ -108,6 +109,10 @@ SIGNATURES = {
     "dnsbox_adjoint_descent": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _DP, _DP]),
     "dnsbox_heun_step_vjp": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "dnsbox_step_pruned": (ctypes.c_int, [_VP]),
+    "dnsbox_implicit_iterations": (ctypes.c_int, [_VP]),
+    "dnsbox_init_yoffe": (ctypes.c_int, [_VP, _VP, ctypes.c_uint64, _VP]),
+    "dnsbox_init_beltrami": (ctypes.c_int, [_VP, ctypes.c_double, _VP]),
+    "dnsbox_set_step_projection": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dnsbox_heun_steps_vjp": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
     "dnsbox_orbit_residual": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _DP]),
     "dnsbox_batch_size": (ctypes.c_int, [_VP]),

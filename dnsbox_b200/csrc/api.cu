@@ -8,6 +8,10 @@
 //   D  forward y FFT                                   (3 in, 3 out)
 //   E  forward z FFT + dealias + projection + forcing + stepper + E/D sums
 // instead of the reference's 15 p3dfft transforms plus pointwise loops.
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "internal.cuh"
 
 static thread_local std::string g_last_error;
@@ -56,6 +60,9 @@ extern "C" void dnsbox_default_params(dnsbox_params *p) {
   p->courant_max = 0.2;
   p->dt_max = 1.0e-2;
   p->dt = 1.0e-3;   // variables.f90:9
+  p->implicit_c = 0.5;          // parameters.f90:47
+  p->implicit_tol = 1.0e-10;    // parameters.f90:26
+  p->implicit_max_iter = 50;
 }
 
 // ------------------------------------------------------------ small kernels
@@ -279,6 +286,188 @@ __global__ void k_project(C *u, long long nh, int nx, int ny, int nz, double ax,
   }
 }
 
+// One fixed-point update of the semi-implicit step (dnsboximplicit.f90:112-173
+// with rhsFix / rhstStepFact restated as the theta scheme of nsbox.f90:192-221):
+//   fac = 1 / (1/dt - c L),  fix = (1/dt + (1 - c) L) u_n,  L = Q - nu |k|^2
+//   FIRST: u = fac (fix + n0);  else u <- fac (fix + c nk + (1 - c) n0)
+// and, for the iterations, chg[i] = max over the modes of |u_i new - u_i old|
+// (block maxima, then an atomic maximum).  dt is the step's device-side dt.
+template <typename C, bool FIRST>
+__global__ void k_si_update(C *u, const C *un, const C *n0, const C *nk, long long nh, int nx, int ny, int nz,
+                            double ax, double ay, double az, double nu, double Q, double cimp, const StepState *st,
+                            double *chg) {
+  using T = decltype(C{}.x);
+  __shared__ double red[3 * 32];
+  const int nxh = nx / 2 + 1;
+  const double dt = st->dt;
+  double mx[3] = {0.0, 0.0, 0.0};
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(m % nxh), ky = (int)((m / nxh) % ny), kz = (int)(m / ((long long)nxh * ny));
+    const double kxr = k_half(kx, nx, ax), kyr = k_full(ky, ny, ay), kzr = k_full(kz, nz, az);
+    const double L = Q - nu * (kxr * kxr + kyr * kyr + kzr * kzr);
+    const double fac = 1.0 / (1.0 / dt - cimp * L), g = 1.0 / dt + (1.0 - cimp) * L;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const long long q = i * nh + m;
+      const C a = un[q], b = n0[q];
+      double re, im;
+      if (FIRST) {
+        re = fac * (g * (double)a.x + (double)b.x);
+        im = fac * (g * (double)a.y + (double)b.y);
+      } else {
+        const C d = nk[q], o = u[q];
+        re = fac * (g * (double)a.x + cimp * (double)d.x + (1.0 - cimp) * (double)b.x);
+        im = fac * (g * (double)a.y + cimp * (double)d.y + (1.0 - cimp) * (double)b.y);
+        const C w = mkc<C>(T(re), T(im));
+        mx[i] = fmax(mx[i], hypot((double)w.x - (double)o.x, (double)w.y - (double)o.y));
+      }
+      u[q] = mkc<C>(T(re), T(im));
+    }
+  }
+  if (FIRST) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) mx[i] = warp_max(mx[i]);
+  if (lane == 0)
+    for (int i = 0; i < 3; ++i) red[32 * i + wid] = mx[i];
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int i = 0; i < 3; ++i) {
+      const double x = warp_max(lane < nw ? red[32 * i + lane] : 0.0);
+      if (lane == 0) atomic_max_nonneg(chg + i, x);
+    }
+  }
+}
+
+// Per-(kz, ky) row sums of E and D of a state (the partials the spectral
+// finish writes for the Heun and AB2 steps), one warp per row, fixed order.
+template <typename C>
+__global__ void k_row_sums(const C *u, long long nh, long long fstride, int nx, int ny, int nz, double ax,
+                           double ay, double az, double *partials) {
+  const int nxh = nx / 2 + 1;
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= ny * nz) return;
+  u += (long long)blockIdx.y * nh;   // box blockIdx.y; components fstride apart
+  partials += 2 * (long long)blockIdx.y * nz * ny;
+  const int kz = w / ny, ky = w - kz * ny;
+  const double kyr = k_full(ky, ny, ay), kzr = k_full(kz, nz, az);
+  const long long row = (long long)w * nxh;
+  double es = 0.0, ds = 0.0;
+  for (int kx = lane; kx < nxh; kx += 32) {
+    const double kxr = k_half(kx, nx, ax);
+    const double wk = kxr == 0.0 ? 0.5 : 1.0, k2 = kxr * kxr + kyr * kyr + kzr * kzr;
+    double e2 = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      const C v = u[i * fstride + row + kx];
+      e2 += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    es += wk * e2;
+    ds += 2.0 * wk * k2 * e2;
+  }
+  es = warp_sum(es);
+  ds = warp_sum(ds);
+  if (lane == 0) {
+    partials[2 * (long long)w] = es;
+    partials[2 * (long long)w + 1] = ds;
+  }
+}
+
+// Uniform noise in [-0.5, 0.5) from a counter-based hash of (seed, index)
+// (SplitMix64 finaliser; Steele, Lea and Flood, "Fast splittable
+// pseudorandom number generators", OOPSLA 2014).
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+template <typename T> __global__ void k_noise(T *out, long long n, uint64_t seed) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const uint64_t h = splitmix64(seed * 0xD1B54A32D192ED03ull + (uint64_t)i);
+    out[i] = (T)((double)(h >> 11) * 0x1.0p-53 - 0.5);
+  }
+}
+
+// state_init_analytic (state.f90:287-307): the Beltrami (Shapiro) field at
+// time t on the grid x(i) = i Lx / Nx, i = -Nx/2 .. Nx/2 - 1
+// (variables.f90:235-266); physical [3][z][y][x].
+template <typename T>
+__global__ void k_beltrami(T *u, int nx, int ny, int nz, double lx, double ly, double lz, double nu, double t) {
+  const long long np = (long long)nx * ny * nz;
+  const double f = sqrt(3.0), dec = exp(-(f * f) * t * nu);
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < np;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(m % nx), iy = (int)((m / nx) % ny), iz = (int)(m / ((long long)nx * ny));
+    const double x = (ix - nx / 2) * lx / nx, y = (iy - ny / 2) * ly / ny, z = (iz - nz / 2) * lz / nz;
+    u[m] = (T)(-0.5 * (f * cos(x) * sin(y) * sin(z) + sin(x) * cos(y) * cos(z)) * dec);
+    u[np + m] = (T)(0.5 * (f * sin(x) * cos(y) * sin(z) - cos(x) * sin(y) * cos(z)) * dec);
+    u[2 * np + m] = (T)(cos(x) * cos(y) * sin(z) * dec);
+  }
+}
+
+// Shell rescale of state_init_rand (state.f90:256-283): the nearest window
+// nk of |k| (the rounding of state.f90:363-367); modes with nk = 0 or
+// nk >= nspec are zeroed, the others multiplied by
+// sqrt(C1 (nk dk)^C2 exp(-C3 (nk dk)^C4) / espec[nk - 1]).
+template <typename C>
+__global__ void k_yoffe_rescale(C *u, long long nh, int nx, int ny, int nz, double ax, double ay, double az,
+                                double dk, int nspec, const double *espec) {
+  using T = decltype(C{}.x);
+  const double c1 = 8.0e-2, c2 = 2.0, c3 = 8.2352309e-2, c4 = 2.0;   // state.f90:218-221
+  const int nxh = nx / 2 + 1;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(m % nxh), ky = (int)((m / nxh) % ny), kz = (int)(m / ((long long)nxh * ny));
+    const double kxr = k_half(kx, nx, ax), kyr = k_full(ky, ny, ay), kzr = k_full(kz, nz, az);
+    const double absk = sqrt(kxr * kxr + kyr * kyr + kzr * kzr);
+    const double base = floor(absk / dk);
+    const int nk = absk < base + 0.5 * dk ? (int)base : (int)base + 1;
+    double f = 0.0;
+    if (nk != 0 && nk < nspec) {
+      const double kn = nk * dk;
+      f = sqrt(c1 * pow(kn, c2) * exp(-c3 * pow(kn, c4)) / espec[nk - 1]);
+    }
+    for (int i = 0; i < 3; ++i) {
+      const C v = u[i * nh + m];
+      u[i * nh + m] = mkc<C>(T(v.x * f), T(v.y * f));
+    }
+  }
+}
+
+// state_project + state_dealias of every box (dnsboxband.f90:142-143): boxes
+// on gridDim.y, components fstride apart, boxes nh apart.
+template <typename C>
+__global__ void k_project_dealias(C *u, long long nh, long long fstride, int nx, int ny, int nz, double ax,
+                                  double ay, double az, int spherical, double cx, double cy, double cz, double sph2) {
+  using T = decltype(C{}.x);
+  const int nxh = nx / 2 + 1;
+  u += (long long)blockIdx.y * nh;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+       m += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(m % nxh), ky = (int)((m / nxh) % ny), kz = (int)(m / ((long long)nxh * ny));
+    const double kr[3] = {k_half(kx, nx, ax), k_full(ky, ny, ay), k_full(kz, nz, az)};
+    const double k2 = kr[0] * kr[0] + kr[1] * kr[1] + kr[2] * kr[2];
+    const bool zero = kr[0] == 0.0 && kr[1] == 0.0 && kr[2] == 0.0;
+    const bool cut = (spherical && k2 >= sph2) || fabs(kr[0]) >= cx || fabs(kr[1]) >= cy || fabs(kr[2]) >= cz || zero;
+    if (cut) {
+      for (int i = 0; i < 3; ++i) u[i * fstride + m] = mkc<C>(0, 0);
+      continue;
+    }
+    const C v[3] = {u[m], u[fstride + m], u[2 * fstride + m]};
+    for (int i = 0; i < 3; ++i) {
+      double re = v[i].x, im = v[i].y;
+      for (int j = 0; j < 3; ++j) {
+        re -= (kr[i] * kr[j] * (double)v[j].x) / k2;
+        im -= (kr[i] * kr[j] * (double)v[j].y) / k2;
+      }
+      u[i * fstride + m] = mkc<C>(T(re), T(im));
+    }
+  }
+}
+
 // state_dealias (state.f90:181-209), in place
 template <typename C>
 __global__ void k_dealias(C *u, long long nh, int nx, int ny, int nz, double ax, double ay, double az,
@@ -435,44 +624,47 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   // pass A: inverse z
   StridedArgs<T> a = strided_base<T>(c, 2);
   a.njobs = 5;
-  set_job<T>(a, 0, cfield(u, c, 0), field(c->W1, c, 0));
-  set_job<T>(a, 1, cfield(u, c, 1), field(c->W1, c, 1));
-  set_job<T>(a, 2, cfield(u, c, 2), field(c->W1, c, 2));
-  set_job<T>(a, 3, cfield(u, c, 1), field(c->W1, c, 3), 0.0, -s, 1);   // -dz v
-  set_job<T>(a, 4, cfield(u, c, 0), field(c->W1, c, 4), 0.0, s, 1);    //  dz u
+  strided_ws<T>(c, a, 2, false, true);   // state -> padded workspace
+  set_job<T>(a, 0, cfield(u, c, 0), wfield(c->W1, c, 0));
+  set_job<T>(a, 1, cfield(u, c, 1), wfield(c->W1, c, 1));
+  set_job<T>(a, 2, cfield(u, c, 2), wfield(c->W1, c, 2));
+  set_job<T>(a, 3, cfield(u, c, 1), wfield(c->W1, c, 3), 0.0, -s, 1);   // -dz v
+  set_job<T>(a, 4, cfield(u, c, 0), wfield(c->W1, c, 4), 0.0, s, 1);    //  dz u
   if (pruned) {   // input zero outside kept (kz rows, ky, kx); outputs there stay unwritten (zero)
     a.kcol = c->keep[0];
     a.koth = c->keep[1];
     a.krin = c->keep[2];
   }
-  RET(run_strided<T>(c, 2, true, a, DNSBOX_PASS_Z_INV));
+  RET(run_strided<T>(c, 2, true, a, DNSBOX_PASS_Z_INV, true, uin, 3));
   // pass B: inverse y
   StridedArgs<T> b = strided_base<T>(c, 1);
+  strided_ws<T>(c, b, 1, true, true);
   b.njobs = 6;
-  set_job<T>(b, 0, field(c->W1, c, 0), field(c->W2, c, 0));
-  set_job<T>(b, 1, field(c->W1, c, 1), field(c->W2, c, 1));
-  set_job<T>(b, 2, field(c->W1, c, 2), field(c->W2, c, 2));
+  set_job<T>(b, 0, wfield(c->W1, c, 0), wfield(c->W2, c, 0));
+  set_job<T>(b, 1, wfield(c->W1, c, 1), wfield(c->W2, c, 1));
+  set_job<T>(b, 2, wfield(c->W1, c, 2), wfield(c->W2, c, 2));
   // omega_x = dy w - dz v ; omega_y = dz u - dx w ; omega_z = dx v - dy u (ks: 0 kx, 1 ky here)
-  set_job<T>(b, 3, field(c->W1, c, 2), field(c->W2, c, 3), 0.0, s, 1, field(c->W1, c, 3));
-  set_job<T>(b, 4, field(c->W1, c, 4), field(c->W2, c, 4), 1.0, 0.0, 0, field(c->W1, c, 2), 0.0, -s, 0);
-  set_job<T>(b, 5, field(c->W1, c, 0), field(c->W2, c, 5), 0.0, -s, 1, field(c->W1, c, 1), 0.0, s, 0);
+  set_job<T>(b, 3, wfield(c->W1, c, 2), wfield(c->W2, c, 3), 0.0, s, 1, wfield(c->W1, c, 3));
+  set_job<T>(b, 4, wfield(c->W1, c, 4), wfield(c->W2, c, 4), 1.0, 0.0, 0, wfield(c->W1, c, 2), 0.0, -s, 0);
+  set_job<T>(b, 5, wfield(c->W1, c, 0), wfield(c->W2, c, 5), 0.0, -s, 1, wfield(c->W1, c, 1), 0.0, s, 0);
   if (pruned) {   // pass-A outputs exist only on kept (ky, kx)
     b.kcol = c->keep[0];
     b.krin = c->keep[1];
   }
-  RET(run_strided<T>(c, 1, true, b, DNSBOX_PASS_Y_INV));
+  RET(run_strided<T>(c, 1, true, b, DNSBOX_PASS_Y_INV, true, c->W1, 6));
   // pass C: fused x pass
   XlineNLArgs<T> x;
   memset(&x, 0, sizeof(x));
-  x.U = reinterpret_cast<const C *>(field(c->W2, c, 0));
-  x.V = reinterpret_cast<const C *>(field(c->W2, c, 1));
-  x.W = reinterpret_cast<const C *>(field(c->W2, c, 2));
-  x.OX = reinterpret_cast<const C *>(field(c->W2, c, 3));
-  x.OY = reinterpret_cast<const C *>(field(c->W2, c, 4));
-  x.OZ = reinterpret_cast<const C *>(field(c->W2, c, 5));
-  x.NX = reinterpret_cast<C *>(field(c->W1, c, 0));
-  x.NY = reinterpret_cast<C *>(field(c->W1, c, 1));
-  x.NZ = reinterpret_cast<C *>(field(c->W1, c, 2));
+  x.U = reinterpret_cast<const C *>(wfield(c->W2, c, 0));
+  x.V = reinterpret_cast<const C *>(wfield(c->W2, c, 1));
+  x.W = reinterpret_cast<const C *>(wfield(c->W2, c, 2));
+  x.OX = reinterpret_cast<const C *>(wfield(c->W2, c, 3));
+  x.OY = reinterpret_cast<const C *>(wfield(c->W2, c, 4));
+  x.OZ = reinterpret_cast<const C *>(wfield(c->W2, c, 5));
+  x.NX = reinterpret_cast<C *>(wfield(c->W1, c, 0));
+  x.NY = reinterpret_cast<C *>(wfield(c->W1, c, 1));
+  x.NZ = reinterpret_cast<C *>(wfield(c->W1, c, 2));
+  x.pin = x.pout = c->wp;
   x.tw = reinterpret_cast<const C *>(c->tw[0]);
   x.st = c->st;
   x.lines_per_box = p.ny * p.nz;
@@ -497,18 +689,20 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   }
   // pass D: forward y
   StridedArgs<T> d = strided_base<T>(c, 1);
+  strided_ws<T>(c, d, 1, true, true);
   d.njobs = 3;
-  for (int f = 0; f < 3; ++f) set_job<T>(d, f, field(c->W1, c, f), field(c->W2, c, f));
+  for (int f = 0; f < 3; ++f) set_job<T>(d, f, wfield(c->W1, c, f), wfield(c->W2, c, f));
   if (pruned) {   // only kept kx columns; ky rows outside the kept set are masked by the finish
     d.kcol = c->keep[0];
     d.krout = c->keep[1];
   }
-  RET(run_strided<T>(c, 1, false, d, DNSBOX_PASS_Y_FWD));
+  RET(run_strided<T>(c, 1, false, d, DNSBOX_PASS_Y_FWD, true, c->W1, 6));
   // pass E1: forward z of the three components, in place (the SIMT kernel in
   // every form); pruned: kept kx columns and ky tiles, kept kz rows written
   StridedArgs<T> z = strided_base<T>(c, 2);
+  strided_ws<T>(c, z, 2, true, true);
   z.njobs = 3;
-  for (int f = 0; f < 3; ++f) set_job<T>(z, f, field(c->W2, c, f), field(c->W2, c, f));
+  for (int f = 0; f < 3; ++f) set_job<T>(z, f, wfield(c->W2, c, f), wfield(c->W2, c, f));
   if (pruned) {
     z.kcol = c->keep[0];
     z.koth = c->keep[1];
@@ -518,6 +712,9 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   // pass E2: spectral finish, one warp per (kz, ky) row
   FinishArgs<T> e = finish_base<T>(c);
   e.n3 = reinterpret_cast<const C *>(c->W2);
+  e.n3_pitch = c->wp;
+  e.n3_nh = (long long)c->wstride;
+  e.n3_bstride = (long long)p.nz * p.ny * c->wp;
   e.uin = reinterpret_cast<const C *>(uin);
   e.out = reinterpret_cast<C *>(out);
   e.state = reinterpret_cast<C *>(state);
@@ -541,6 +738,149 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
     default: k_finish_rows<T, FIN_AB2><<<grid, 256, 0, c->stream>>>(e, nrows); break;
   }
   CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+// ------------------------------------------------------------ TMA passes
+// cuTensorMapEncodeTiled, from the driver through the runtime (no link
+// dependency on libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// First rows of the 8-row boxes that cover the rows a pass keeps on a full
+// axis of length n (all rows when k.a = 0): [0, a), the Nyquist row n/2 and
+// (n - a, n), each range rounded out to whole boxes.  Returns the count, or
+// the full cover when the rounded ranges would overlap.
+static int tma_row_boxes(const AxisKeep &k, int n, unsigned short *rows) {
+  int nb = 0;
+  if (k.a > 0) {
+    const int lo_end = (k.a + 7) / 8 * 8;
+    int hi_start = n;
+    while (hi_start - 8 >= 0 && hi_start > n - k.a + 1) hi_start -= 8;
+    const int nq = n / 2;
+    if (lo_end <= nq && nq + 8 <= hi_start && nq % 8 == 0) {
+      for (int r = 0; r < lo_end; r += 8) rows[nb++] = (unsigned short)r;
+      rows[nb++] = (unsigned short)nq;
+      for (int r = hi_start; r < n; r += 8) rows[nb++] = (unsigned short)r;
+      return nb;
+    }
+  }
+  for (int r = 0; r < n; r += 8) rows[nb++] = (unsigned short)r;
+  return nb;
+}
+
+int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> &a, const void *base, int nslots,
+                    int kind) {
+  const dnsbox_params &p = c->p;
+  const int n = axis == 2 ? p.nz : p.ny;
+  const int width = 4096 / n;   // TmaPlan<n>::TCW
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return set_err(DNSBOX_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  TmaArgs t;
+  memset(&t, 0, sizeof(t));
+  // tile grid (as run_strided)
+  t.kcol = a.kcol;
+  t.koth = a.koth;
+  t.krin = a.krin;
+  t.krout = a.krout;
+  if (a.kcol.a) {
+    t.ntx_lo = (a.kcol.a + width - 1) / width;
+    const int nt = (p.nx / 2) / width;
+    t.nyq_tile = nt < t.ntx_lo ? 0 : (a.kcol.a % width ? -1 : nt);
+  }
+  const int ntx = t.ntx_lo ? t.ntx_lo + (t.nyq_tile > 0 ? 1 : 0) : (c->nxh + width - 1) / width;
+  const int nother = a.koth.a ? a.koth.count() : (axis == 2 ? p.ny : p.nz);
+  const int nbatch = a.nbatch > 0 ? a.nbatch : 1;
+  const long long total = (long long)a.njobs * ntx * nother * nbatch;
+  if (total >= (1LL << 31)) return set_err(DNSBOX_ERR_SIZE, "TMA pass: too many tiles");
+  t.total = (int)total;
+  t.per_box.init((unsigned)(a.njobs * ntx * nother));
+  t.njobs_d.init((unsigned)a.njobs);
+  t.ntxd.init((unsigned)ntx);
+  // jobs: slot coordinates of the inputs within `base`
+  const size_t slot_bytes = (axis == 2 ? c->fstride : c->wstride) * sizeof(float2);
+  auto slot_of = [&](const void *ptr) -> int {
+    const long long d = reinterpret_cast<const char *>(ptr) - reinterpret_cast<const char *>(base);
+    if (d < 0 || d % (long long)slot_bytes || d / (long long)slot_bytes >= nslots) return -2;
+    return (int)(d / (long long)slot_bytes);
+  };
+  t.njobs = a.njobs;
+  for (int j = 0; j < a.njobs; ++j) {
+    const StridedJob<float> &J = a.job[j];
+    TmaJob &T = t.job[j];
+    T.in1 = J.in1;
+    T.in2 = J.in2;
+    T.out = J.out;
+    T.a1 = (float)J.a1;
+    T.b1 = (float)J.b1;
+    T.a2 = (float)J.a2;
+    T.b2 = (float)J.b2;
+    T.ks1 = J.ks1;
+    T.ks2 = J.ks2;
+    T.slot1 = slot_of(J.in1);
+    T.slot2 = J.in2 ? slot_of(J.in2) : -1;
+    if (T.slot1 < 0 || T.slot2 < -1) return set_err(DNSBOX_ERR_STATE, "TMA pass: job input outside its tensor");
+    if (J.in2) t.two = 1;
+  }
+  t.tw = reinterpret_cast<const float2 *>(a.tw);
+  t.rowstride = a.rowstride;
+  t.otherstride = a.otherstride;
+  t.bstride = a.bstride;
+  t.rso = out_rowstride(a);
+  t.oso = out_otherstride(a);
+  t.bso = out_bstride(a);
+  if ((t.rso | t.oso | t.bso) & 1) return set_err(DNSBOX_ERR_STATE, "TMA pass: output rows must be 16-byte aligned");
+  t.plane = axis == 2;
+  t.in_pitch = c->nxh;
+  t.ncols = a.ncols;
+  t.nx = a.nx;
+  t.n_other = a.n_other;
+  t.alpha_row = (float)a.alpha_row;
+  t.alpha_x = (float)a.alpha_x;
+  t.alpha_other = (float)a.alpha_other;
+  t.nbox = tma_row_boxes(a.krin, n, t.box_row);
+  // the input tensor map
+  const int spc = width + 2;
+  cuuint64_t dims[5], strides[4];
+  const cuuint32_t box[5] = {(cuuint32_t)(2 * spc), 8, 1, 1, 1}, estr[5] = {1, 1, 1, 1, 1};
+  if (axis == 2) {   // state: (plane floats, z, box, component, 1)
+    const unsigned long long plane = (unsigned long long)p.ny * c->nxh;
+    dims[0] = 2 * plane;
+    dims[1] = (cuuint64_t)p.nz;
+    dims[2] = (cuuint64_t)nbatch;
+    dims[3] = (cuuint64_t)nslots;
+    dims[4] = 1;
+    strides[0] = plane * 8;
+    strides[1] = (cuuint64_t)c->nh * 8;
+    strides[2] = (cuuint64_t)c->fstride * 8;
+    strides[3] = (cuuint64_t)c->fstride * 8 * nslots;
+  } else {           // padded workspace: (row floats, y, z, box, slot)
+    dims[0] = 2ull * c->nxh;
+    dims[1] = (cuuint64_t)p.ny;
+    dims[2] = (cuuint64_t)p.nz;
+    dims[3] = (cuuint64_t)nbatch;
+    dims[4] = (cuuint64_t)nslots;
+    strides[0] = (cuuint64_t)c->wp * 8;
+    strides[1] = (cuuint64_t)p.ny * c->wp * 8;
+    strides[2] = (cuuint64_t)p.nz * p.ny * c->wp * 8;
+    strides[3] = (cuuint64_t)c->wstride * 8;
+  }
+  const CUresult r = encode(&t.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, const_cast<void *>(base), dims, strides, box,
+                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_err(DNSBOX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  Prof pr(c, kind);
+  CK(Ops<float>::strided_tma(n, t, inv, c->adft, c->tc_status, c->nsm, c->stream));
   return DNSBOX_OK;
 }
 
@@ -577,12 +917,68 @@ static int ring_read(dnsbox_ctx *c, long long first, int n, dnsbox_diag *host) {
   return DNSBOX_OK;
 }
 
-// One step of every box of the context (no host synchronisation).
+// The semi-implicit step (dnsboximplicit.f90:88-181) of one box: N(u_n), the
+// first guess, fixed-point iterations until the summed component change is at
+// most implicit_tol (one host read-back per iteration, at most
+// implicit_max_iter), state_project; then the row sums the step record needs.
+template <typename T> static int semi_implicit_step(dnsbox_ctx *c, void *uh) {
+  using C = typename CT<T>::type;
+  const dnsbox_params &p = c->p;
+  const long long nh = (long long)c->nh;
+  C *u = reinterpret_cast<C *>(c->ustar);
+  const C *un = reinterpret_cast<const C *>(uh), *n0 = reinterpret_cast<const C *>(c->nold);
+  const C *nk = reinterpret_cast<const C *>(c->sibuf);
+  RET(ensure_red(c, 3));
+  double *chg = c->red;   // 3 doubles
+  double *hchg = c->hstage + 48;
+  RET(run_rhs<T>(c, uh, FIN_RHS, c->nold, nullptr, nullptr, false, 1, nullptr, c->prune_now));   // :93
+  {
+    Prof pr(c, DNSBOX_PASS_SMALL);
+    k_si_update<C, true><<<grid_for(nh), 256, 0, c->stream>>>(u, un, n0, nullptr, nh, p.nx, p.ny, p.nz, p.alpha_x,
+                                                             p.alpha_y, p.alpha_z, p.nu, p.Q, p.implicit_c, c->st,
+                                                             nullptr);
+    CK(cudaGetLastError());
+  }
+  int it = 0;
+  while (it < p.implicit_max_iter) {   // :126-175
+    ++it;
+    RET(run_rhs<T>(c, u, FIN_RHS, c->sibuf, nullptr, nullptr, false, 0, nullptr, c->prune_now));
+    CK(cudaMemsetAsync(chg, 0, 3 * sizeof(double), c->stream));
+    {
+      Prof pr(c, DNSBOX_PASS_SMALL);
+      k_si_update<C, false><<<grid_for(nh), 256, 0, c->stream>>>(u, un, n0, nk, nh, p.nx, p.ny, p.nz, p.alpha_x,
+                                                                p.alpha_y, p.alpha_z, p.nu, p.Q, p.implicit_c,
+                                                                c->st, chg);
+      CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(hchg, chg, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const double total = hchg[0] + hchg[1] + hchg[2];
+    if (!(total == total)) return set_err(DNSBOX_ERR_NONFINITE, "semi-implicit iteration: non-finite change");
+    if (total <= p.implicit_tol) break;
+  }
+  c->si_iters = it;
+  Prof pr(c, DNSBOX_PASS_SMALL, 2);
+  k_project<C><<<grid_for(nh), 256, 0, c->stream>>>(u, nh, p.nx, p.ny, p.nz, p.alpha_x, p.alpha_y, p.alpha_z);   // :177
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(uh, u, 3 * (size_t)nh * sizeof(C), cudaMemcpyDeviceToDevice, c->stream));
+  if (!c->proj_every) {   // otherwise step_once sums the rows after the projection
+    k_row_sums<C><<<(p.ny * p.nz + 7) / 8, 256, 0, c->stream>>>(reinterpret_cast<const C *>(uh), nh, nh, p.nx, p.ny,
+                                                                p.nz, p.alpha_x, p.alpha_y, p.alpha_z, c->partials);
+    CK(cudaGetLastError());
+  }
+  return DNSBOX_OK;
+}
+
+// One step of every box of the context (no host synchronisation, except the
+// semi-implicit step's per-iteration read-back).
 template <typename T> static int step_once(dnsbox_ctx *c, void *uh) {
   const dnsbox_params &p = c->p;
   const double s = 1.0 / ((double)p.nx * p.ny * p.nz);
-  const bool pc = (p.stepper == DNSBOX_HEUN) || !c->ab2_started;
-  if (pc) {
+  const bool pc = (p.stepper == DNSBOX_HEUN) || (p.stepper == DNSBOX_AB2 && !c->ab2_started);
+  if (p.stepper == DNSBOX_SEMI_IMPLICIT) {
+    RET(semi_implicit_step<T>(c, uh));
+  } else if (pc) {
     // dnsboxheun.f90:85-126 (and dnsbox.f90:87-141 for the AB2 first step)
     RET(run_rhs<T>(c, uh, FIN_PRED, c->ustar, nullptr, p.stepper == DNSBOX_AB2 ? c->nold : nullptr, false, 1,
                    nullptr, c->prune_now));
@@ -592,8 +988,27 @@ template <typename T> static int step_once(dnsbox_ctx *c, void *uh) {
     // dnsbox.f90:143-191
     RET(run_rhs<T>(c, uh, FIN_AB2, nullptr, uh, c->nold, true, 1, nullptr, c->prune_now));
   }
-  const AxisKeep ky = c->prune_now ? c->keep[1] : AxisKeep{0, p.ny, 1};
-  const AxisKeep kz = c->prune_now ? c->keep[2] : AxisKeep{0, p.nz, 1};
+  if (c->proj_every) {
+    // dnsboxband.f90:142-143: project and dealias the new state, then its row sums
+    using C = typename CT<T>::type;
+    const dim3 g((unsigned)grid_for((long long)c->nh, 256, 148 * 8), (unsigned)c->nbatch);
+    Prof pr(c, DNSBOX_PASS_SMALL, 2);
+    k_project_dealias<C><<<g, 256, 0, c->stream>>>(reinterpret_cast<C *>(uh), (long long)c->nh,
+                                                    (long long)c->fstride, p.nx, p.ny, p.nz, p.alpha_x, p.alpha_y,
+                                                    p.alpha_z, p.spherical, (p.nx / 2.0) * (2.0 * p.alpha_x / 3.0),
+                                                    (p.ny / 2.0) * (2.0 * p.alpha_y / 3.0),
+                                                    (p.nz / 2.0) * (2.0 * p.alpha_z / 3.0),
+                                                    pow((p.nx / 2.0) * (2.0 / 3.0) * p.alpha_x, 2));
+    CK(cudaGetLastError());
+    k_row_sums<C><<<dim3((unsigned)((p.ny * p.nz + 7) / 8), (unsigned)c->nbatch), 256, 0, c->stream>>>(
+        reinterpret_cast<const C *>(uh), (long long)c->nh, (long long)c->fstride, p.nx, p.ny, p.nz, p.alpha_x,
+        p.alpha_y, p.alpha_z, c->partials);
+    CK(cudaGetLastError());
+  }
+  // k_row_sums visits every row
+  const bool rows_pruned = c->prune_now && p.stepper != DNSBOX_SEMI_IMPLICIT && !c->proj_every;
+  const AxisKeep ky = rows_pruned ? c->keep[1] : AxisKeep{0, p.ny, 1};
+  const AxisKeep kz = rows_pruned ? c->keep[2] : AxisKeep{0, p.nz, 1};
   double *planes = c->partials + 2 * (size_t)c->npartials * c->nbatch;
   Prof pr(c, DNSBOX_PASS_SMALL, 2);
   k_plane_sums<<<dim3((unsigned)p.nz, (unsigned)c->nbatch), 256, 0, c->stream>>>(c->partials, planes, p.nz, p.ny, ky,
@@ -692,6 +1107,8 @@ static int alloc_dft64(dnsbox_ctx *c) {
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   c->tc_ctas = TcPlan<256>::CTAS_PER_SM * nsm;   // persistent: every resident CTA slot
+  c->nsm = nsm;
+  c->tma_on = 1;
   return DNSBOX_OK;
 }
 
@@ -705,6 +1122,7 @@ static void free_ctx(dnsbox_ctx *c) {
   cudaFree(c->W2);
   cudaFree(c->ustar);
   cudaFree(c->nold);
+  cudaFree(c->sibuf);
   for (int i = 0; i < 3; ++i) cudaFree(c->tw[i]);
   cudaFree(c->st);
   cudaFree(c->partials);
@@ -729,8 +1147,13 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
   if (!(p->nu >= 0.0) || !(p->Deltak > 0.0) || !(p->dt > 0.0) || !(p->alpha_x > 0) || !(p->alpha_y > 0) ||
       !(p->alpha_z > 0))
     return set_err(DNSBOX_ERR_ARG, "invalid physical parameter");
-  if (p->stepper != DNSBOX_HEUN && p->stepper != DNSBOX_AB2)
+  if (p->stepper != DNSBOX_HEUN && p->stepper != DNSBOX_AB2 && p->stepper != DNSBOX_SEMI_IMPLICIT)
     return set_err(DNSBOX_ERR_ARG, "invalid stepper %d", p->stepper);
+  if (p->stepper == DNSBOX_SEMI_IMPLICIT &&
+      (p->nbatch > 1 || p->implicit_max_iter < 1 || !(p->implicit_tol >= 0.0) || !(p->implicit_c > 0.0) ||
+       !(p->implicit_c <= 1.0)))
+    return set_err(DNSBOX_ERR_ARG, "semi-implicit stepper: one box, implicit_max_iter >= 1, implicit_tol >= 0, "
+                                   "0 < implicit_c <= 1");
   CK(cudaSetDevice(p->device));
   if (p->nbatch < 0 || p->nbatch > 65535) return set_err(DNSBOX_ERR_ARG, "nbatch %d out of range", p->nbatch);
   dnsbox_ctx *c = new dnsbox_ctx();
@@ -742,18 +1165,25 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
   c->nh = (size_t)p->nz * p->ny * c->nxh;
   c->np = (size_t)p->nz * p->ny * p->nx;
   c->fstride = c->nh * c->nbatch;
+  {
+    const int q = c->fp64 ? 8 : 16;   // complex elements per 128 bytes
+    c->wp = (c->nxh + q - 1) / q * q;
+    c->wstride = (size_t)c->nbatch * p->nz * p->ny * c->wp;
+  }
   int rc = DNSBOX_OK;
   auto fail = [&](int r) {
     free_ctx(c);
     return r;
   };
   const size_t fb = c->fstride * c->cbytes;
+  const size_t wb = (c->wstride > c->fstride ? c->wstride : c->fstride) * c->cbytes;   // one workspace slot
   c->ring_cap = 1024;
   cudaError_t e;
-  if ((e = cudaMalloc(&c->W1, 6 * fb)) != cudaSuccess ||
-      (e = cudaMalloc(&c->W2, 6 * fb)) != cudaSuccess ||
+  if ((e = cudaMalloc(&c->W1, 6 * wb)) != cudaSuccess ||
+      (e = cudaMalloc(&c->W2, 6 * wb)) != cudaSuccess ||
       (e = cudaMalloc(&c->ustar, 3 * fb)) != cudaSuccess ||
-      (p->stepper == DNSBOX_AB2 && (e = cudaMalloc(&c->nold, 3 * fb)) != cudaSuccess) ||
+      (p->stepper != DNSBOX_HEUN && (e = cudaMalloc(&c->nold, 3 * fb)) != cudaSuccess) ||
+      (p->stepper == DNSBOX_SEMI_IMPLICIT && (e = cudaMalloc(&c->sibuf, 3 * fb)) != cudaSuccess) ||
       (e = cudaMalloc(&c->st, c->nbatch * sizeof(StepState))) != cudaSuccess ||
       (e = cudaMalloc(&c->ddiag, (size_t)c->ring_cap * c->nbatch * sizeof(dnsbox_diag))) != cudaSuccess ||
       (c->nbatch > 1 && (e = cudaMalloc(&c->d_nu, c->nbatch * sizeof(double))) != cudaSuccess)) {
@@ -796,7 +1226,8 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
       return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed"));
     // pruned steps leave the cut set of these buffers untouched: start at zero
     if ((e = cudaMemset(c->ustar, 0, 3 * fb)) != cudaSuccess ||
-        (c->nold && (e = cudaMemset(c->nold, 0, 3 * fb)) != cudaSuccess))
+        (c->nold && (e = cudaMemset(c->nold, 0, 3 * fb)) != cudaSuccess) ||
+        (c->sibuf && (e = cudaMemset(c->sibuf, 0, 3 * fb)) != cudaSuccess))
       return fail(set_err(DNSBOX_ERR_CUDA, "%s", cudaGetErrorString(e)));
   }
   c->npartials = p->nz * p->ny;   // one (E, D) pair per (kz, ky) row, then one per kz plane
@@ -885,6 +1316,7 @@ extern "C" int dnsbox_field_bytes(const dnsbox_ctx *ctx, size_t *sb, size_t *pb)
 extern "C" int dnsbox_nspec(const dnsbox_ctx *ctx) { return ctx ? ctx->nspec : -1; }
 
 extern "C" int dnsbox_step_pruned(const dnsbox_ctx *ctx) { return ctx ? ctx->prune_now : -1; }
+extern "C" int dnsbox_implicit_iterations(const dnsbox_ctx *ctx) { return ctx ? ctx->si_iters : -1; }
 
 #define BEGIN(ctx)                                              \
   if (!(ctx)) return set_err(DNSBOX_ERR_ARG, "null context");   \
@@ -1257,6 +1689,74 @@ extern "C" int dnsbox_upload_physical(dnsbox_ctx *ctx, const double *host, void 
   return DNSBOX_OK;
 }
 
+// 3D R2C of three physical fields of the context precision (3 np elements at
+// phys; may live in W2, which the x-line pass consumes before it is reused).
+template <typename T> static int phys3_to_state(dnsbox_ctx *ctx, const void *phys, void *uh) {
+  const void *in[3];
+  void *out[3];
+  for (int c = 0; c < 3; ++c) {
+    in[c] = reinterpret_cast<const T *>(phys) + (size_t)c * ctx->np;
+    out[c] = field(reinterpret_cast<char *>(uh), ctx, c);
+  }
+  return r2c_fields<T>(ctx, 3, in, out);
+}
+
+extern "C" int dnsbox_init_yoffe(dnsbox_ctx *ctx, const void *noise3_dev, uint64_t seed, void *uh) {
+  BEGIN(ctx);
+  SINGLE(ctx);
+  if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  const void *noise = noise3_dev;
+  if (!noise) {   // intent of state.f90:231-236: all three components uniform in [-0.5, 0.5)
+    const long long n3 = 3 * (long long)ctx->np;
+    if (ctx->fp64) k_noise<double><<<grid_for(n3), 256, 0, ctx->stream>>>((double *)ctx->W2, n3, seed);
+    else k_noise<float><<<grid_for(n3), 256, 0, ctx->stream>>>((float *)ctx->W2, n3, seed);
+    CK(cudaGetLastError());
+    noise = ctx->W2;
+  }
+  RET(ctx->fp64 ? phys3_to_state<double>(ctx, noise, uh) : phys3_to_state<float>(ctx, noise, uh));   // :240
+  RET(dnsbox_dealias(ctx, uh));   // :242
+  RET(dnsbox_project(ctx, uh));   // :243
+  std::vector<double> v;          // :244 (state_spectrum, in the context's spectrum mode)
+  RET(specdiag(ctx, uh, p.spectrum_mode == DNSBOX_SPECTRUM_SINGLE, v));
+  const int ns = ctx->nspec;
+  RET(ensure_red(ctx, (size_t)ns));
+  CK(cudaMemcpyAsync(ctx->red, v.data(), ns * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  const long long nh = (long long)ctx->nh;
+  if (ctx->fp64)
+    k_yoffe_rescale<double2><<<grid_for(nh), 256, 0, ctx->stream>>>((double2 *)uh, nh, p.nx, p.ny, p.nz, p.alpha_x,
+                                                                    p.alpha_y, p.alpha_z, p.Deltak, ns, ctx->red);
+  else
+    k_yoffe_rescale<float2><<<grid_for(nh), 256, 0, ctx->stream>>>((float2 *)uh, nh, p.nx, p.ny, p.nz, p.alpha_x,
+                                                                   p.alpha_y, p.alpha_z, p.Deltak, ns, ctx->red);
+  CK(cudaGetLastError());
+  RET(tc_check(ctx));   // the host vector v is read by the copy above before it goes out of scope
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_init_beltrami(dnsbox_ctx *ctx, double t, void *uh) {
+  BEGIN(ctx);
+  SINGLE(ctx);
+  if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  const dnsbox_params &p = ctx->p;
+  const double lx = 2 * M_PI / p.alpha_x, ly = 2 * M_PI / p.alpha_y, lz = 2 * M_PI / p.alpha_z;
+  const long long np = (long long)ctx->np;
+  if (ctx->fp64)
+    k_beltrami<double><<<grid_for(np), 256, 0, ctx->stream>>>((double *)ctx->W2, p.nx, p.ny, p.nz, lx, ly, lz, p.nu, t);
+  else
+    k_beltrami<float><<<grid_for(np), 256, 0, ctx->stream>>>((float *)ctx->W2, p.nx, p.ny, p.nz, lx, ly, lz, p.nu, t);
+  CK(cudaGetLastError());
+  RET(ctx->fp64 ? phys3_to_state<double>(ctx, ctx->W2, uh) : phys3_to_state<float>(ctx, ctx->W2, uh));
+  RET(tc_check(ctx));
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_set_step_projection(dnsbox_ctx *ctx, int on) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  ctx->proj_every = on ? 1 : 0;
+  return DNSBOX_OK;
+}
+
 extern "C" int dnsbox_download_physical(dnsbox_ctx *ctx, const void *uh, double *host) {
   BEGIN(ctx);
   SINGLE(ctx);
@@ -1397,6 +1897,8 @@ extern "C" int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *stat
     if (!ctxs[i] || !states[i]) return set_err(DNSBOX_ERR_ARG, "null context or state %d", i);
     if (ctxs[i]->p.device != ctxs[0]->p.device) return set_err(DNSBOX_ERR_ARG, "contexts on different devices");
     if (ctxs[i]->prof_on) return set_err(DNSBOX_ERR_STATE, "profiling must be off while capturing");
+    if (ctxs[i]->p.stepper == DNSBOX_SEMI_IMPLICIT)
+      return set_err(DNSBOX_ERR_UNSUPPORTED, "the semi-implicit step reads its iterations back: not capturable");
   }
   CK(cudaSetDevice(ctxs[0]->p.device));
   dnsbox_ensemble *e = new dnsbox_ensemble();

@@ -58,6 +58,9 @@ struct dnsbox_ctx {
   cudaStream_t stream = 0;
   char *W1 = nullptr, *W2 = nullptr;     // 6 spectral fields each
   char *ustar = nullptr, *nold = nullptr;
+  char *sibuf = nullptr;                 // semi-implicit step: N of the current iterate (3 fields)
+  int si_iters = 0;                      // fixed-point iterations of the last semi-implicit step
+  int proj_every = 0;                    // project and dealias the state after every step
   char *tw[3] = {nullptr, nullptr, nullptr};
   StepState *st = nullptr;               // device
   double *partials = nullptr;            // device, 2 per finish CTA
@@ -74,6 +77,12 @@ struct dnsbox_ctx {
   int cfl_first = 1;                     // reference calls set_time_step before the loop
   int nbatch = 1;                        // boxes of this size advanced together
   size_t fstride = 0;                    // elements between components / work slots (nbatch * nh)
+  // The right-hand side keeps its workspace fields (W1, W2) with a padded row
+  // pitch: wp complex elements per (z, y) row, a multiple of 128 bytes, so that
+  // every row starts on a 128-byte boundary (whole sectors for the strided
+  // passes and the x lines, 16-byte aligned tensor-map rows for TMA).
+  int wp = 0;
+  size_t wstride = 0;                    // elements between workspace slots (nbatch * nz * ny * wp)
   double *d_nu = nullptr;                // per-box viscosity (nbatch > 1) or null
   int ring_cap = 0;                      // device ring of step records: ring_cap steps x nbatch
   long long host_step = 0;               // steps issued so far (ring position)
@@ -86,6 +95,8 @@ struct dnsbox_ctx {
   void *adft = nullptr;                  // device DFT-64 operands (forward hi, lo, inverse hi, lo)
   int *tc_status = nullptr;              // device flag: an MMA completion wait gave up
   int tc_ctas = 0;                       // persistent grid of the tensor-core passes
+  int nsm = 0;                           // streaming multiprocessors of the device
+  int tma_on = 0;                        // the right-hand side uses the TMA-staged tensor-core passes
   char *adj = nullptr;                   // adjoint arena
   size_t adj_bytes = 0;
   char *orbit = nullptr;                 // checkpoints and segment states of the step-transpose chain
@@ -183,6 +194,19 @@ template <typename T> struct Ops {
     switch (n) { DNSBOX_SIZES(DNSBOX_CASE_TC) }
     return cudaErrorInvalidValue;
   }
+#define DNSBOX_CASE_TMA(NN) \
+  case NN: return Launcher<T, NN>::strided_tma(a, inv, adft, status, nctas, st);
+  static cudaError_t strided_tma(int n, const TmaArgs &a, bool inv, const void *adft, int *status, int nctas,
+                                 cudaStream_t st) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_TMA) }
+    return cudaErrorInvalidValue;
+  }
+#define DNSBOX_CASE_HASTMA(NN) \
+  case NN: return Launcher<T, NN>::has_tma();
+  static bool has_tma(int n) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_HASTMA) }
+    return false;
+  }
 #define DNSBOX_CASE_HASTC(NN) \
   case NN: return Launcher<T, NN>::has_tc();
   static bool has_tc(int n) {
@@ -222,6 +246,33 @@ static inline char *field(char *base, const dnsbox_ctx *c, int slot) {
 }
 static inline const char *cfield(const char *base, const dnsbox_ctx *c, int slot) {
   return base + (size_t)slot * c->fstride * c->cbytes;
+}
+// Slot of W1 / W2 in the padded layout of the right-hand side.
+static inline char *wfield(char *base, const dnsbox_ctx *c, int slot) {
+  return base + (size_t)slot * c->wstride * c->cbytes;
+}
+
+// Sets the input (in_ws) and output (out_ws) strides of a strided pass along
+// `axis` (2: z, 1: y) to the padded workspace layout; the other side keeps
+// the state layout of strided_base.
+template <typename T> static void strided_ws(const dnsbox_ctx *c, StridedArgs<T> &a, int axis, bool in_ws,
+                                             bool out_ws) {
+  const long long wp = c->wp, plane = (long long)c->p.ny * wp, box = plane * c->p.nz;
+  const long long rs = axis == 2 ? plane : wp, os = axis == 2 ? wp : plane;
+  if (in_ws) {
+    a.rowstride = rs;
+    a.otherstride = os;
+    a.bstride = box;
+  }
+  if (out_ws) {
+    a.rowstride_o = rs;
+    a.otherstride_o = os;
+    a.bstride_o = box;
+  } else if (in_ws) {   // the output keeps the state layout
+    a.rowstride_o = axis == 2 ? (long long)c->p.ny * c->nxh : c->nxh;
+    a.otherstride_o = axis == 2 ? c->nxh : (long long)c->p.ny * c->nxh;
+    a.bstride_o = (long long)c->nh;
+  }
 }
 
 static inline int ensure_red(dnsbox_ctx *c, size_t ndoubles) {
@@ -286,10 +337,19 @@ static void set_job(StridedArgs<T> &a, int j, const void *in1, void *out, double
 // the cut with the Nyquist column in the first free slot past the cut (or in
 // a tile of its own when the cut fills the last low tile); a.koth prunes the
 // other axis.
+// TMA-staged tensor-core pass (api.cu): `base` is the buffer whose `nslots`
+// fields the jobs read (the state for a z pass, W1 for a y pass).
+int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> &a, const void *base, int nslots,
+                    int kind);
+
 template <typename T>
 static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int kind = DNSBOX_PASS_OTHER,
-                       bool allow_tc = true) {
+                       bool allow_tc = true, const void *tma_base = nullptr, int tma_slots = 0) {
   const int n = axis == 2 ? c->p.nz : c->p.ny;
+  if constexpr (sizeof(T) == 4) {
+    if (allow_tc && tma_base && c->tc && c->tma_on && Ops<T>::has_tma(n))
+      return run_strided_tma(c, axis, inv, a, tma_base, tma_slots, kind);
+  }
   const bool tc = allow_tc && c->tc && Ops<T>::has_tc(n);
   const int width = tc ? 4096 / n : TileCols<T>::v;
   if (a.kcol.a) {

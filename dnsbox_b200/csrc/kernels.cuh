@@ -99,7 +99,21 @@ template <typename T> struct StridedArgs {
   // tile (see strided_col).
   AxisKeep kcol, koth, krin, krout;
   int ntx_lo, nyq_tile;
+  // strides of the output when its row pitch differs from the input's (the
+  // padded workspace fields of a right-hand side); 0: the input's
+  long long rowstride_o, otherstride_o, bstride_o;
 };
+
+// Output strides of a strided launch (the input's where unset).
+template <typename T> __host__ __device__ __forceinline__ long long out_rowstride(const StridedArgs<T> &a) {
+  return a.rowstride_o ? a.rowstride_o : a.rowstride;
+}
+template <typename T> __host__ __device__ __forceinline__ long long out_otherstride(const StridedArgs<T> &a) {
+  return a.otherstride_o ? a.otherstride_o : a.otherstride;
+}
+template <typename T> __host__ __device__ __forceinline__ long long out_bstride(const StridedArgs<T> &a) {
+  return a.bstride_o ? a.bstride_o : a.bstride;
+}
 
 // Column tiles of the grid of a strided launch with tile width tcw.
 template <typename T>
@@ -192,10 +206,11 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
   }
   fft_regs<C, N, INV>(v, s, TC, col, p, act, a.tw);
   if (valid) {
-    C *out = J.out + base;
+    const long long rso = out_rowstride(a);
+    C *out = J.out + ((long long)other * out_otherstride(a) + kx + (long long)blockIdx.y * out_bstride(a));
 #pragma unroll
     for (int i = 0; i < E; ++i)
-      if (a.krout.keep(EN::out_row(p, i))) out[(long long)EN::out_row(p, i) * a.rowstride] = v[i];
+      if (a.krout.keep(EN::out_row(p, i))) out[(long long)EN::out_row(p, i) * rso] = v[i];
   }
 }
 
@@ -209,6 +224,7 @@ template <typename T> struct XlineNLArgs {
   int nlines, nxh;
   int lines_per_box;                   // ny * nz
   int kxa;                             // pruning: only kx < kxa and kx = N/2 are read and written (0: all)
+  int pin, pout;                       // row pitch (complex elements) of the inputs / outputs; 0: nxh
   double alpha_x;
   double s;                            // scalemodes
 };
@@ -278,7 +294,8 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
       default: f1 = a.OZ; l1 = la; f2 = a.OZ; l2 = lb; break;
     }
     const bool v1 = act && l1 < a.nlines, v2 = act && l2 < a.nlines;
-    const C *r1 = f1 + (long long)l1 * a.nxh, *r2 = f2 + (long long)l2 * a.nxh;
+    const long long pin = a.pin ? a.pin : a.nxh;
+    const C *r1 = f1 + (long long)l1 * pin, *r2 = f2 + (long long)l2 * pin;
     C v[E];
 #pragma unroll
     for (int i = 0; i < E; ++i) {
@@ -339,6 +356,7 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
   }
   __syncthreads();
   // unpack two real transforms per sequence and store
+  const long long pout = a.pout ? a.pout : a.nxh;
   for (int it = threadIdx.x; it < NQ * H; it += NT) {
     const int k = it % H, q = it / H;
     const int j = q / 3, c = q % 3;
@@ -350,16 +368,16 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
     if (!xkeep(a.kxa, k, N)) continue;
     if (c == 0) {
       if (la < a.nlines) {
-        a.NX[(long long)la * a.nxh + k] = X1;
-        a.NY[(long long)la * a.nxh + k] = X2;
+        a.NX[(long long)la * pout + k] = X1;
+        a.NY[(long long)la * pout + k] = X2;
       }
     } else if (c == 1) {
-      if (la < a.nlines) a.NZ[(long long)la * a.nxh + k] = X1;
-      if (lb < a.nlines) a.NZ[(long long)lb * a.nxh + k] = X2;
+      if (la < a.nlines) a.NZ[(long long)la * pout + k] = X1;
+      if (lb < a.nlines) a.NZ[(long long)lb * pout + k] = X2;
     } else {
       if (lb < a.nlines) {
-        a.NX[(long long)lb * a.nxh + k] = X1;
-        a.NY[(long long)lb * a.nxh + k] = X2;
+        a.NX[(long long)lb * pout + k] = X1;
+        a.NY[(long long)lb * pout + k] = X2;
       }
     }
   }
@@ -430,6 +448,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
   const long long l1s[6] = {la, lb, la, la, lb, la};
   const long long l2s[6] = {la, lb, lb, la, lb, lb};
   const int p = lane % P, h = lane / P;   // position in the sequence, sequence slot
+  const long long pin = a.pin ? a.pin : a.nxh, pout = a.pout ? a.pout : a.nxh;
   // inverse transforms: round r transforms sequences SPW r + h; the loads of
   // the next round are issued before this round's transform
   C x1[E], x2[E];
@@ -438,8 +457,8 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
     const int n = EN::in_row(p, i);
     const int kk = n <= N / 2 ? n : N - n;
     const bool kp = xkeep(a.kxa, kk, N);
-    x1[i] = kp ? f1s[h][l1s[h] * a.nxh + kk] : mkc<C>(0, 0);
-    x2[i] = kp ? f2s[h][l2s[h] * a.nxh + kk] : mkc<C>(0, 0);
+    x1[i] = kp ? f1s[h][l1s[h] * pin + kk] : mkc<C>(0, 0);
+    x2[i] = kp ? f2s[h][l2s[h] * pin + kk] : mkc<C>(0, 0);
   }
 #pragma unroll 1
   for (int r = 0; r < 6 / SPW; ++r) {
@@ -449,7 +468,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
     for (int i = 0; i < E; ++i) v[i] = pack_pair<C, N>(EN::in_row(p, i), x1[i], x2[i]);
     if (r + 1 < 6 / SPW) {
       const int qn = q + SPW;
-      const C *g1 = f1s[qn] + l1s[qn] * a.nxh, *g2 = f2s[qn] + l2s[qn] * a.nxh;
+      const C *g1 = f1s[qn] + l1s[qn] * pin, *g2 = f2s[qn] + l2s[qn] * pin;
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const int n = EN::in_row(p, i);
@@ -533,14 +552,14 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
       const C X1 = mkc<C>(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
       const C X2 = mkc<C>(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
       if (q == 0) {
-        a.NX[la * a.nxh + k] = X1;
-        a.NY[la * a.nxh + k] = X2;
+        a.NX[la * pout + k] = X1;
+        a.NY[la * pout + k] = X2;
       } else if (q == 1) {
-        a.NZ[la * a.nxh + k] = X1;
-        a.NZ[lb * a.nxh + k] = X2;
+        a.NZ[la * pout + k] = X1;
+        a.NZ[lb * pout + k] = X2;
       } else {
-        a.NX[lb * a.nxh + k] = X1;
-        a.NY[lb * a.nxh + k] = X2;
+        a.NX[lb * pout + k] = X1;
+        a.NY[lb * pout + k] = X2;
       }
     }
   }
@@ -687,6 +706,10 @@ template <typename T> struct FinishArgs {
   int bandlim, spherical, mode, ab2_standard;
   double s;                // scalemodes
   AxisKeep kx, ky, kz;     // pruning: only kept (kz, ky) rows and kept kx modes are visited
+  // layout of n3 when it is a padded workspace field: row pitch, elements
+  // between components and between boxes; 0: the state's (nxh, nh, bstride)
+  int n3_pitch;
+  long long n3_nh, n3_bstride;
 };
 
 // Spectral finish after the forward z transform (the second half of one
@@ -711,6 +734,9 @@ __global__ void __launch_bounds__(256) k_finish_rows(const __grid_constant__ Fin
   const int kz = a.kz.map(oz), ky = a.ky.map(w - oz * nky);
   const int box = blockIdx.y;
   const long long rowbase = ((long long)kz * a.ny + ky) * a.nxh + (long long)box * a.bstride;
+  const long long n3nh = a.n3_nh ? a.n3_nh : a.nh;
+  const long long n3row = ((long long)kz * a.ny + ky) * (a.n3_pitch ? a.n3_pitch : a.nxh) +
+                          (long long)box * (a.n3_bstride ? a.n3_bstride : a.bstride);
   const StepState *st = a.st + box;
   const double nu = a.nu_box ? a.nu_box[box] : a.nu;
   const double dt = st->dt;
@@ -742,7 +768,7 @@ __global__ void __launch_bounds__(256) k_finish_rows(const __grid_constant__ Fin
       const long long idx = rowbase + kx;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        nn[h][c] = ok[h] ? a.n3[c * a.nh + idx] : mkc<C>(0, 0);
+        nn[h][c] = ok[h] ? a.n3[c * n3nh + n3row + kx] : mkc<C>(0, 0);
         uu[h][c] = ok[h] && need_u ? a.uin[c * a.nh + idx] : mkc<C>(0, 0);
         ss[h][c] = ok[h] && MODE == FIN_CORR ? a.state[c * a.nh + idx] : mkc<C>(0, 0);
         no[h][c] = ok[h] && MODE == FIN_AB2 ? a.nold[c * a.nh + idx] : mkc<C>(0, 0);

@@ -125,7 +125,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Work item w -> (job, base offset, column origin, other-axis index).
 struct TcItem {
   int job, kx0, other;
-  long long base0;
+  long long base0, base0o;   // input and output offsets of the tile origin
 };
 template <int TCW>
 __device__ __forceinline__ TcItem tc_item(const StridedArgs<float> &a, const TcArgs &g, unsigned w) {
@@ -139,6 +139,7 @@ __device__ __forceinline__ TcItem tc_item(const StridedArgs<float> &a, const TcA
   it.other = a.koth.map(o);
   it.kx0 = (a.ntx_lo == 0 || kt < a.ntx_lo ? kt : a.nyq_tile) * TCW;
   it.base0 = (long long)box * a.bstride + (long long)it.other * a.otherstride + it.kx0;
+  it.base0o = (long long)box * out_bstride(a) + (long long)it.other * out_otherstride(a) + it.kx0;
   return it;
 }
 
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
   TcItem nxt;   // decoded work item of the tile being fetched
   // Row offsets within one field fit in 32 bits (the launcher checks
   // N * rowstride < 2^31); the 64-bit part is the per-tile base.
-  const int rs = (int)a.rowstride;
+  const int rs = (int)a.rowstride, rso = (int)out_rowstride(a);
   // Kept-row masks, fixed per thread for the whole launch: bit 8 h + i for
   // input row N2 (8 q + i) + n2 of run h, bit N2 r + k2 for output row
   // k1 + 64 k2 of stage-2 item r.
@@ -430,10 +431,10 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
       }
       const int dc = strided_col(a, it.kx0 + cc) - it.kx0;
       if (it.kx0 + dc < a.ncols && a.kcol.keep(it.kx0 + dc)) {
-        C *out = J.out + (it.base0 + dc);
+        C *out = J.out + (it.base0o + dc);
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-          if ((outmask >> k) & 1u) out[(k1 + 64 * (8 * sp + k)) * rs] = z[k];
+          if ((outmask >> k) & 1u) out[(k1 + 64 * (8 * sp + k)) * rso] = z[k];
       }
     } else
 #pragma unroll
@@ -457,10 +458,10 @@ __global__ void __launch_bounds__(TcPlan<N>::THREADS, TcPlan<N>::CTAS_PER_SM)
       dft<N2, C, INV>(z);
       const int dc = strided_col(a, it.kx0 + cc) - it.kx0;
       if (it.kx0 + dc < a.ncols && a.kcol.keep(it.kx0 + dc)) {
-        C *out = J.out + (it.base0 + dc);
+        C *out = J.out + (it.base0o + dc);
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2)
-          if ((outmask >> (N2 * r + k2)) & 1u) out[(k1 + 64 * k2) * rs] = z[k2];
+          if ((outmask >> (N2 * r + k2)) & 1u) out[(k1 + 64 * k2) * rso] = z[k2];
       }
     }
     __syncthreads();

@@ -7,6 +7,7 @@
 
 #include "kernels.cuh"
 #include "kernels_tc.cuh"
+#include "kernels_tma.cuh"
 
 namespace dnsbox {
 
@@ -17,6 +18,10 @@ template <typename T, int N> struct Launcher {
   static cudaError_t strided_tc(const StridedArgs<T> &a, bool inv, int nother, const void *adft, int *status,
                                 int nctas, cudaStream_t st);
   static bool has_tc();
+  // TMA-staged tensor-core pass of the right-hand side (FP32, N = 128 .. 512)
+  static cudaError_t strided_tma(const TmaArgs &a, bool inv, const void *adft, int *status, int nctas,
+                                 cudaStream_t st);
+  static bool has_tma();
   static cudaError_t xline_nl(const XlineNLArgs<T> &a, cudaStream_t st);
   static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);
   static cudaError_t xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_t st);
@@ -71,7 +76,8 @@ cudaError_t Launcher<T, N>::strided_tc(const StridedArgs<T> &a, bool inv, int no
     const long long total = (long long)a.njobs * g.ntx * nother * (a.nbatch > 0 ? a.nbatch : 1);
     if (total == 0) return cudaSuccess;
     if (total + 2LL * nctas >= (1LL << 31)) return cudaErrorInvalidValue;
-    if ((long long)N * a.rowstride >= (1LL << 31)) return cudaErrorInvalidValue;   // 32-bit row offsets
+    if ((long long)N * a.rowstride >= (1LL << 31) || (long long)N * out_rowstride(a) >= (1LL << 31))
+      return cudaErrorInvalidValue;   // 32-bit row offsets
     g.total = (int)total;
     g.per_box.init((unsigned)(a.njobs * g.ntx * nother));
     g.njobs.init((unsigned)a.njobs);
@@ -93,6 +99,33 @@ cudaError_t Launcher<T, N>::strided_tc(const StridedArgs<T> &a, bool inv, int no
     return cudaGetLastError();
   } else {
     (void)a, (void)inv, (void)nother, (void)adft, (void)status, (void)nctas, (void)st;
+    return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T, int N> bool Launcher<T, N>::has_tma() {
+  return std::is_same<T, float>::value && TmaPlan<N>::on;
+}
+
+template <typename T, int N>
+cudaError_t Launcher<T, N>::strided_tma(const TmaArgs &a, bool inv, const void *adft, int *status, int nctas,
+                                        cudaStream_t st) {
+  if constexpr (std::is_same<T, float>::value && TmaPlan<N>::on) {
+    using PL = TmaPlan<N>;
+    if (a.total == 0) return cudaSuccess;
+    const unsigned nb = (unsigned)(a.total < nctas ? a.total : nctas);
+    const __half *A = reinterpret_cast<const __half *>(adft) + (inv ? 2 * 128 * 64 : 0);
+    cudaError_t e;
+    if (inv) {
+      if ((e = set_smem(k_strided_tma<N, true>, PL::SMEM)) != cudaSuccess) return e;
+      k_strided_tma<N, true><<<nb, PL::THREADS, PL::SMEM, st>>>(a, A, status);
+    } else {
+      if ((e = set_smem(k_strided_tma<N, false>, PL::SMEM)) != cudaSuccess) return e;
+      k_strided_tma<N, false><<<nb, PL::THREADS, PL::SMEM, st>>>(a, A, status);
+    }
+    return cudaGetLastError();
+  } else {
+    (void)a, (void)inv, (void)adft, (void)status, (void)nctas, (void)st;
     return cudaErrorInvalidValue;
   }
 }

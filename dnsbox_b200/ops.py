@@ -34,7 +34,7 @@ from . import _lib
 from .grid import nspec as _nspec
 
 PRECISION = {"fp64": 0, "fp32": 1, "tc_split": 2}
-STEPPER = {"heun": 0, "ab2": 1}
+STEPPER = {"heun": 0, "ab2": 1, "semi_implicit": 2}
 AB2_MODE = {"reference": 0, "standard": 1}
 SPECTRUM_MODE = {"mpi": 0, "single": 1}
 ADJ_PHAT = {"intent": 0, "literal": 1}
@@ -51,7 +51,8 @@ class Box:
                  ab2="reference", nu=0.005, Q=0.0, kCutOff=2.0, Pin=0.1, Deltak=1.0,
                  courant_min=0.15, courant_max=0.2, dt_max=1.0e-2, dt=1.0e-3, bandlim=True,
                  spherical=False, tstep_fix=False, hminone=True, spectrum_mode="mpi",
-                 adj_phat="intent", alpha=(1.0, 1.0, 1.0), device=None, nbatch=1, prune=True):
+                 adj_phat="intent", alpha=(1.0, 1.0, 1.0), device=None, nbatch=1, prune=True,
+                 implicit_c=0.5, implicit_tol=1e-10, implicit_max_iter=50):
         if not torch.cuda.is_available():
             raise RuntimeError("dnsbox_b200 needs a CUDA device (there is no CPU path)")
         lib = _lib.load()
@@ -76,6 +77,7 @@ class Box:
         p.alpha_x, p.alpha_y, p.alpha_z = alpha
         p.nu, p.Q, p.kCutOff, p.Pin, p.Deltak = nu, Q, kCutOff, Pin, Deltak
         p.courant_min, p.courant_max, p.dt_max, p.dt = courant_min, courant_max, dt_max, dt
+        p.implicit_c, p.implicit_tol, p.implicit_max_iter = implicit_c, implicit_tol, int(implicit_max_iter)
         self.params = p
         self.nx, self.ny, self.nz = nx, ny, nz
         self.nxh = nx // 2 + 1
@@ -292,6 +294,33 @@ class Box:
         """Waits for the work queued on this Box and raises if a device-side
         wait gave up (a tensor-core pass whose output is then invalid)."""
         _lib.check(self._lib.dnsbox_sync(self._h))
+
+    def init_yoffe(self, noise: torch.Tensor | None = None, seed: int = 0) -> torch.Tensor:
+        """state_init_rand (state.f90:211-285) on the device: from the physical
+        noise field (3, nz, ny, nx) in the Box's real dtype, or drawn from seed."""
+        if noise is not None:
+            noise = noise.contiguous()
+            assert noise.shape == (3, self.nz, self.ny, self.nx) and noise.dtype == self.rdtype
+        uh = self.zeros()
+        self._sync_stream()
+        _lib.check(self._lib.dnsbox_init_yoffe(self._h, _ptr(noise) if noise is not None else None,
+                                               ctypes.c_uint64(seed), _ptr(uh)))
+        return uh
+
+    def init_beltrami(self, t: float = 0.0) -> torch.Tensor:
+        """state_init_analytic (state.f90:287-307) at time t, as a spectral state."""
+        uh = self.zeros()
+        self._sync_stream()
+        _lib.check(self._lib.dnsbox_init_beltrami(self._h, float(t), _ptr(uh)))
+        return uh
+
+    def set_step_projection(self, on: bool = True):
+        """Project and dealias the state after every step (dnsboxband.f90:142-143)."""
+        _lib.check(self._lib.dnsbox_set_step_projection(self._h, int(bool(on))))
+
+    def implicit_iterations(self) -> int:
+        """Fixed-point iterations of the last semi-implicit step."""
+        return self._lib.dnsbox_implicit_iterations(self._h)
 
     def step_pruned(self) -> bool:
         """Whether the last step call ran the pruned (2/3-rule) passes."""

@@ -45,7 +45,9 @@ enum {
 };
 
 enum dnsbox_precision { DNSBOX_FP64 = 0, DNSBOX_FP32 = 1, DNSBOX_TC_SPLIT = 2 };
-enum dnsbox_stepper { DNSBOX_HEUN = 0, DNSBOX_AB2 = 1 };
+/* DNSBOX_SEMI_IMPLICIT: the fixed-point semi-implicit step of
+ * dnsboximplicit.f90:88-181 (implicitness implicit_c, parameters.f90:47) */
+enum dnsbox_stepper { DNSBOX_HEUN = 0, DNSBOX_AB2 = 1, DNSBOX_SEMI_IMPLICIT = 2 };
 /* dnsbox.f90:150-161 literal coefficients (quirk Q2) or standard IF-AB2 */
 enum dnsbox_ab2_mode { DNSBOX_AB2_REFERENCE = 0, DNSBOX_AB2_STANDARD = 1 };
 /* state.f90:350-411 (MPI build) or single/state.f90:191-230 (quirk Q4) */
@@ -69,7 +71,7 @@ typedef struct dnsbox_params {
   int32_t nbatch;                /* boxes of this size advanced together (0 or 1: one box) */
   int32_t no_prune;              /* 1: dnsbox_step never prunes the 2/3-rule zeros (default 0: it
                                     prunes when the state vanishes on the cut set; bit-identical) */
-  int32_t reserved_i[1];
+  int32_t implicit_max_iter;     /* DNSBOX_SEMI_IMPLICIT: fixed-point iterations per step at most */
   double alpha_x, alpha_y, alpha_z; /* parameters.f90:18-20                  */
   double nu;                     /* parameters.f90:21                        */
   double Q;                      /* parameters.f90:22                        */
@@ -79,7 +81,10 @@ typedef struct dnsbox_params {
   double courant_min, courant_max; /* parameters.f90:33-34                   */
   double dt_max;                 /* parameters.f90:35 (tStepMax)             */
   double dt;                     /* initial time step (variables.f90:9)      */
-  double reserved_d[4];
+  double implicit_c;             /* parameters.f90:47 (implicitness, 0.5)    */
+  double implicit_tol;           /* parameters.f90:26 (tol: sum of the component max |change|
+                                    of the spectral iterate, unnormalised)   */
+  double reserved_d[2];
 } dnsbox_params;
 
 /* Per-step diagnostics (the quantities io_save_stats writes to Ekin.dat,
@@ -128,12 +133,19 @@ int dnsbox_reset_history(dnsbox_ctx *ctx);
  * uhat3_dev -> nonlin3_dev (may not alias); eband_host may be NULL. */
 int dnsbox_rhs_nonlinear(dnsbox_ctx *ctx, const void *uhat3_dev, void *nonlin3_dev,
                          double *eband_host);
-/* Integrating-factor Heun (dnsboxheun.f90:85-126) or IF-AB2 with a
- * predictor-corrector first step (dnsbox.f90:87-218), nsteps in place, with
- * CFL control (dnsboxheun.f90:153-157 + io_Courant, io.f90:664-676) unless
+/* Integrating-factor Heun (dnsboxheun.f90:85-126), IF-AB2 with a
+ * predictor-corrector first step (dnsbox.f90:87-218) or the semi-implicit
+ * fixed-point step (dnsboximplicit.f90:88-181), nsteps in place, with CFL
+ * control (dnsboxheun.f90:153-157 + io_Courant, io.f90:664-676) unless
  * tstep_fix.  diag_host (nsteps records) may be NULL; when given, the call
- * synchronises the stream before returning. */
+ * synchronises the stream before returning.  The semi-implicit step reads the
+ * change of every fixed-point iteration back to the host (one
+ * synchronisation per iteration); dnsbox_implicit_iterations reports the
+ * iterations of the last step. */
 int dnsbox_step(dnsbox_ctx *ctx, void *uhat3_dev, int nsteps, dnsbox_diag *diag_host);
+/* Fixed-point iterations of the last semi-implicit step (the `iter` counter of
+ * dnsboximplicit.f90:127-131), -1 for a null context. */
+int dnsbox_implicit_iterations(const dnsbox_ctx *ctx);
 /* 1 if the last dnsbox_step call ran the pruned passes (the state vanished on
  * the 2/3-rule cut set, so loads of those zeros and transforms of modes the
  * mask discards were skipped, bit-identically), 0 if it ran the full passes,
@@ -175,6 +187,26 @@ int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec_dev, void *phys_dev);
  * share the scratch array, so calls that overlap on the GPU race. */
 int dnsbox_c2r_noalloc(int nx, int ny, int nz, int precision, const void *spec_dev, void *phys_dev,
                        void *cuda_stream);
+
+/* ---- initial conditions on the device ---------------------------------- */
+/* state_init_rand, state.f90:211-285 (Yoffe 2012, s. 2.2.5): a random physical
+ * field, R2C, state_dealias, state_project, state_spectrum (in the context's
+ * spectrum mode) and a rescale of every mode by
+ * sqrt(C1 (nk dk)^C2 exp(-C3 (nk dk)^C4) / E(nk)) with C1..C4 of
+ * state.f90:218-221 and nk the nearest shell (modes with nk = 0 or
+ * nk >= Nspec zeroed).  noise3_dev: the physical random field, [3][nz][ny][nx]
+ * reals of the context precision, or NULL to draw it on the device from seed
+ * (uniform in [-0.5, 0.5) for all three components; the reference's draw
+ * leaves w undrawn, quirk Q7).  Writes the spectral state (the reference then
+ * transforms it to physical space, state_uhat2u). */
+int dnsbox_init_yoffe(dnsbox_ctx *ctx, const void *noise3_dev, uint64_t seed, void *uhat3_dev);
+/* state_init_analytic, state.f90:287-307: the Beltrami (Shapiro) solution at
+ * time t, transformed to the spectral state. */
+int dnsbox_init_beltrami(dnsbox_ctx *ctx, double t, void *uhat3_dev);
+/* dnsboxband.f90:142-143: when on, every step ends with state_project and
+ * state_dealias of the new state (the step records then describe the
+ * projected state). */
+int dnsbox_set_step_projection(dnsbox_ctx *ctx, int on);
 
 /* Device storage for one spectral state (3 fields) in the context's precision,
  * for callers without a CUDA allocator of their own (the Fortran driver's

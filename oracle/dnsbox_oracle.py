@@ -236,6 +236,37 @@ def heun_step(g: Grid, uh, dt, force=None):
     return un + dt * n2 * 0.5                               # :122-124
 
 
+def semi_implicit_step(g: Grid, uh, dt, c=0.5, tol=1e-10, max_iter=50):
+    """dnsboximplicit.f90:88-181: the semi-implicit step with fixed-point
+    iterations (implicitness ``c``, parameters.f90:47; tolerance ``tol``,
+    parameters.f90:26).  The driver's ``rhsFix`` and ``rhstStepFact`` are
+    defined nowhere in the reference; they are restated here as the theta
+    scheme of the Crank-Nicolson solver nsbox.f90:192-221 with ``c`` the
+    implicitness of both the linear and the nonlinear term:
+      fac = 1 / (1/dt - c L),  fix = (1/dt + (1 - c) L) u_n,  L = nu k.k + Q
+      u^0 = fac (fix + N(u_n))                                       (:112-120)
+      u^(k+1) = fac (fix + c N(u^k) + (1 - c) N(u_n))               (:149-162)
+    until sum_i max |u_i^(k+1) - u_i^k| <= tol on the (unnormalised) spectral
+    values (:164-173), at most ``max_iter`` iterations; then state_project
+    (:177).  Returns (new state, iterations)."""
+    p = g.p
+    L = p.nu * np.real(g.kx * g.kx + g.ky * g.ky + g.kz * g.kz) + p.Q
+    fac = 1.0 / (1.0 / dt - c * L)
+    fix = (1.0 / dt + (1.0 - c) * L) * uh
+    n0 = rhs_nonlinear(g, uh)                               # :93
+    u = fac * (fix + n0)                                    # :112-120
+    it = 0
+    while it < max_iter:
+        it += 1
+        nk = rhs_nonlinear(g, u)                            # :137
+        un = fac * (fix + c * nk + (1.0 - c) * n0)          # :149-162
+        chg = sum(float(np.max(np.abs(un[i] - u[i]))) for i in range(3))   # :164-173
+        u = un
+        if chg <= tol:
+            break
+    return state_project(g, u), it                          # :177
+
+
 class AB2Stepper:
     """dnsbox.f90:87-218 (timestepper = 2): PC first step, then IF-AB2.
 
@@ -407,6 +438,27 @@ def needs_time_step(g: Grid, dt, courant):
     p = g.p
     return (not p.tstep_fix) and (courant > p.courant_max
                                   or (courant < p.courant_min and dt < p.dt_max))
+
+
+YOFFE_C = (8.0e-2, 2.0, 8.2352309e-2, 2.0)   # state.f90:218-221 (C1..C4)
+
+
+def state_init_rand(g: Grid, noise):
+    """state.f90:211-285 (Yoffe 2012, s. 2.2.5) from a given physical noise
+    field ``noise`` (3, nz, ny, nx): R2C, dealias, project, spectrum, and every
+    mode multiplied by sqrt(C1 (nk dk)^C2 exp(-C3 (nk dk)^C4) / Espec(nk)) with
+    nk the nearest shell; nk = 0 and nk >= Nspec are zeroed (:251-283).
+    Returns the spectral state (the reference continues with state_uhat2u)."""
+    p = g.p
+    uh = state_project(g, state_dealias(g, state_u2uhat(g, noise)))   # :240-243
+    espec, *_ = state_spectrum(g, uh)                                  # :244
+    nk = _shell_index(g)                                               # :249-254
+    c1, c2, c3, c4 = YOFFE_C
+    ok = (nk != 0) & (nk < g.nspec)                                    # :256
+    kn = np.where(ok, nk, 1) * p.Deltak
+    fac = np.where(ok, np.sqrt(c1 * kn ** c2 * np.exp(-c3 * kn ** c4)
+                               / np.where(ok, espec[np.where(ok, nk, 1) - 1], 1.0)), 0.0)
+    return uh * fac
 
 
 def beltrami(g: Grid, t):

@@ -253,3 +253,37 @@ def test_convective_equals_rotational_off_nyquist():
     uh = ic.random_field(n, seed=1, k0=3.0)
     keep = ~g.dealias_mask(0.5) & ~_nyquist_planes(n)
     assert rel(O.adj_rhs_nonlinear(g, uh)[:, keep], O.rhs_nonlinear(g, uh)[:, keep]) < 1e-13
+
+
+def test_yoffe_oracle_hits_the_target_spectrum():
+    """state.f90:211-285 restated: the rescaled field is solenoidal, dealiased
+    and its MPI-mode spectrum equals C1 k^C2 exp(-C3 k^C4) on shells
+    1 .. Nspec-1 (state.f90:218-221), with shell Nspec empty."""
+    n = 24
+    g = O.Grid(O.Params(nx=n, ny=n, nz=n))
+    noise = np.random.default_rng(3).random((3, n, n, n)) - 0.5
+    uh = O.state_init_rand(g, noise)
+    es, *_ = O.state_spectrum(g, uh)
+    c1, c2, c3, c4 = O.YOFFE_C
+    k = np.arange(1, g.nspec)
+    target = c1 * k ** c2 * np.exp(-c3 * k ** c4)
+    assert np.max(np.abs(es[:-1] - target) / target) < 1e-13 and es[-1] == 0.0
+    assert rel(O.state_dealias(g, O.state_project(g, uh)), uh) < 1e-14
+
+
+def test_semi_implicit_oracle_orders():
+    """dnsboximplicit.f90:88-181 restated: at c = 1/2 one step agrees with
+    IF-Heun to second order (the difference shrinks 8x when dt halves), at
+    c = 1 to first order, and the fixed point is reached within a few
+    iterations."""
+    n = 16
+    g = O.Grid(O.Params(nx=n, ny=n, nz=n, nu=0.01, bandlim=False))
+    uh = ic.random_field(n, seed=1, k0=3.0)
+    d = {}
+    for c in (0.5, 1.0):
+        for dt in (4e-3, 2e-3):
+            u, it = O.semi_implicit_step(g, uh, dt, c=c)
+            assert it <= 8
+            d[c, dt] = rel(u, O.heun_step(g, uh, dt))
+    assert 6.0 < d[0.5, 4e-3] / d[0.5, 2e-3] < 10.0
+    assert 3.0 < d[1.0, 4e-3] / d[1.0, 2e-3] < 5.0
