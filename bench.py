@@ -260,9 +260,11 @@ def extra_sizes(args):
         box = make_box(512, prec, 0, nu=8e-4)
         u = ic.random_field_gpu(box, seed=0, k0=WORKLOAD["k0"])
         box.step(u, args.warmup, diag=False)
+        sched = box.autotune(u, nsteps=2) if not args.no_tune else box.schedule()
         k = max(2, args.steps // 2)
         ms = timed_steps(box, u, k, False)
-        out[f"{prec}_512"] = {"value": k / (ms / 1e3), "ms_per_step": ms / k, "steps": k, "nu": 8e-4}
+        out[f"{prec}_512"] = {"value": k / (ms / 1e3), "ms_per_step": ms / k, "steps": k, "nu": 8e-4,
+                              "schedule": sched}
         box.close()
         del u
         torch.cuda.empty_cache()
@@ -426,6 +428,7 @@ def run_ours(args, rank, world, dist_on):
         box = make_box(n, prec, rank)
         u = box.from_numpy(uh_np)
         box.step(u, args.warmup, diag=False)
+        sched = box.autotune(u, nsteps=4) if not args.no_tune else box.schedule()
         torch.cuda.synchronize()
         box.profile_read(reset=True)
         sampler = ClockSampler(torch.cuda.current_device())
@@ -437,6 +440,7 @@ def run_ours(args, rank, world, dist_on):
             final[prec] = u.to(torch.complex128).cpu()   # after W + K steps from the same field
         pr = profile_passes(box, u, args.steps)
         res = {"ms": ms, "launches": launches, "profile": pr, "clocks": sampler.summary(), "pruned": pruned,
+               "schedule": sched,
                "pass_fields": pruned_pass_fields(n) if pruned else PASS_FIELDS_HEUN}
         if prec == args.precisions[0] and rank == 0:
             res["e2e"] = measure_e2e(box, uh_np, max(3, min(args.steps, 20)))
@@ -496,6 +500,7 @@ def run_ours(args, rank, world, dist_on):
         "passes": {k: {kk: round(vv, 3) for kk, vv in v.items()} for k, v in per_pass.items()},
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
+        "schedule": r["schedule"],
     }
     if e2e:
         line["e2e"] = {"value": e2e[0] * world, "unit": UNIT, "h2d_bytes_per_step": e2e[1],
@@ -513,7 +518,7 @@ def run_ours(args, rank, world, dist_on):
         prr = rr["profile"]
         line.setdefault("variants", {})[prec] = {
             "value": world * args.steps / (rr["ms"] / 1e3), "ms_per_step": rr["ms"] / args.steps,
-            "gpu_launches": rr["launches"], "clocks": rr["clocks"],
+            "gpu_launches": rr["launches"], "clocks": rr["clocks"], "schedule": rr["schedule"],
             "passes": {k: {"avg_us": round(1e3 * prr["ms"][k] / prr["launches"][k], 2),
                            "gbs": round(sum(f[i % len(f)] for i in range(prr["launches"][k])) * rr["field_bytes"]
                                         / (prr["ms"][k] / 1e3) / 1e9, 1)}
@@ -546,6 +551,7 @@ def main():
     ap.add_argument("--precisions", default="tc_split,fp64,fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 512^3 and adjoint legs")
+    ap.add_argument("--no-tune", action="store_true", help="time the default kernel schedule (no autotuning)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-budget", type=float, default=90.0)
     args = ap.parse_args()

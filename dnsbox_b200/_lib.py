@@ -54,6 +54,14 @@ class Diag(ctypes.Structure):
     ]
 
 
+class Schedule(ctypes.Structure):
+    """``dnsbox_schedule``: the right-hand side's kernel choices."""
+    _fields_ = [
+        ("tc_kernel", ctypes.c_int32 * 3), ("x_kernel", ctypes.c_int32), ("tuned", ctypes.c_int32),
+        ("reserved", ctypes.c_int32), ("ms_default", ctypes.c_double), ("ms_tuned", ctypes.c_double),
+    ]
+
+
 NPASS = 8
 PASS_NAMES = ["z_inv", "y_inv", "x_nl", "y_fwd", "z_fin", "small", "other", "z_fwd"]
 
@@ -124,6 +132,9 @@ SIGNATURES = {
     "dnsbox_ensemble_destroy": (ctypes.c_int, [_VP]),
     "dnsbox_profile_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dnsbox_sync": (ctypes.c_int, [_VP]),
+    "dnsbox_get_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(Schedule)]),
+    "dnsbox_set_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(Schedule)]),
+    "dnsbox_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.POINTER(Schedule)]),
     "dnsbox_profile_read": (ctypes.c_int, [_VP, ctypes.POINTER(Profile), ctypes.c_int]),
 }
 

@@ -675,7 +675,7 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   if (pruned) x.kxa = c->keep[0].a;   // read only kept kx; write only kx the finish keeps
   {
     Prof pr(c, DNSBOX_PASS_X_NL);
-    CK(Ops<T>::xline_nl(p.nx, x, c->stream));
+    CK(Ops<T>::xline_nl(p.nx, x, c->sched_x, c->stream));
   }
   if (cfl) {
     const double dx = (2 * M_PI / p.alpha_x) / p.nx, dy = (2 * M_PI / p.alpha_y) / p.ny,
@@ -1108,7 +1108,10 @@ static int alloc_dft64(dnsbox_ctx *c) {
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   c->tc_ctas = TcPlan<256>::CTAS_PER_SM * nsm;   // persistent: every resident CTA slot
   c->nsm = nsm;
-  c->tma_on = 1;
+  // DNSBOX_TC_KERNEL=legacy keeps the right-hand side on the cp.async-fed
+  // tensor-core kernel of the standalone transforms (for comparisons)
+  const char *kern = getenv("DNSBOX_TC_KERNEL");
+  c->tma_on = !(kern && strcmp(kern, "legacy") == 0);
   return DNSBOX_OK;
 }
 
@@ -1288,6 +1291,7 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
                           pow((p->nz / 2.0) * (2.0 * p->alpha_z / 3.0), 2)) /
                      p->Deltak) -
                1;
+  schedule_from_cache(c);   // a schedule tuned earlier for this device and shape
   *out = c;
   return DNSBOX_OK;
 }

@@ -47,6 +47,8 @@ void descent_graphs_free(dnsbox_ctx *c);
 // Synchronises the context's stream and returns DNSBOX_ERR_TIMEOUT (clearing
 // the flag) if a tensor-core pass gave up waiting for its MMAs (api.cu).
 int tc_check(dnsbox_ctx *c);
+// Applies the schedule cached for the context's device and shape (tune.cu).
+void schedule_from_cache(dnsbox_ctx *c);
 
 // ------------------------------------------------------------------ context
 struct dnsbox_ctx {
@@ -97,6 +99,11 @@ struct dnsbox_ctx {
   int tc_ctas = 0;                       // persistent grid of the tensor-core passes
   int nsm = 0;                           // streaming multiprocessors of the device
   int tma_on = 0;                        // the right-hand side uses the TMA-staged tensor-core passes
+  // kernel schedule of the right-hand side (chosen by dnsbox_autotune, or the
+  // defaults): per tensor-core pass A, B, D 0 = TMA-staged, 1 = legacy
+  // cp.async-fed kernel; x pass 0 = default, 1 = block, 2 = warp kernel
+  int sched_tc[3] = {0, 0, 0};
+  int sched_x = 0;
   char *adj = nullptr;                   // adjoint arena
   size_t adj_bytes = 0;
   char *orbit = nullptr;                 // checkpoints and segment states of the step-transpose chain
@@ -214,10 +221,16 @@ template <typename T> struct Ops {
     return false;
   }
 #define DNSBOX_CASE_NL(NN) \
-  case NN: return Launcher<T, NN>::xline_nl(a, st);
-  static cudaError_t xline_nl(int n, const XlineNLArgs<T> &a, cudaStream_t st) {
+  case NN: return Launcher<T, NN>::xline_nl(a, variant, st);
+  static cudaError_t xline_nl(int n, const XlineNLArgs<T> &a, int variant, cudaStream_t st) {
     switch (n) { DNSBOX_SIZES(DNSBOX_CASE_NL) }
     return cudaErrorInvalidValue;
+  }
+#define DNSBOX_CASE_HASXW(NN) \
+  case NN: return Launcher<T, NN>::has_xline_warp();
+  static bool has_xline_warp(int n) {
+    switch (n) { DNSBOX_SIZES(DNSBOX_CASE_HASXW) }
+    return false;
   }
 #define DNSBOX_CASE_C2R(NN) \
   case NN: return Launcher<T, NN>::xline_c2r(a, nf, st);
@@ -347,7 +360,8 @@ static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int 
                        bool allow_tc = true, const void *tma_base = nullptr, int tma_slots = 0) {
   const int n = axis == 2 ? c->p.nz : c->p.ny;
   if constexpr (sizeof(T) == 4) {
-    if (allow_tc && tma_base && c->tc && c->tma_on && Ops<T>::has_tma(n))
+    const int si = kind == DNSBOX_PASS_Z_INV ? 0 : kind == DNSBOX_PASS_Y_INV ? 1 : kind == DNSBOX_PASS_Y_FWD ? 2 : -1;
+    if (allow_tc && tma_base && c->tc && c->tma_on && Ops<T>::has_tma(n) && si >= 0 && c->sched_tc[si] == 0)
       return run_strided_tma(c, axis, inv, a, tma_base, tma_slots, kind);
   }
   const bool tc = allow_tc && c->tc && Ops<T>::has_tc(n);

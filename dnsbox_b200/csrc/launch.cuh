@@ -22,7 +22,9 @@ template <typename T, int N> struct Launcher {
   static cudaError_t strided_tma(const TmaArgs &a, bool inv, const void *adft, int *status, int nctas,
                                  cudaStream_t st);
   static bool has_tma();
-  static cudaError_t xline_nl(const XlineNLArgs<T> &a, cudaStream_t st);
+  // variant: 0 the default kernel for N, 1 the block kernel, 2 the warp kernel (where it exists)
+  static cudaError_t xline_nl(const XlineNLArgs<T> &a, int variant, cudaStream_t st);
+  static bool has_xline_warp();
   static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);
   static cudaError_t xline_r2c(const XlineArgs<T> &a, int nf, cudaStream_t st);
   static int strided_threads();
@@ -130,10 +132,13 @@ cudaError_t Launcher<T, N>::strided_tma(const TmaArgs &a, bool inv, const void *
   }
 }
 
+template <typename T, int N> bool Launcher<T, N>::has_xline_warp() { return XlineWarp<T, N>::on; }
+
 template <typename T, int N>
-cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, cudaStream_t st) {
+cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaStream_t st) {
   using C = typename CT<T>::type;
   if constexpr (XlineWarp<T, N>::on) {
+    if (variant != 1) {
     // warp-granular kernel: one warp per line pair
     constexpr int WPB = XlineWarp<T, N>::wpb;
     constexpr int LDC = N + N / XlineWarp<T, N>::Plan::R[0];
@@ -144,6 +149,7 @@ cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, cudaStream_t st) {
     const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
     k_xline_nl_w<T, N><<<nb, 32 * WPB, smem, st>>>(a);
     return cudaGetLastError();
+    }
   }
   constexpr int B = XlineB<T, N>::v;
   const size_t smem = (size_t)N * (3 * B + 1) * sizeof(C);

@@ -1,0 +1,223 @@
+// Kernel-schedule autotuner of the right-hand side: dnsbox_autotune,
+// dnsbox_get_schedule, dnsbox_set_schedule.
+//
+// The reference leaves its transform plans to p3dfft / FFTW
+// (variables.f90:154, p3dfft_setup measuring FFTW plans).  Here the
+// transforms are the library's own kernels, and the choices that measured
+// differently across sizes are made by timing: for each of the tensor-core
+// strided passes (A inverse z, B inverse y, D forward y) the TMA-staged or
+// the cp.async-fed kernel, and for the fused x pass the block or the warp
+// kernel.  Each uniform candidate schedule advances a copy of the caller's
+// state for a few steps with pass timing on (CUDA events on the context's
+// stream); every pass keeps its fastest kernel; the chosen schedule is timed
+// once more.  The context's clock, time step and step history are restored,
+// and the choice is cached per (device, precision, grid, boxes) so that later
+// contexts of the same shape start with it.
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace {
+
+using Key = std::tuple<int, int, int, int, int, int>;   // device, precision, nx, ny, nz, nbatch
+std::map<Key, dnsbox_schedule> g_cache;
+std::mutex g_cache_mu;
+
+Key key_of(const dnsbox_ctx *c) {
+  return Key(c->p.device, c->p.precision, c->p.nx, c->p.ny, c->p.nz, c->nbatch);
+}
+
+void apply(dnsbox_ctx *c, const dnsbox_schedule &s) {
+  for (int i = 0; i < 3; ++i) c->sched_tc[i] = s.tc_kernel[i] ? 1 : 0;
+  c->sched_x = s.x_kernel;
+}
+
+dnsbox_schedule current(const dnsbox_ctx *c) {
+  dnsbox_schedule s;
+  memset(&s, 0, sizeof(s));
+  for (int i = 0; i < 3; ++i) s.tc_kernel[i] = c->sched_tc[i];
+  s.x_kernel = c->sched_x;
+  return s;
+}
+
+// Saved per-context stepping state (clock, dt, CFL and AB2 history),
+// restored after each trial.
+struct Saved {
+  std::vector<StepState> st;
+  long long host_step;
+  int ab2_started, cfl_first;
+  void *nold = nullptr;   // copy of the AB2 history
+};
+
+int save(dnsbox_ctx *c, Saved &sv) {
+  sv.st.resize(c->nbatch);
+  CK(cudaMemcpyAsync(sv.st.data(), c->st, c->nbatch * sizeof(StepState), cudaMemcpyDeviceToHost, c->stream));
+  if (c->nold) {
+    CK(cudaMalloc(&sv.nold, 3 * c->fstride * c->cbytes));
+    CK(cudaMemcpyAsync(sv.nold, c->nold, 3 * c->fstride * c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  sv.host_step = c->host_step;
+  sv.ab2_started = c->ab2_started;
+  sv.cfl_first = c->cfl_first;
+  return DNSBOX_OK;
+}
+
+int restore(dnsbox_ctx *c, const Saved &sv) {
+  CK(cudaMemcpyAsync(c->st, sv.st.data(), c->nbatch * sizeof(StepState), cudaMemcpyHostToDevice, c->stream));
+  if (sv.nold) CK(cudaMemcpyAsync(c->nold, sv.nold, 3 * c->fstride * c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->host_step = sv.host_step;
+  c->ab2_started = sv.ab2_started;
+  c->cfl_first = sv.cfl_first;
+  return DNSBOX_OK;
+}
+
+// Times `nsteps` steps of the schedule on a copy of the state: per-pass event
+// time (ms) and the whole steps' time.
+int trial(dnsbox_ctx *c, const dnsbox_schedule &s, const void *uh, void *scratch, size_t bytes, const Saved &sv,
+          int nsteps, double pass_ms[DNSBOX_NPASS], double *step_ms) {
+  apply(c, s);
+  RET(restore(c, sv));
+  CK(cudaMemcpyAsync(scratch, uh, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  RET(step_advance_decided(c, scratch, 2, true));   // warm-up (and kernel loading)
+  dnsbox_profile pr;
+  RET(dnsbox_profile_read(c, &pr, 1));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int prof = c->prof_on;
+  c->prof_on = 1;
+  CK(cudaEventRecord(e0, c->stream));
+  const int rc = step_advance_decided(c, scratch, nsteps, false);
+  CK(cudaEventRecord(e1, c->stream));
+  c->prof_on = prof;
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  RET(rc);
+  RET(dnsbox_profile_read(c, &pr, 1));
+  for (int k = 0; k < DNSBOX_NPASS; ++k) pass_ms[k] = pr.ms[k];
+  *step_ms = ms / nsteps;
+  return DNSBOX_OK;
+}
+
+}  // namespace
+
+// Applies a cached schedule to a new context (api.cu calls it at creation).
+void schedule_from_cache(dnsbox_ctx *c) {
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  auto it = g_cache.find(key_of(c));
+  if (it != g_cache.end()) apply(c, it->second);
+}
+
+extern "C" int dnsbox_get_schedule(const dnsbox_ctx *ctx, dnsbox_schedule *out) {
+  if (!ctx || !out) return set_err(DNSBOX_ERR_ARG, "null argument");
+  *out = current(ctx);
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_set_schedule(dnsbox_ctx *ctx, const dnsbox_schedule *s) {
+  if (!ctx || !s) return set_err(DNSBOX_ERR_ARG, "null argument");
+  for (int i = 0; i < 3; ++i)
+    if (s->tc_kernel[i] != 0 && s->tc_kernel[i] != 1) return set_err(DNSBOX_ERR_ARG, "tc_kernel must be 0 or 1");
+  if (s->x_kernel < 0 || s->x_kernel > 2) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0, 1 or 2");
+  apply(ctx, *s);
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsbox_schedule *out) {
+  if (!ctx) return set_err(DNSBOX_ERR_ARG, "null context");
+  CK(cudaSetDevice(ctx->p.device));
+  if (!uh || nsteps < 1) return set_err(DNSBOX_ERR_ARG, "invalid argument");
+  if (ctx->p.stepper == DNSBOX_SEMI_IMPLICIT)
+    return set_err(DNSBOX_ERR_UNSUPPORTED, "the semi-implicit step is not tuned (it reads back every iteration)");
+  const dnsbox_params &p = ctx->p;
+  const bool fp64 = ctx->fp64;
+  // candidate kernels
+  std::vector<int> tc_opts = {0};
+  if (ctx->tc && !fp64) {
+    const bool tz = Ops<float>::has_tma(p.nz) && Ops<float>::has_tc(p.nz);
+    const bool ty = Ops<float>::has_tma(p.ny) && Ops<float>::has_tc(p.ny);
+    if (ctx->tma_on && (tz || ty)) tc_opts.push_back(1);
+  }
+  std::vector<int> x_opts = {0};
+  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1};
+  const dnsbox_schedule saved_sched = current(ctx);
+  Saved sv;
+  RET(save(ctx, sv));
+  const size_t bytes = 3 * ctx->fstride * ctx->cbytes;
+  void *scratch = nullptr;
+  CK(cudaMalloc(&scratch, bytes));
+  struct Run {
+    dnsbox_schedule s;
+    double pass[DNSBOX_NPASS];
+    double step;
+  };
+  std::vector<Run> runs;
+  int rc = DNSBOX_OK;
+  for (int tcv : tc_opts) {
+    for (int xv : x_opts) {
+      Run r;
+      memset(&r, 0, sizeof(r));
+      for (int i = 0; i < 3; ++i) r.s.tc_kernel[i] = tcv;
+      r.s.x_kernel = xv;
+      if ((rc = trial(ctx, r.s, uh, scratch, bytes, sv, nsteps, r.pass, &r.step)) != DNSBOX_OK) break;
+      runs.push_back(r);
+    }
+    if (rc != DNSBOX_OK) break;
+  }
+  dnsbox_schedule best;
+  memset(&best, 0, sizeof(best));
+  if (rc == DNSBOX_OK) {
+    // per pass: the kernel whose runs took least time on average
+    const int pass_of[3] = {DNSBOX_PASS_Z_INV, DNSBOX_PASS_Y_INV, DNSBOX_PASS_Y_FWD};
+    for (int i = 0; i < 3; ++i) {
+      double bestv = 1e300;
+      for (int tcv : tc_opts) {
+        double sum = 0.0;
+        int n = 0;
+        for (const Run &r : runs)
+          if (r.s.tc_kernel[i] == tcv) sum += r.pass[pass_of[i]], ++n;
+        if (n && sum / n < bestv) bestv = sum / n, best.tc_kernel[i] = tcv;
+      }
+    }
+    double bestx = 1e300;
+    for (int xv : x_opts) {
+      double sum = 0.0;
+      int n = 0;
+      for (const Run &r : runs)
+        if (r.s.x_kernel == xv) sum += r.pass[DNSBOX_PASS_X_NL], ++n;
+      if (n && sum / n < bestx) bestx = sum / n, best.x_kernel = xv;
+    }
+    best.ms_default = runs.empty() ? 0.0 : runs[0].step;   // TMA passes, default x kernel
+    double pass_tmp[DNSBOX_NPASS];
+    rc = trial(ctx, best, uh, scratch, bytes, sv, nsteps, pass_tmp, &best.ms_tuned);
+    // keep the default when the combination measures slower than it
+    if (rc == DNSBOX_OK && best.ms_tuned > best.ms_default) {
+      const double mt = best.ms_default;
+      best = runs[0].s;
+      best.ms_default = best.ms_tuned = mt;
+    }
+    best.tuned = 1;
+  }
+  cudaFree(scratch);
+  const int rc2 = restore(ctx, sv);
+  cudaFree(sv.nold);
+  if (rc != DNSBOX_OK || rc2 != DNSBOX_OK) {
+    apply(ctx, saved_sched);
+    return rc != DNSBOX_OK ? rc : rc2;
+  }
+  apply(ctx, best);
+  {
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    g_cache[key_of(ctx)] = best;
+  }
+  if (out) *out = best;
+  return DNSBOX_OK;
+}

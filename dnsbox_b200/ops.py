@@ -93,6 +93,11 @@ class Box:
         self._lib = lib
 
     # ---------------------------------------------------------------- plumbing
+    @property
+    def handle(self) -> int:
+        """The dnsbox_ctx pointer, the context argument of torch.ops.dnsbox.*."""
+        return int(self._h.value or 0)
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             self._lib.dnsbox_destroy(self._h)
@@ -317,6 +322,34 @@ class Box:
     def set_step_projection(self, on: bool = True):
         """Project and dealias the state after every step (dnsboxband.f90:142-143)."""
         _lib.check(self._lib.dnsbox_set_step_projection(self._h, int(bool(on))))
+
+    # ---------------------------------------------------------- kernel schedule
+    @staticmethod
+    def _sched_dict(sc):
+        return {"tc_kernel": ["tma" if v == 0 else "cp.async" for v in sc.tc_kernel],
+                "x_kernel": {0: "default", 1: "block", 2: "warp"}[sc.x_kernel], "tuned": bool(sc.tuned),
+                "ms_default": sc.ms_default, "ms_tuned": sc.ms_tuned}
+
+    def schedule(self) -> dict:
+        sc = _lib.Schedule()
+        _lib.check(self._lib.dnsbox_get_schedule(self._h, ctypes.byref(sc)))
+        return self._sched_dict(sc)
+
+    def set_schedule(self, tc_kernel=(0, 0, 0), x_kernel=0):
+        sc = _lib.Schedule()
+        for i in range(3):
+            sc.tc_kernel[i] = int(tc_kernel[i])
+        sc.x_kernel = int(x_kernel)
+        _lib.check(self._lib.dnsbox_set_schedule(self._h, ctypes.byref(sc)))
+
+    def autotune(self, uh: torch.Tensor, nsteps: int = 4) -> dict:
+        """Times the candidate kernels of every pass on a copy of uh and keeps
+        the fastest (cached for this device and shape)."""
+        self._check_state(uh)
+        self._sync_stream()
+        sc = _lib.Schedule()
+        _lib.check(self._lib.dnsbox_autotune(self._h, _ptr(uh), int(nsteps), ctypes.byref(sc)))
+        return self._sched_dict(sc)
 
     def implicit_iterations(self) -> int:
         """Fixed-point iterations of the last semi-implicit step."""

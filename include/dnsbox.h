@@ -297,6 +297,29 @@ int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *states_dev, int
 int dnsbox_ensemble_run(dnsbox_ensemble *ens, int nsteps);
 int dnsbox_ensemble_destroy(dnsbox_ensemble *ens);
 
+/* ---- kernel schedule and its autotuner ---------------------------------------
+ * No reference counterpart as code: the reference leaves transform planning to
+ * p3dfft / FFTW (variables.f90:154).  The schedule picks, per tensor-core
+ * strided pass of the right-hand side, the TMA-staged or the cp.async-fed
+ * kernel, and for the fused x pass the block or the warp kernel. */
+typedef struct dnsbox_schedule {
+  int32_t tc_kernel[3];   /* passes A (inverse z), B (inverse y), D (forward y): 0 TMA-staged, 1 cp.async-fed */
+  int32_t x_kernel;       /* fused x pass: 0 default for the size, 1 block kernel, 2 warp kernel */
+  int32_t tuned;          /* 1 when chosen by dnsbox_autotune */
+  int32_t reserved;
+  double ms_default;      /* step time of the default schedule in the tuning run (ms) */
+  double ms_tuned;        /* step time of the chosen schedule (ms) */
+} dnsbox_schedule;
+int dnsbox_get_schedule(const dnsbox_ctx *ctx, dnsbox_schedule *out);
+int dnsbox_set_schedule(dnsbox_ctx *ctx, const dnsbox_schedule *s);
+/* Times every candidate kernel of every pass on nsteps steps of a copy of the
+ * state (uhat3_dev is not modified; the context's clock, dt and history are
+ * restored; the pass-timing counters are reset), keeps the fastest per pass
+ * (never a schedule slower than the default as measured), and caches the
+ * choice per device and shape: contexts created later with the same device,
+ * precision, grid and box count start with it.  out may be NULL. */
+int dnsbox_autotune(dnsbox_ctx *ctx, const void *uhat3_dev, int nsteps, dnsbox_schedule *out);
+
 /* ---- measurement ------------------------------------------------------------
  * No reference counterpart (the reference times nothing; Makefile:3 passes
  * -DMEASURE to p3dfft only).  When enabled, CUDA events are recorded on the

@@ -68,3 +68,16 @@ def test_struct_layouts_match_c(tmp_path):
     assert int(out[1]) == ctypes.sizeof(_lib.Diag)
     assert int(out[2]) == _lib.Params.nu.offset
     assert int(out[3]) == _lib.Diag.nonfinite.offset
+
+
+def test_torch_operator_library_registers():
+    """torch.ops.dnsbox.* (csrc/torch_ops.cpp) loads without a GPU and declares
+    the operators with their schemas."""
+    from dnsbox_b200 import torch_ops
+    if not os.path.exists(torch_ops.OUT):
+        pytest.skip("libdnsbox_torch.so not built")
+    ops = torch_ops.load()
+    names = ["rhs_nonlinear", "rhs_nonlinear_vjp", "step_", "residual", "residual_grad", "c2r", "r2c"]
+    for n in names:
+        assert hasattr(ops, n)
+    assert "Tensor(a!)" in str(ops.step_.default._schema)
