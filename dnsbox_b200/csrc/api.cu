@@ -665,6 +665,7 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
   x.NY = reinterpret_cast<C *>(wfield(c->W1, c, 1));
   x.NZ = reinterpret_cast<C *>(wfield(c->W1, c, 2));
   x.pin = x.pout = c->wp;
+  x.status = c->tc_status;
   x.tw = reinterpret_cast<const C *>(c->tw[0]);
   x.st = c->st;
   x.lines_per_box = p.ny * p.nz;
@@ -890,12 +891,13 @@ int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> 
 // flag to the next such call or to dnsbox_sync.
 int tc_check(dnsbox_ctx *c) {
   int *flag = reinterpret_cast<int *>(c->hstage + 63);
-  if (c->tc) CK(cudaMemcpyAsync(flag, c->tc_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  *flag = 0;
+  if (c->tc_status) CK(cudaMemcpyAsync(flag, c->tc_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (c->tc && *flag) {
+  if (*flag) {
     CK(cudaMemsetAsync(c->tc_status, 0, sizeof(int), c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    return set_err(DNSBOX_ERR_TIMEOUT, "tensor-core DFT pass: MMA completion wait gave up");
+    return set_err(DNSBOX_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core MMA or staged copy)");
   }
   return DNSBOX_OK;
 }
@@ -1199,6 +1201,9 @@ extern "C" int dnsbox_create(const dnsbox_params *p, dnsbox_ctx **out) {
   if (p->precision == DNSBOX_TC_SPLIT) {
     c->tc = 1;
     if ((rc = alloc_dft64(c))) return fail(rc);
+  } else {   // the status flag of bounded device waits (the staged x pass)
+    if ((e = cudaMalloc(&c->tc_status, sizeof(int))) != cudaSuccess || (e = cudaMemset(c->tc_status, 0, sizeof(int))) != cudaSuccess)
+      return fail(set_err(DNSBOX_ERR_OOM, "device allocation failed: %s", cudaGetErrorString(e)));
   }
   // pruning rule per axis, derived from the dealiasing mask and checked against it
   {
@@ -1876,6 +1881,11 @@ struct dnsbox_ensemble {
   cudaEvent_t in = nullptr, out = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // capture: one branch stream per context, forked from and joined into `own`,
+  // so that the graph runs the contexts' steps as independent branches
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t fork = nullptr;
 };
 
 static int step_any(dnsbox_ctx *c, void *u) {
@@ -1889,6 +1899,11 @@ static void ensemble_free(dnsbox_ensemble *e) {
   if (e->graph) cudaGraphDestroy(e->graph);
   if (e->in) cudaEventDestroy(e->in);
   if (e->out) cudaEventDestroy(e->out);
+  if (e->fork) cudaEventDestroy(e->fork);
+  for (cudaEvent_t j : e->joins)
+    if (j) cudaEventDestroy(j);
+  for (cudaStream_t b : e->branch)
+    if (b) cudaStreamDestroy(b);
   if (e->own) cudaStreamDestroy(e->own);
   for (auto *c : e->ctxs) c->stream = e->user;
   delete e;
@@ -1917,6 +1932,13 @@ extern "C" int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *stat
   if ((err = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking)) != cudaSuccess) return fail(err, "stream");
   if ((err = cudaEventCreateWithFlags(&e->in, cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
   if ((err = cudaEventCreateWithFlags(&e->out, cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
+  if ((err = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
+  e->branch.assign(n, nullptr);
+  e->joins.assign(n, nullptr);
+  for (int i = 0; i < n; ++i) {
+    if ((err = cudaStreamCreateWithFlags(&e->branch[i], cudaStreamNonBlocking)) != cudaSuccess) return fail(err, "stream");
+    if ((err = cudaEventCreateWithFlags(&e->joins[i], cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
+  }
   for (auto *c : e->ctxs) {
     c->stream = e->user;
     c->prune_now = 0;   // the captured step uses the full passes (no per-call state check inside a graph)
@@ -1937,7 +1959,15 @@ extern "C" int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *stat
   if ((err = cudaStreamBeginCapture(e->own, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return fail(err, "cudaStreamBeginCapture");
   int rc = DNSBOX_OK;
-  for (int i = 0; i < n && rc == DNSBOX_OK; ++i) rc = step_any(e->ctxs[i], e->states[i]);
+  cudaError_t cerr = cudaEventRecord(e->fork, e->own);
+  for (int i = 0; i < n && rc == DNSBOX_OK && cerr == cudaSuccess; ++i) {
+    if ((cerr = cudaStreamWaitEvent(e->branch[i], e->fork, 0)) != cudaSuccess) break;
+    e->ctxs[i]->stream = e->branch[i];
+    rc = step_any(e->ctxs[i], e->states[i]);
+    if (rc == DNSBOX_OK && (cerr = cudaEventRecord(e->joins[i], e->branch[i])) == cudaSuccess)
+      cerr = cudaStreamWaitEvent(e->own, e->joins[i], 0);
+  }
+  if (rc == DNSBOX_OK && cerr != cudaSuccess) rc = set_err(DNSBOX_ERR_CUDA, "ensemble capture: %s", cudaGetErrorString(cerr));
   err = cudaStreamEndCapture(e->own, &e->graph);
   for (auto *c : e->ctxs) c->host_step -= 1;   // the captured step has not run
   if (rc != DNSBOX_OK) {

@@ -225,6 +225,7 @@ template <typename T> struct XlineNLArgs {
   int lines_per_box;                   // ny * nz
   int kxa;                             // pruning: only kx < kxa and kx = N/2 are read and written (0: all)
   int pin, pout;                       // row pitch (complex elements) of the inputs / outputs; 0: nxh
+  int *status;                         // set to 1 when a bounded wait of a staged kernel gives up (or null)
   double alpha_x;
   double s;                            // scalemodes
 };
@@ -424,64 +425,24 @@ template <typename T, int N> struct XlineWarp {
   using Plan = typename std::conditional<N == 256, FftPlan<256>, WarpPlan<N>>::type;
 };
 
+// Second half of the warp-granular fused x pass for one line pair (la, lb):
+// the inverse transforms are in the warp's tile s (column-major, skewed);
+// (omega x u) * s, the three forward transforms, the unpacking into the
+// output half lines and the CFL maxima of the pair.
 template <typename T, int N>
-__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
-    k_xline_nl_w(const __grid_constant__ XlineNLArgs<T> a) {
+__device__ __forceinline__ void xline_w_tail(typename CT<T>::type *s, const XlineNLArgs<T> &a, long long la,
+                                             long long lb, int lane, long long pout) {
   using C = typename CT<T>::type;
   using PL = typename XlineWarp<T, N>::Plan;
   using EN = FftEndsP<PL>;
   using AD = AddrSkew<PL::R[0]>;
   constexpr int E = PL::E;
-  constexpr int P = N / E;                // threads per sequence
-  constexpr int SPW = 32 / P;             // sequences a warp transforms at once
+  constexpr int P = N / E;
+  constexpr int SPW = 32 / P;
   constexpr int H = N / 2 + 1;
-  constexpr int LDC = N + N / PL::R[0];   // column length with the skew
-  constexpr int WPB = XlineWarp<T, N>::wpb;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C *s = reinterpret_cast<C *>(smem_raw) + (size_t)warp * 6 * LDC;
-  const long long la = 2 * ((long long)blockIdx.x * WPB + warp), lb = la + 1;
-  if (la >= a.nlines) return;
+  constexpr int LDC = N + N / PL::R[0];
+  const int p = lane % P, h = lane / P;
   const T sc = T(a.s);
-  const C *f1s[6] = {a.U, a.U, a.W, a.OX, a.OX, a.OZ};
-  const C *f2s[6] = {a.V, a.V, a.W, a.OY, a.OY, a.OZ};
-  const long long l1s[6] = {la, lb, la, la, lb, la};
-  const long long l2s[6] = {la, lb, lb, la, lb, lb};
-  const int p = lane % P, h = lane / P;   // position in the sequence, sequence slot
-  const long long pin = a.pin ? a.pin : a.nxh, pout = a.pout ? a.pout : a.nxh;
-  // inverse transforms: round r transforms sequences SPW r + h; the loads of
-  // the next round are issued before this round's transform
-  C x1[E], x2[E];
-#pragma unroll
-  for (int i = 0; i < E; ++i) {
-    const int n = EN::in_row(p, i);
-    const int kk = n <= N / 2 ? n : N - n;
-    const bool kp = xkeep(a.kxa, kk, N);
-    x1[i] = kp ? f1s[h][l1s[h] * pin + kk] : mkc<C>(0, 0);
-    x2[i] = kp ? f2s[h][l2s[h] * pin + kk] : mkc<C>(0, 0);
-  }
-#pragma unroll 1
-  for (int r = 0; r < 6 / SPW; ++r) {
-    const int q = SPW * r + h;
-    C v[E];
-#pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = pack_pair<C, N>(EN::in_row(p, i), x1[i], x2[i]);
-    if (r + 1 < 6 / SPW) {
-      const int qn = q + SPW;
-      const C *g1 = f1s[qn] + l1s[qn] * pin, *g2 = f2s[qn] + l2s[qn] * pin;
-#pragma unroll
-      for (int i = 0; i < E; ++i) {
-        const int n = EN::in_row(p, i);
-        const int kk = n <= N / 2 ? n : N - n;
-        const bool kp = xkeep(a.kxa, kk, N);
-        x1[i] = kp ? g1[kk] : mkc<C>(0, 0);
-        x2[i] = kp ? g2[kk] : mkc<C>(0, 0);
-      }
-    }
-    fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, p, true, a.tw);
-#pragma unroll
-    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
-  }
   __syncwarp();
   // (omega x u) * s, written back as (px_a,py_a) (pz_a,pz_b) (px_b,py_b) in
   // columns 0..2; the CFL maxima are taken in T (exact) and widened at the end
@@ -573,6 +534,65 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
     atomic_max_nonneg(um + 1, (double)m1 * a.s);
     atomic_max_nonneg(um + 2, (double)m2 * a.s);
   }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
+    k_xline_nl_w(const __grid_constant__ XlineNLArgs<T> a) {
+  using C = typename CT<T>::type;
+  using PL = typename XlineWarp<T, N>::Plan;
+  using EN = FftEndsP<PL>;
+  using AD = AddrSkew<PL::R[0]>;
+  constexpr int E = PL::E;
+  constexpr int P = N / E;                // threads per sequence
+  constexpr int SPW = 32 / P;             // sequences a warp transforms at once
+  constexpr int LDC = N + N / PL::R[0];   // column length with the skew
+  constexpr int WPB = XlineWarp<T, N>::wpb;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C *s = reinterpret_cast<C *>(smem_raw) + (size_t)warp * 6 * LDC;
+  const long long la = 2 * ((long long)blockIdx.x * WPB + warp), lb = la + 1;
+  if (la >= a.nlines) return;
+  const C *f1s[6] = {a.U, a.U, a.W, a.OX, a.OX, a.OZ};
+  const C *f2s[6] = {a.V, a.V, a.W, a.OY, a.OY, a.OZ};
+  const long long l1s[6] = {la, lb, la, la, lb, la};
+  const long long l2s[6] = {la, lb, lb, la, lb, lb};
+  const int p = lane % P, h = lane / P;   // position in the sequence, sequence slot
+  const long long pin = a.pin ? a.pin : a.nxh, pout = a.pout ? a.pout : a.nxh;
+  // inverse transforms: round r transforms sequences SPW r + h; the loads of
+  // the next round are issued before this round's transform
+  C x1[E], x2[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int n = EN::in_row(p, i);
+    const int kk = n <= N / 2 ? n : N - n;
+    const bool kp = xkeep(a.kxa, kk, N);
+    x1[i] = kp ? f1s[h][l1s[h] * pin + kk] : mkc<C>(0, 0);
+    x2[i] = kp ? f2s[h][l2s[h] * pin + kk] : mkc<C>(0, 0);
+  }
+#pragma unroll 1
+  for (int r = 0; r < 6 / SPW; ++r) {
+    const int q = SPW * r + h;
+    C v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = pack_pair<C, N>(EN::in_row(p, i), x1[i], x2[i]);
+    if (r + 1 < 6 / SPW) {
+      const int qn = q + SPW;
+      const C *g1 = f1s[qn] + l1s[qn] * pin, *g2 = f2s[qn] + l2s[qn] * pin;
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const int n = EN::in_row(p, i);
+        const int kk = n <= N / 2 ? n : N - n;
+        const bool kp = xkeep(a.kxa, kk, N);
+        x1[i] = kp ? g1[kk] : mkc<C>(0, 0);
+        x2[i] = kp ? g2[kk] : mkc<C>(0, 0);
+      }
+    }
+    fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, p, true, a.tw);
+#pragma unroll
+    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
+  }
+  xline_w_tail<T, N>(s, a, la, lb, lane, pout);
 }
 
 // Plain x-line transforms of nf fields (blockIdx.y = field).

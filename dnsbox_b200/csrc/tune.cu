@@ -126,7 +126,7 @@ extern "C" int dnsbox_set_schedule(dnsbox_ctx *ctx, const dnsbox_schedule *s) {
   if (!ctx || !s) return set_err(DNSBOX_ERR_ARG, "null argument");
   for (int i = 0; i < 3; ++i)
     if (s->tc_kernel[i] != 0 && s->tc_kernel[i] != 1) return set_err(DNSBOX_ERR_ARG, "tc_kernel must be 0 or 1");
-  if (s->x_kernel < 0 || s->x_kernel > 2) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0, 1 or 2");
+  if (s->x_kernel < 0 || s->x_kernel > 3) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0 .. 3");
   apply(ctx, *s);
   return DNSBOX_OK;
 }
@@ -147,7 +147,7 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
     if (ctx->tma_on && (tz || ty)) tc_opts.push_back(1);
   }
   std::vector<int> x_opts = {0};
-  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1};
+  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1, 3};
   const dnsbox_schedule saved_sched = current(ctx);
   Saved sv;
   RET(save(ctx, sv));

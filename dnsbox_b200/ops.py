@@ -327,7 +327,7 @@ class Box:
     @staticmethod
     def _sched_dict(sc):
         return {"tc_kernel": ["tma" if v == 0 else "cp.async" for v in sc.tc_kernel],
-                "x_kernel": {0: "default", 1: "block", 2: "warp"}[sc.x_kernel], "tuned": bool(sc.tuned),
+                "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-bulk"}[sc.x_kernel], "tuned": bool(sc.tuned),
                 "ms_default": sc.ms_default, "ms_tuned": sc.ms_tuned}
 
     def schedule(self) -> dict:

@@ -290,8 +290,10 @@ int dnsbox_set_batch_nu(dnsbox_ctx *ctx, const double *nu_host);
  * major); the device keeps the last 1024 steps. */
 int dnsbox_diag_read(dnsbox_ctx *ctx, int nrecent, dnsbox_diag *diag_host);
 /* Captures one step of every (context, state) pair into a CUDA graph on the
- * first context's stream (all contexts are switched to it).  Every state is
- * first advanced by one step eagerly, so the captured step is a steady one. */
+ * first context's stream (all contexts are switched to it), each context's
+ * step an independent branch of the graph (the branches may run
+ * concurrently).  Every state is first advanced by one step eagerly, so the
+ * captured step is a steady one. */
 int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *states_dev, int n, dnsbox_ensemble **out);
 /* Replays the captured step nsteps times (asynchronous). */
 int dnsbox_ensemble_run(dnsbox_ensemble *ens, int nsteps);
@@ -304,7 +306,8 @@ int dnsbox_ensemble_destroy(dnsbox_ensemble *ens);
  * kernel, and for the fused x pass the block or the warp kernel. */
 typedef struct dnsbox_schedule {
   int32_t tc_kernel[3];   /* passes A (inverse z), B (inverse y), D (forward y): 0 TMA-staged, 1 cp.async-fed */
-  int32_t x_kernel;       /* fused x pass: 0 default for the size, 1 block kernel, 2 warp kernel */
+  int32_t x_kernel;       /* fused x pass: 0 default for the size, 1 block kernel, 2 warp kernel,
+                             3 warp kernel with bulk-copied (TMA) input lines */
   int32_t tuned;          /* 1 when chosen by dnsbox_autotune */
   int32_t reserved;
   double ms_default;      /* step time of the default schedule in the tuning run (ms) */
