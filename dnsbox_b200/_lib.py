@@ -57,8 +57,8 @@ class Diag(ctypes.Structure):
 class Schedule(ctypes.Structure):
     """``dnsbox_schedule``: the right-hand side's kernel choices."""
     _fields_ = [
-        ("tc_kernel", ctypes.c_int32 * 3), ("x_kernel", ctypes.c_int32), ("tuned", ctypes.c_int32),
-        ("reserved", ctypes.c_int32), ("ms_default", ctypes.c_double), ("ms_tuned", ctypes.c_double),
+        ("tc_kernel", ctypes.c_int32 * 4), ("x_kernel", ctypes.c_int32), ("tuned", ctypes.c_int32),
+        ("ms_default", ctypes.c_double), ("ms_tuned", ctypes.c_double),
     ]
 
 

@@ -709,7 +709,7 @@ static int run_rhs(dnsbox_ctx *c, const void *uin, int mode, void *out, void *st
     z.koth = c->keep[1];
     z.krout = c->keep[2];
   }
-  RET(run_strided<T>(c, 2, false, z, DNSBOX_PASS_Z_FWD, false));
+  RET(run_strided<T>(c, 2, false, z, DNSBOX_PASS_Z_FWD, c->sched_tc[3] != 0, c->W2, 3));
   // pass E2: spectral finish, one warp per (kz, ky) row
   FinishArgs<T> e = finish_base<T>(c);
   e.n3 = reinterpret_cast<const C *>(c->W2);
@@ -762,26 +762,29 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // axis of length n (all rows when k.a = 0): [0, a), the Nyquist row n/2 and
 // (n - a, n), each range rounded out to whole boxes.  Returns the count, or
 // the full cover when the rounded ranges would overlap.
-static int tma_row_boxes(const AxisKeep &k, int n, unsigned short *rows) {
+static int tma_row_boxes(const AxisKeep &k, int n, int br, unsigned short *rows) {
   int nb = 0;
   if (k.a > 0) {
-    const int lo_end = (k.a + 7) / 8 * 8;
+    const int lo_end = (k.a + br - 1) / br * br;
     int hi_start = n;
-    while (hi_start - 8 >= 0 && hi_start > n - k.a + 1) hi_start -= 8;
+    while (hi_start - br >= 0 && hi_start > n - k.a + 1) hi_start -= br;
     const int nq = n / 2;
-    if (lo_end <= nq && nq + 8 <= hi_start && nq % 8 == 0) {
-      for (int r = 0; r < lo_end; r += 8) rows[nb++] = (unsigned short)r;
+    if (lo_end <= nq && nq + br <= hi_start && nq % br == 0) {
+      for (int r = 0; r < lo_end; r += br) rows[nb++] = (unsigned short)r;
       rows[nb++] = (unsigned short)nq;
-      for (int r = hi_start; r < n; r += 8) rows[nb++] = (unsigned short)r;
+      for (int r = hi_start; r < n; r += br) rows[nb++] = (unsigned short)r;
       return nb;
     }
   }
-  for (int r = 0; r < n; r += 8) rows[nb++] = (unsigned short)r;
+  for (int r = 0; r < n; r += br) rows[nb++] = (unsigned short)r;
   return nb;
 }
 
 int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> &a, const void *base, int nslots,
                     int kind) {
+  // a z pass reads the state (pitch nxh, components fstride apart) unless its
+  // inputs live in the padded workspace (W2: the forward z pass)
+  const bool ws_z = axis == 2 && base != nullptr && (base == c->W1 || base == c->W2);
   const dnsbox_params &p = c->p;
   const int n = axis == 2 ? p.nz : p.ny;
   const int width = 4096 / n;   // TmaPlan<n>::TCW
@@ -809,7 +812,7 @@ int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> 
   t.njobs_d.init((unsigned)a.njobs);
   t.ntxd.init((unsigned)ntx);
   // jobs: slot coordinates of the inputs within `base`
-  const size_t slot_bytes = (axis == 2 ? c->fstride : c->wstride) * sizeof(float2);
+  const size_t slot_bytes = (axis == 2 && !ws_z ? c->fstride : c->wstride) * sizeof(float2);
   auto slot_of = [&](const void *ptr) -> int {
     const long long d = reinterpret_cast<const char *>(ptr) - reinterpret_cast<const char *>(base);
     if (d < 0 || d % (long long)slot_bytes || d / (long long)slot_bytes >= nslots) return -2;
@@ -842,29 +845,32 @@ int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> 
   t.bso = out_bstride(a);
   if ((t.rso | t.oso | t.bso) & 1) return set_err(DNSBOX_ERR_STATE, "TMA pass: output rows must be 16-byte aligned");
   t.plane = axis == 2;
-  t.in_pitch = c->nxh;
+  t.in_pitch = ws_z ? c->wp : c->nxh;
   t.ncols = a.ncols;
   t.nx = a.nx;
   t.n_other = a.n_other;
   t.alpha_row = (float)a.alpha_row;
   t.alpha_x = (float)a.alpha_x;
   t.alpha_other = (float)a.alpha_other;
-  t.nbox = tma_row_boxes(a.krin, n, t.box_row);
+  t.box_rows = c->tma_box_rows;
+  t.nbox = tma_row_boxes(a.krin, n, t.box_rows, t.box_row);
   // the input tensor map
   const int spc = width + 2;
   cuuint64_t dims[5], strides[4];
-  const cuuint32_t box[5] = {(cuuint32_t)(2 * spc), 8, 1, 1, 1}, estr[5] = {1, 1, 1, 1, 1};
-  if (axis == 2) {   // state: (plane floats, z, box, component, 1)
-    const unsigned long long plane = (unsigned long long)p.ny * c->nxh;
+  const cuuint32_t box[5] = {(cuuint32_t)(2 * spc), (cuuint32_t)t.box_rows, 1, 1, 1}, estr[5] = {1, 1, 1, 1, 1};
+  if (axis == 2) {   // (plane floats, z, box, slot, 1): the state, or the padded workspace
+    const unsigned long long pitch = ws_z ? c->wp : c->nxh;
+    const unsigned long long plane = (unsigned long long)p.ny * pitch;
+    const unsigned long long boxs = plane * p.nz, slots = ws_z ? c->wstride : c->fstride;
     dims[0] = 2 * plane;
     dims[1] = (cuuint64_t)p.nz;
     dims[2] = (cuuint64_t)nbatch;
     dims[3] = (cuuint64_t)nslots;
     dims[4] = 1;
     strides[0] = plane * 8;
-    strides[1] = (cuuint64_t)c->nh * 8;
-    strides[2] = (cuuint64_t)c->fstride * 8;
-    strides[3] = (cuuint64_t)c->fstride * 8 * nslots;
+    strides[1] = boxs * 8;
+    strides[2] = slots * 8;
+    strides[3] = slots * 8 * nslots;
   } else {           // padded workspace: (row floats, y, z, box, slot)
     dims[0] = 2ull * c->nxh;
     dims[1] = (cuuint64_t)p.ny;
@@ -1114,6 +1120,10 @@ static int alloc_dft64(dnsbox_ctx *c) {
   // tensor-core kernel of the standalone transforms (for comparisons)
   const char *kern = getenv("DNSBOX_TC_KERNEL");
   c->tma_on = !(kern && strcmp(kern, "legacy") == 0);
+  // rows per TMA box of the staged tiles (8, 16, 32 or 64; DNSBOX_TMA_BOX_ROWS)
+  const char *br = getenv("DNSBOX_TMA_BOX_ROWS");
+  const int brv = br ? atoi(br) : 32;
+  c->tma_box_rows = (brv == 8 || brv == 16 || brv == 32 || brv == 64) ? brv : 32;
   return DNSBOX_OK;
 }
 

@@ -99,10 +99,12 @@ struct dnsbox_ctx {
   int tc_ctas = 0;                       // persistent grid of the tensor-core passes
   int nsm = 0;                           // streaming multiprocessors of the device
   int tma_on = 0;                        // the right-hand side uses the TMA-staged tensor-core passes
+  int tma_box_rows = 32;                 // rows per TMA box of their staged tiles
   // kernel schedule of the right-hand side (chosen by dnsbox_autotune, or the
-  // defaults): per tensor-core pass A, B, D 0 = TMA-staged, 1 = legacy
-  // cp.async-fed kernel; x pass 0 = default, 1 = block, 2 = warp kernel
-  int sched_tc[3] = {0, 0, 0};
+  // defaults): passes A, B, D 0 = TMA-staged tensor-core kernel, 1 = the
+  // cp.async-fed one; pass E1 0 = SIMT, 1 = TMA-staged tensor-core kernel;
+  // x pass 0 = default, 1 = block, 2 = warp, 3 = warp with bulk-staged lines
+  int sched_tc[4] = {0, 0, 0, 0};
   int sched_x = 0;
   char *adj = nullptr;                   // adjoint arena
   size_t adj_bytes = 0;
@@ -360,8 +362,11 @@ static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int 
                        bool allow_tc = true, const void *tma_base = nullptr, int tma_slots = 0) {
   const int n = axis == 2 ? c->p.nz : c->p.ny;
   if constexpr (sizeof(T) == 4) {
-    const int si = kind == DNSBOX_PASS_Z_INV ? 0 : kind == DNSBOX_PASS_Y_INV ? 1 : kind == DNSBOX_PASS_Y_FWD ? 2 : -1;
-    if (allow_tc && tma_base && c->tc && c->tma_on && Ops<T>::has_tma(n) && si >= 0 && c->sched_tc[si] == 0)
+    const int si = kind == DNSBOX_PASS_Z_INV ? 0 : kind == DNSBOX_PASS_Y_INV ? 1 : kind == DNSBOX_PASS_Y_FWD ? 2
+                 : kind == DNSBOX_PASS_Z_FWD ? 3 : -1;
+    // passes A, B, D: TMA unless scheduled on the cp.async kernel; E1: TMA when scheduled
+    const bool want = si >= 0 && (si == 3 ? c->sched_tc[3] == 1 : c->sched_tc[si] == 0);
+    if (allow_tc && tma_base && c->tc && c->tma_on && Ops<T>::has_tma(n) && want)
       return run_strided_tma(c, axis, inv, a, tma_base, tma_slots, kind);
   }
   const bool tc = allow_tc && c->tc && Ops<T>::has_tc(n);

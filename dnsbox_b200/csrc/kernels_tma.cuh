@@ -58,7 +58,7 @@ template <int N> struct TmaPlan {
   static constexpr int SMEM = 1024 + 2 * A_PART + 4 * B_PART + 2 * STAGE;
 };
 
-constexpr int kTmaMaxBoxes = 64;   // 8-row boxes per staged tile (N / 8 at most)
+constexpr int kTmaMaxBoxes = 64;   // boxes per staged tile (N / 8 at most)
 
 struct TmaJob {
   const float2 *in1, *in2;   // field pointers (the merged Nyquist column is read through them)
@@ -84,7 +84,8 @@ struct TmaArgs {
   int two;                   // 1: a job has two inputs (one staging buffer per input)
   int ncols, nx, n_other;
   float alpha_row, alpha_x, alpha_other;
-  int nbox;                  // 8-row boxes per staged input tile
+  int nbox;                  // boxes per staged input tile
+  int box_rows;              // rows per box (8, 16, 32 or 64; the tensor map's box height)
   unsigned short box_row[kTmaMaxBoxes];
   AxisKeep kcol, koth, krin, krout;
   int ntx_lo, nyq_tile;
@@ -195,24 +196,25 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, 1)
   const int NST = a.two ? 1 : 2;      // staging buffers in rotation
   const unsigned nb = gridDim.x;
   const int my_n = (int)blockIdx.x < a.total ? (a.total - (int)blockIdx.x + (int)nb - 1) / (int)nb : 0;
-  constexpr uint32_t kBoxBytes = 8 * SPC * 8;
+  const uint32_t box_bytes = (uint32_t)a.box_rows * SPC * 8;
 
-  // tile i of this CTA: loads into staging buffer s (thread 0)
+  // tile i of this CTA: loads into staging buffer s, issued by the lanes of
+  // warp 0 (one box each, after lane 0 has armed the barrier)
   auto issue_loads = [&](int i, int s) {
     const TmaItem it = tma_item<TCW>(a, blockIdx.x + (unsigned)i * nb);
     const TmaJob &J = a.job[it.job];
     const int nin = J.slot2 >= 0 ? 2 : 1;
-    tma::expect_tx(&full[s], (uint32_t)(nin * a.nbox) * kBoxBytes);
+    if (lane == 0) tma::expect_tx(&full[s], (uint32_t)(nin * a.nbox) * box_bytes);
+    __syncwarp();
     const int off = it.other * a.in_pitch + it.kx0;   // plane mode: column index within the plane
     const int x = a.plane ? 2 * (off - (off & 1)) : 2 * it.kx0;   // 16-byte aligned start
-    for (int q = 0; q < nin; ++q) {
+    for (int k = lane; k < nin * a.nbox; k += 32) {
+      const int q = k >= a.nbox ? 1 : 0, b = k - q * a.nbox;
       const int slot = q ? J.slot2 : J.slot1;
-      unsigned char *dst = stg + (size_t)(s + q) * PL::STAGE;
-      for (int b = 0; b < a.nbox; ++b) {
-        const int r0 = a.box_row[b];
-        if (a.plane) tma::load5(dst + (size_t)r0 * SPC * 8, &a.map, x, r0, it.box, slot, 0, &full[s]);
-        else tma::load5(dst + (size_t)r0 * SPC * 8, &a.map, x, r0, it.other, it.box, slot, &full[s]);
-      }
+      unsigned char *dst = stg + (size_t)(s + q) * PL::STAGE + (size_t)a.box_row[b] * SPC * 8;
+      const int r0 = a.box_row[b];
+      if (a.plane) tma::load5(dst, &a.map, x, r0, it.box, slot, 0, &full[s]);
+      else tma::load5(dst, &a.map, x, r0, it.other, it.box, slot, &full[s]);
     }
   };
 
@@ -223,7 +225,7 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, 1)
   const int n1 = 8 * (warp >> 1) + (jq & 1) * D1 + 4 * (jq >> 1) + (warp & 1) * (D1 == 1 ? 2 : 1);
   const int c0 = cg * G;
 
-  if (t == 0)
+  if (warp == 0)
     for (int i = 0; i < NST && i < my_n; ++i) issue_loads(i, i);
   // Tile k of this CTA uses staging buffer k % NST with mbarrier parity
   // (k / NST) & 1 and accumulator k & 1 with parity (k >> 1) & 1.  Thread 0
@@ -329,12 +331,14 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, 1)
       tc::fence_proxy_async();
       tc::fence_before_sync();
       __syncthreads();   // #2: operands written, staging buffer s consumed
-      if (t == 0) {
+      if (warp == 0) {
         tc::fence_after_sync();
         if (loads_issued < my_n) {
           issue_loads(loads_issued, NST == 2 ? (loads_issued & 1) : 0);
           ++loads_issued;
         }
+      }
+      if (t == 0) {
         // 3 x 4 MMAs (K = 16 each) into accumulator bb: Al Bh, Ah Bl, then Ah Bh
         constexpr uint32_t lboA = (128 / 8) * 128, sboA = 128, lboB = 8192, sboB = 1024;
 #pragma unroll

@@ -6,8 +6,9 @@
 // transforms are the library's own kernels, and the choices that measured
 // differently across sizes are made by timing: for each of the tensor-core
 // strided passes (A inverse z, B inverse y, D forward y) the TMA-staged or
-// the cp.async-fed kernel, and for the fused x pass the block or the warp
-// kernel.  Each uniform candidate schedule advances a copy of the caller's
+// the cp.async-fed kernel, for the forward z pass (E1) the SIMT or the
+// TMA-staged tensor-core kernel, and for the fused x pass the block, the warp
+// or the bulk-staged warp kernel.  Each uniform candidate schedule advances a copy of the caller's
 // state for a few steps with pass timing on (CUDA events on the context's
 // stream); every pass keeps its fastest kernel; the chosen schedule is timed
 // once more.  The context's clock, time step and step history are restored,
@@ -31,14 +32,14 @@ Key key_of(const dnsbox_ctx *c) {
 }
 
 void apply(dnsbox_ctx *c, const dnsbox_schedule &s) {
-  for (int i = 0; i < 3; ++i) c->sched_tc[i] = s.tc_kernel[i] ? 1 : 0;
+  for (int i = 0; i < 4; ++i) c->sched_tc[i] = s.tc_kernel[i] ? 1 : 0;
   c->sched_x = s.x_kernel;
 }
 
 dnsbox_schedule current(const dnsbox_ctx *c) {
   dnsbox_schedule s;
   memset(&s, 0, sizeof(s));
-  for (int i = 0; i < 3; ++i) s.tc_kernel[i] = c->sched_tc[i];
+  for (int i = 0; i < 4; ++i) s.tc_kernel[i] = c->sched_tc[i];
   s.x_kernel = c->sched_x;
   return s;
 }
@@ -124,7 +125,7 @@ extern "C" int dnsbox_get_schedule(const dnsbox_ctx *ctx, dnsbox_schedule *out) 
 
 extern "C" int dnsbox_set_schedule(dnsbox_ctx *ctx, const dnsbox_schedule *s) {
   if (!ctx || !s) return set_err(DNSBOX_ERR_ARG, "null argument");
-  for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < 4; ++i)
     if (s->tc_kernel[i] != 0 && s->tc_kernel[i] != 1) return set_err(DNSBOX_ERR_ARG, "tc_kernel must be 0 or 1");
   if (s->x_kernel < 0 || s->x_kernel > 3) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0 .. 3");
   apply(ctx, *s);
@@ -140,11 +141,12 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
   const dnsbox_params &p = ctx->p;
   const bool fp64 = ctx->fp64;
   // candidate kernels
-  std::vector<int> tc_opts = {0};
-  if (ctx->tc && !fp64) {
+  std::vector<int> tc_opts = {0}, e1_opts = {0};
+  if (ctx->tc && !fp64 && ctx->tma_on) {
     const bool tz = Ops<float>::has_tma(p.nz) && Ops<float>::has_tc(p.nz);
     const bool ty = Ops<float>::has_tma(p.ny) && Ops<float>::has_tc(p.ny);
-    if (ctx->tma_on && (tz || ty)) tc_opts.push_back(1);
+    if (tz || ty) tc_opts.push_back(1);
+    if (Ops<float>::has_tma(p.nz)) e1_opts.push_back(1);
   }
   std::vector<int> x_opts = {0};
   if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1, 3};
@@ -162,13 +164,17 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
   std::vector<Run> runs;
   int rc = DNSBOX_OK;
   for (int tcv : tc_opts) {
-    for (int xv : x_opts) {
-      Run r;
-      memset(&r, 0, sizeof(r));
-      for (int i = 0; i < 3; ++i) r.s.tc_kernel[i] = tcv;
-      r.s.x_kernel = xv;
-      if ((rc = trial(ctx, r.s, uh, scratch, bytes, sv, nsteps, r.pass, &r.step)) != DNSBOX_OK) break;
-      runs.push_back(r);
+    for (int ev : e1_opts) {
+      for (int xv : x_opts) {
+        Run r;
+        memset(&r, 0, sizeof(r));
+        for (int i = 0; i < 3; ++i) r.s.tc_kernel[i] = tcv;
+        r.s.tc_kernel[3] = ev;
+        r.s.x_kernel = xv;
+        if ((rc = trial(ctx, r.s, uh, scratch, bytes, sv, nsteps, r.pass, &r.step)) != DNSBOX_OK) break;
+        runs.push_back(r);
+      }
+      if (rc != DNSBOX_OK) break;
     }
     if (rc != DNSBOX_OK) break;
   }
@@ -176,10 +182,10 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
   memset(&best, 0, sizeof(best));
   if (rc == DNSBOX_OK) {
     // per pass: the kernel whose runs took least time on average
-    const int pass_of[3] = {DNSBOX_PASS_Z_INV, DNSBOX_PASS_Y_INV, DNSBOX_PASS_Y_FWD};
-    for (int i = 0; i < 3; ++i) {
+    const int pass_of[4] = {DNSBOX_PASS_Z_INV, DNSBOX_PASS_Y_INV, DNSBOX_PASS_Y_FWD, DNSBOX_PASS_Z_FWD};
+    for (int i = 0; i < 4; ++i) {
       double bestv = 1e300;
-      for (int tcv : tc_opts) {
+      for (int tcv : (i == 3 ? e1_opts : tc_opts)) {
         double sum = 0.0;
         int n = 0;
         for (const Run &r : runs)

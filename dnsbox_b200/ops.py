@@ -326,7 +326,8 @@ class Box:
     # ---------------------------------------------------------- kernel schedule
     @staticmethod
     def _sched_dict(sc):
-        return {"tc_kernel": ["tma" if v == 0 else "cp.async" for v in sc.tc_kernel],
+        return {"tc_kernel": ["tma" if v == 0 else "cp.async" for v in sc.tc_kernel[:3]],
+                "z_fwd_kernel": "tma" if sc.tc_kernel[3] else "simt",
                 "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-bulk"}[sc.x_kernel], "tuned": bool(sc.tuned),
                 "ms_default": sc.ms_default, "ms_tuned": sc.ms_tuned}
 
@@ -335,10 +336,11 @@ class Box:
         _lib.check(self._lib.dnsbox_get_schedule(self._h, ctypes.byref(sc)))
         return self._sched_dict(sc)
 
-    def set_schedule(self, tc_kernel=(0, 0, 0), x_kernel=0):
+    def set_schedule(self, tc_kernel=(0, 0, 0), x_kernel=0, z_fwd_tma=False):
         sc = _lib.Schedule()
         for i in range(3):
             sc.tc_kernel[i] = int(tc_kernel[i])
+        sc.tc_kernel[3] = int(bool(z_fwd_tma))
         sc.x_kernel = int(x_kernel)
         _lib.check(self._lib.dnsbox_set_schedule(self._h, ctypes.byref(sc)))
 

@@ -30,9 +30,10 @@ def test_every_schedule_matches_the_oracle(prec):
     tcs = list(itertools.product((0, 1), repeat=3)) if prec == "tc_split" else [(0, 0, 0)]
     for tc in tcs:
         for xk in (0, 1, 2, 3):
-            b.set_schedule(tc, xk)
-            got, _ = b.rhs_nonlinear(u)
-            assert rel(got.cpu().numpy(), want) < 2e-6, (tc, xk)
+            for zt in ((False, True) if prec == "tc_split" else (False,)):
+                b.set_schedule(tc, xk, zt)
+                got, _ = b.rhs_nonlinear(u)
+                assert rel(got.cpu().numpy(), want) < 2e-6, (tc, xk, zt)
     b.close()
 
 
@@ -56,7 +57,7 @@ def test_autotune_keeps_state_clock_and_caches(prec):
     v = c.from_numpy(ic.random_field(n, seed=3, k0=3.0))
     c.step(v, 2)
     assert c.schedule()["tc_kernel"] == sch["tc_kernel"]   # the cached choice
-    c.set_schedule((0, 0, 0), 0)
+    c.set_schedule((0, 0, 0), 0, False)
     b.step(u, 2)
     c.step(v, 2)
     assert rel(u.to(torch.complex128).cpu().numpy(), v.to(torch.complex128).cpu().numpy()) < (
