@@ -8,7 +8,6 @@
 #include "kernels.cuh"
 #include "kernels_tc.cuh"
 #include "kernels_tma.cuh"
-#include "kernels_xbulk.cuh"
 
 namespace dnsbox {
 
@@ -23,8 +22,7 @@ template <typename T, int N> struct Launcher {
   static cudaError_t strided_tma(const TmaArgs &a, bool inv, const void *adft, int *status, int nctas,
                                  cudaStream_t st);
   static bool has_tma();
-  // variant: 0 the default kernel for N, 1 the block kernel, 2 the warp kernel, 3 the warp kernel with
-  // bulk-staged inputs (2 and 3 where they exist; 3 needs 16-byte aligned rows)
+  // variant: 0 the default kernel for N, 1 the block kernel, 2 the warp kernel (where it exists)
   static cudaError_t xline_nl(const XlineNLArgs<T> &a, int variant, cudaStream_t st);
   static bool has_xline_warp();
   static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);
@@ -139,27 +137,6 @@ template <typename T, int N> bool Launcher<T, N>::has_xline_warp() { return Xlin
 template <typename T, int N>
 cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaStream_t st) {
   using C = typename CT<T>::type;
-  if constexpr (XlineBulk<T, N>::on) {
-    if (variant == 3) {
-      using XB = XlineBulk<T, N>;
-      cudaError_t e;
-      if ((e = set_smem(k_xline_nl_wb<T, N>, XB::SMEM)) != cudaSuccess) return e;
-      static int grid = 0;   // resident blocks on every SM (persistent warps)
-      if (!grid) {
-        int dev = 0, nsm = 0, per = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-        if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_xline_nl_wb<T, N>, 32 * XB::WPB, XB::SMEM)) !=
-            cudaSuccess)
-          return e;
-        grid = nsm * (per > 0 ? per : 1);
-      }
-      const long long pairs = a.nlines / 2;
-      const unsigned nb = (unsigned)((pairs + XB::WPB - 1) / XB::WPB < grid ? (pairs + XB::WPB - 1) / XB::WPB : grid);
-      k_xline_nl_wb<T, N><<<nb, 32 * XB::WPB, XB::SMEM, st>>>(a);
-      return cudaGetLastError();
-    }
-  }
   if constexpr (XlineWarp<T, N>::on) {
     if (variant != 1) {
     // warp-granular kernel: one warp per line pair
