@@ -844,6 +844,7 @@ int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> 
   t.oso = out_otherstride(a);
   t.bso = out_bstride(a);
   if ((t.rso | t.oso | t.bso) & 1) return set_err(DNSBOX_ERR_STATE, "TMA pass: output rows must be 16-byte aligned");
+  if ((long long)n * t.rso >= (1LL << 31)) return set_err(DNSBOX_ERR_SIZE, "TMA pass: 32-bit row offsets");
   t.plane = axis == 2;
   t.in_pitch = ws_z ? c->wp : c->nxh;
   t.ncols = a.ncols;
@@ -887,7 +888,7 @@ int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> 
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_err(DNSBOX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   Prof pr(c, kind);
-  CK(Ops<float>::strided_tma(n, t, inv, c->adft, c->tc_status, c->nsm, c->stream));
+  CK(Ops<float>::strided_tma(n, t, inv, c->adft, c->tc_status, 2 * c->nsm, c->stream));   // two CTAs per SM
   return DNSBOX_OK;
 }
 

@@ -25,17 +25,21 @@
 // and imaginary parts of X sit in different accumulator columns, so each
 // accumulation chain is one 64-term real dot product.
 //
-// Data movement: one thread issues the tile's input loads as TMA boxes of 8
-// rows (only the rows the pass keeps, when pruning) into a staging tile that
-// completes on an mbarrier; the next tile's loads are in flight while the
-// current one is processed (two staging buffers, or one staging buffer per
-// input for two-input jobs).  The B operands are double buffered and written
-// in the MN-major 128-byte-swizzle layout, so the MMAs of one tile run while
-// stage A of the next proceeds, and the accumulators (two 128-column TMEM
-// regions) are drained one tile behind.  One persistent CTA of 512 threads
-// per SM.  Every wait is bounded: a wait that gives up sets the status flag,
-// the copies and MMAs in flight are waited for (again bounded), TMEM is freed
-// and the kernel returns.
+// Data movement: the lanes of warp 0 issue the tile's input loads as TMA
+// boxes (only the rows the pass keeps, when pruning) into a staging tile that
+// completes on an mbarrier; the next tile's loads are issued as soon as the
+// current tile's stage A has read the staging tile, so they land while its
+// DFT, split and MMAs run (a two-input job stages its second input after the
+// first).  Two 256-thread CTAs share an SM, each with its own staging tile, B
+// operand (MN-major 128-byte swizzle) and 128-column TMEM accumulator, so the
+// phases and waits of one overlap the work of the other; a tile's
+// accumulator is drained straight to HBM at the start of the next tile's
+// split, before the next MMAs are issued.  Per-tile column data (half-axis
+// index, wavenumber, unscale factor) is tabulated once in shared memory and
+// the thread's kept-row masks and row offsets once per launch.  Every wait is
+// bounded (one thread polls each barrier): a wait that gives up sets the
+// status flag, the copies and MMAs in flight are waited for (again bounded),
+// TMEM is freed and the kernel returns.
 #pragma once
 
 #include <cuda.h>
@@ -48,14 +52,15 @@ template <int N> struct TmaPlan {
   static constexpr bool on = N == 128 || N == 256 || N == 512;
   static constexpr int N2 = on ? N / 64 : 1;
   static constexpr int TCW = 64 / N2;            // kx columns per tile
-  static constexpr int G = on ? 8 / N2 : 1;      // columns per stage-A item: G * N2 = 8 values a thread
+  static constexpr int G = on ? 8 / N2 : 1;      // columns per stage-A item: G * N2 = 8 values
   static constexpr int SPC = TCW + 2;            // staging row pitch (complex): the tile and a one-column shift
-  static constexpr int STAGE = N * SPC * 8;      // bytes of one staged input tile
-  static constexpr int THREADS = 512;            // 64 n1 x 8 column groups
+  static constexpr int STAGE = N * SPC * 8;      // bytes of the staged input tile
+  static constexpr int THREADS = 256;            // 8 warps; 512 stage-A items (64 n1 x 8 column groups), 2 each
+  static constexpr int CTAS_PER_SM = 2;
   static constexpr int A_PART = 128 * 64 * 2;    // f16 128 x 64 operand
   static constexpr int B_PART = 64 * 128 * 2;    // f16 64 (K) x 128 (MN) operand
-  static constexpr int TMEM_COLS = 256;          // two 128-column accumulators
-  static constexpr int SMEM = 1024 + 2 * A_PART + 4 * B_PART + 2 * STAGE;
+  static constexpr int TMEM_COLS = 128;          // one 128-column accumulator
+  static constexpr int SMEM = 1024 + 2 * A_PART + 2 * B_PART + STAGE;
 };
 
 constexpr int kTmaMaxBoxes = 64;   // boxes per staged tile (N / 8 at most)
@@ -148,7 +153,7 @@ __device__ __forceinline__ int tma_col(const TmaArgs &a, int kx) {
 }
 
 template <int N, bool INV>
-__global__ void __launch_bounds__(TmaPlan<N>::THREADS, 1)
+__global__ void __launch_bounds__(TmaPlan<N>::THREADS, TmaPlan<N>::CTAS_PER_SM)
     k_strided_tma(const __grid_constant__ TmaArgs a, const __half *__restrict__ Adft, int *status) {
   using C = float2;
   using PL = TmaPlan<N>;
@@ -158,14 +163,18 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, 1)
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   unsigned char *sAh = base;                        // K-major, no swizzle
   unsigned char *sAl = base + PL::A_PART;
-  unsigned char *sB = base + 2 * PL::A_PART;        // [buffer][hi, lo], 1024-byte aligned
-  unsigned char *stg = sB + 4 * PL::B_PART;         // staging: [2][N][SPC] complex
-  __shared__ __align__(8) uint64_t full[2], mmab[2];
+  unsigned char *sBh = base + 2 * PL::A_PART;       // MN-major, 128-byte swizzle, 1024-byte aligned
+  unsigned char *sBl = sBh + PL::B_PART;
+  const C *stg = reinterpret_cast<const C *>(sBh + 2 * PL::B_PART);   // staging: [N][SPC] complex
+  __shared__ __align__(8) uint64_t full, mmab;
   __shared__ uint32_t taddr_s;
   __shared__ int abort_s;
-  __shared__ unsigned pm[3][TCW];      // per-column max |Re|, |Im| bits, rotating over tiles
-  __shared__ float krow[N];            // wavenumber of each row index along the transformed axis
-  __shared__ C tws[(N2 - 1) * 64];     // W_N^(n1 k2), k2 = 1 .. N2-1
+  __shared__ unsigned pm[2][TCW];              // per-column max |Re|, |Im| bits (tile parity)
+  __shared__ __align__(16) float usc[2][TCW];  // per-column unscale 2^e (tile parity)
+  __shared__ int colkx[2][TCW];                // half-axis index of each tile column, -1 if not kept (tile parity)
+  __shared__ float colk[TCW];                  // its wavenumber
+  __shared__ float krow[N];                    // wavenumber of each row index along the transformed axis
+  __shared__ C tws[(N2 - 1) * 64];             // W_N^(n1 k2), k2 = 1 .. N2-1
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   for (int i = t; i < (N2 - 1) * 64; i += PL::THREADS) tws[i] = a.tw[(i / 64 + 1) * (i % 64)];
   for (int n = t; n < N; n += PL::THREADS) krow[n] = (float)k_full(n, N, a.alpha_row);
@@ -174,16 +183,14 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, 1)
     uint4 *dst = reinterpret_cast<uint4 *>(sAh);
     for (int i = t; i < 2 * PL::A_PART / 16; i += PL::THREADS) dst[i] = src[i];
   }
-  if (t < 3 * TCW) pm[t / TCW][t % TCW] = 0u;
+  if (t < 2 * TCW) pm[t / TCW][t % TCW] = 0u;
   if (warp == 0) {
     tc::tmem_alloc(&taddr_s, PL::TMEM_COLS);
     tc::tmem_relinquish();
   }
   if (t == 0) {
-    tc::mbar_init(&full[0], 1);
-    tc::mbar_init(&full[1], 1);
-    tc::mbar_init(&mmab[0], 1);
-    tc::mbar_init(&mmab[1], 1);
+    tc::mbar_init(&full, 1);
+    tc::mbar_init(&mmab, 1);
     tma::fence_mbar_init();
     abort_s = 0;
   }
@@ -193,241 +200,336 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, 1)
   tc::fence_after_sync();
   const uint32_t taddr = taddr_s;
   constexpr uint32_t idesc = (1u << 4) | (1u << 16) | ((uint32_t)(128 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-  const int NST = a.two ? 1 : 2;      // staging buffers in rotation
   const unsigned nb = gridDim.x;
   const int my_n = (int)blockIdx.x < a.total ? (a.total - (int)blockIdx.x + (int)nb - 1) / (int)nb : 0;
   const uint32_t box_bytes = (uint32_t)a.box_rows * SPC * 8;
 
-  // tile i of this CTA: loads into staging buffer s, issued by the lanes of
-  // warp 0 (one box each, after lane 0 has armed the barrier)
-  auto issue_loads = [&](int i, int s) {
+  // one staged input of tile i (input q: 0 in1, 1 in2), issued by the lanes
+  // of warp 0 (one box each) after lane 0 has armed the barrier
+  auto issue_load = [&](int i, int q) {
     const TmaItem it = tma_item<TCW>(a, blockIdx.x + (unsigned)i * nb);
-    const TmaJob &J = a.job[it.job];
-    const int nin = J.slot2 >= 0 ? 2 : 1;
-    if (lane == 0) tma::expect_tx(&full[s], (uint32_t)(nin * a.nbox) * box_bytes);
+    const int slot = q ? a.job[it.job].slot2 : a.job[it.job].slot1;
+    if (lane == 0) tma::expect_tx(&full, (uint32_t)a.nbox * box_bytes);
     __syncwarp();
     const int off = it.other * a.in_pitch + it.kx0;   // plane mode: column index within the plane
     const int x = a.plane ? 2 * (off - (off & 1)) : 2 * it.kx0;   // 16-byte aligned start
-    for (int k = lane; k < nin * a.nbox; k += 32) {
-      const int q = k >= a.nbox ? 1 : 0, b = k - q * a.nbox;
-      const int slot = q ? J.slot2 : J.slot1;
-      unsigned char *dst = stg + (size_t)(s + q) * PL::STAGE + (size_t)a.box_row[b] * SPC * 8;
+    for (int b = lane; b < a.nbox; b += 32) {
       const int r0 = a.box_row[b];
-      if (a.plane) tma::load5(dst, &a.map, x, r0, it.box, slot, 0, &full[s]);
-      else tma::load5(dst, &a.map, x, r0, it.other, it.box, slot, &full[s]);
+      unsigned char *dst = const_cast<unsigned char *>(reinterpret_cast<const unsigned char *>(stg)) +
+                           (size_t)r0 * SPC * 8;
+      if (a.plane) tma::load5(dst, &a.map, x, r0, it.box, slot, 0, &full);
+      else tma::load5(dst, &a.map, x, r0, it.other, it.box, slot, &full);
     }
   };
 
-  // stage-A item of this thread: n1 (four per warp, chosen so that the
-  // warp's operand stores fall in distinct bank groups) and column group cg
+  // Stage-A items of this thread: item h covers n1(h) (four per warp, chosen
+  // so that a warp's operand stores fall in distinct bank groups) and the G
+  // columns c0 .. c0 + G - 1.
   const int cg = lane & 7, jq = lane >> 3;
   constexpr int D1 = G >= 2 ? 1 : 2;
-  const int n1 = 8 * (warp >> 1) + (jq & 1) * D1 + 4 * (jq >> 1) + (warp & 1) * (D1 == 1 ? 2 : 1);
+  int n1s[2];
+  unsigned rin = 0;   // kept input rows: bit h N2 + n2 for row 64 n2 + n1(h)
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int vw = warp + 8 * h;
+    n1s[h] = 8 * (vw >> 1) + (jq & 1) * D1 + 4 * (jq >> 1) + (vw & 1) * (D1 == 1 ? 2 : 1);
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) rin |= (a.krin.keep(64 * n2 + n1s[h]) ? 1u : 0u) << (h * N2 + n2);
+  }
   const int c0 = cg * G;
+  // Drain: warp w reads TMEM lanes 32 (w % 4) + lane (k1 = 16 (w % 4) + lane / 2)
+  // and the two 32-column blocks 64 (w / 4) .. + 63 (pencils 32 (w / 4) .. + 31).
+  const int q4 = warp & 3;
+  const bool odd = lane & 1;
+  const int k1 = 16 * q4 + (lane >> 1);
+  unsigned rout = 0;  // kept output rows: bit 4 sb + k / 2 for pair k of sub-block sb
+  int roff[8];        // their row offsets (complex elements)
+#pragma unroll
+  for (int sb = 0; sb < 2; ++sb)
+#pragma unroll
+    for (int k = 0; k < 8; k += 2) {
+      const int j = 32 * (warp >> 2) + 16 * sb + (odd ? 8 : 0) + k;
+      const int row = j / TCW + N2 * k1;
+      rout |= (a.krout.keep(row) ? 1u : 0u) << (4 * sb + k / 2);
+      roff[4 * sb + k / 2] = row * (int)a.rso;
+    }
 
-  if (warp == 0)
-    for (int i = 0; i < NST && i < my_n; ++i) issue_loads(i, i);
-  // Tile k of this CTA uses staging buffer k % NST with mbarrier parity
-  // (k / NST) & 1 and accumulator k & 1 with parity (k >> 1) & 1.  Thread 0
-  // counts the tiles whose loads it issued and whose loads / MMAs it saw
-  // complete, for the bounded clean-up after an abort.
-  int loads_issued = NST < my_n ? NST : my_n, loads_seen = 0, mma_issued = 0, mma_seen = 0;
+  // Tile k uses the staging barrier once per input (parity = running input
+  // count & 1) and the MMA barrier once (parity k & 1).  Thread 0 counts the
+  // inputs and MMAs issued and seen, for the bounded clean-up after an abort.
+  int loads_issued = 0, loads_seen = 0, mma_issued = 0, mma_seen = 0;
+  if (warp == 0 && my_n > 0) {
+    issue_load(0, 0);
+    ++loads_issued;
+  }
   TmaItem prev{};
   bool aborted = false;
+  auto wait_load = [&]() {   // thread 0
+    if (tc::mbar_wait_bounded(&full, (uint32_t)loads_seen & 1u, kTmaWaitLimit)) ++loads_seen;
+    else abort_s = 1;
+  };
   for (int i = 0; i <= my_n; ++i) {
-    const int bb = i & 1;
+    const int par = i & 1;
+    C z[2][G][N2];   // stage-A values of this thread's items (tile i)
     if (i < my_n) {
-      const int s = NST == 2 ? (i & 1) : 0;
       const TmaItem it = tma_item<TCW>(a, blockIdx.x + (unsigned)i * nb);
-      const TmaJob &J = a.job[it.job];
-      // ---- wait for the staged tile (every thread polls, bounded)
-      if (tc::mbar_wait_bounded(&full[s], (uint32_t)(i / NST) & 1u, kTmaWaitLimit)) ++loads_seen;
-      else abort_s = 1;
-      // ---- stage A: multipliers, N2-point DFT, twiddle, column maxima
-      const C *st1 = reinterpret_cast<const C *>(stg + (size_t)s * PL::STAGE);
-      const C *st2 = reinterpret_cast<const C *>(stg + (size_t)(s + 1) * PL::STAGE);
-      const int shift = a.plane ? ((it.other * a.in_pitch + it.kx0) & 1) : 0;
-      const float koth = a.n_other ? (float)k_full(it.other, a.n_other, a.alpha_other) : 0.f;
-      C z[G][N2];
-      float cmax[G];
-#pragma unroll
-      for (int g = 0; g < G; ++g) {
-        const int c = c0 + g;
-        const int kx = tma_col(a, it.kx0 + c);
-        const bool valid = kx < a.ncols && a.kcol.keep(kx);
-        const bool slotcol = kx != it.kx0 + c;   // merged Nyquist column: read from global memory
-        const float kcol = (float)k_half(kx, a.nx, a.alpha_x);
-        const float kc1 = J.ks1 == 2 ? koth : kcol, kc2 = J.ks2 == 2 ? koth : kcol;
-        const long long gbase = (long long)it.box * a.bstride + (long long)it.other * a.otherstride + kx;
-#pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) {
-          const int n = 64 * n2 + n1;
-          const bool ok = valid && a.krin.keep(n);
-          C v = mkc<C>(0.f, 0.f);
-          if (ok) {
-            v = slotcol ? J.in1[gbase + (long long)n * a.rowstride] : st1[n * SPC + c + shift];
-            if (!(J.a1 == 1.f && J.b1 == 0.f)) {
-              const float bk = J.b1 * (J.ks1 == 1 ? krow[n] : kc1);
-              v = mkc<C>(v.x * J.a1 - v.y * bk, v.y * J.a1 + v.x * bk);
-            }
-            if (J.slot2 >= 0) {
-              const C w2 = slotcol ? J.in2[gbase + (long long)n * a.rowstride] : st2[n * SPC + c + shift];
-              const float bk = J.b2 * (J.ks2 == 1 ? krow[n] : kc2);
-              v = mkc<C>(v.x + (w2.x * J.a2 - w2.y * bk), v.y + (w2.y * J.a2 + w2.x * bk));
-            }
-          }
-          z[g][n2] = v;
-        }
-        dft<N2, C, INV>(z[g]);
-        float m = fmaxf(fabsf(z[g][0].x), fabsf(z[g][0].y));
-#pragma unroll
-        for (int k2 = 1; k2 < N2; ++k2) {
-          const C tw = tws[(k2 - 1) * 64 + n1];
-          z[g][k2] = INV ? cmulc(z[g][k2], tw) : cmul(z[g][k2], tw);
-          m = fmaxf(m, fmaxf(fabsf(z[g][k2].x), fabsf(z[g][k2].y)));
-        }
-        // the warp's four n1 of this column group are lanes cg + 8 jq
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 8));
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 16));
-        cmax[g] = m;
+      const TmaJob J = a.job[it.job];
+      const bool two = J.slot2 >= 0;
+      // ---- per-tile column table, staging wait
+      if (t < TCW) {
+        const int kx = tma_col(a, it.kx0 + t);
+        const bool ok = kx < a.ncols && a.kcol.keep(kx);
+        colkx[par][t] = ok ? kx : -1;
+        colk[t] = (float)k_half(kx, a.nx, a.alpha_x);
       }
-      unsigned *pmi = pm[i % 3];
-      if (jq == 0)
-#pragma unroll
-        for (int g = 0; g < G; ++g) atomicMax(&pmi[c0 + g], __float_as_uint(cmax[g]));
-      __syncthreads();   // #1: column maxima complete
+      if (t == 0) wait_load();
+      __syncthreads();   // A: staged input 1 and the column table visible
       if (abort_s) {
         aborted = true;
         break;
       }
-      if (t < TCW) pm[(i + 1) % 3][t] = 0u;   // used by tile i - 2, drained in the previous iteration
-      // ---- scale, split into f16 hi + lo, store the B operands
-      unsigned char *Bh = sB + (size_t)bb * 2 * PL::B_PART, *Bl = Bh + PL::B_PART;
-      float sc[G];
+      if (t < TCW) pm[par ^ 1][t] = 0u;   // for tile i + 1 (its last reader, tile i - 1's split, is done)
+      const int shift = a.plane ? ((it.other * a.in_pitch + it.kx0) & 1) : 0;
+      const float koth = a.n_other ? (float)k_full(it.other, a.n_other, a.alpha_other) : 0.f;
+      const bool mult1 = !(J.a1 == 1.f && J.b1 == 0.f);
+      // ---- stage A, input 1
 #pragma unroll
-      for (int g = 0; g < G; ++g) sc[g] = __int_as_float((127 - tc_exp(pmi[c0 + g])) << 23);   // 2^-e
-#pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) {
-        __align__(16) __half2 hv[G], lv[G];
+      for (int h = 0; h < 2; ++h)
 #pragma unroll
         for (int g = 0; g < G; ++g) {
-          const float2 x = make_float2(z[g][k2].x * sc[g], z[g][k2].y * sc[g]);
-          hv[g] = __float22half2_rn(x);
-          const float2 hb = __half22float2(hv[g]);
-          lv[g] = __float22half2_rn(make_float2(x.x - hb.x, x.y - hb.y));
-        }
-        const int off = tma::b_offset(n1, 2 * (k2 * TCW + c0));
-        if constexpr (G == 4) {
-          *reinterpret_cast<uint4 *>(Bh + off) = *reinterpret_cast<const uint4 *>(hv);
-          *reinterpret_cast<uint4 *>(Bl + off) = *reinterpret_cast<const uint4 *>(lv);
-        } else if constexpr (G == 2) {
-          *reinterpret_cast<uint2 *>(Bh + off) = *reinterpret_cast<const uint2 *>(hv);
-          *reinterpret_cast<uint2 *>(Bl + off) = *reinterpret_cast<const uint2 *>(lv);
-        } else {
-          *reinterpret_cast<__half2 *>(Bh + off) = hv[0];
-          *reinterpret_cast<__half2 *>(Bl + off) = lv[0];
-        }
-      }
-      tc::fence_proxy_async();
-      tc::fence_before_sync();
-      __syncthreads();   // #2: operands written, staging buffer s consumed
-      if (warp == 0) {
-        tc::fence_after_sync();
-        if (loads_issued < my_n) {
-          issue_loads(loads_issued, NST == 2 ? (loads_issued & 1) : 0);
-          ++loads_issued;
-        }
-      }
-      if (t == 0) {
-        // 3 x 4 MMAs (K = 16 each) into accumulator bb: Al Bh, Ah Bl, then Ah Bh
-        constexpr uint32_t lboA = (128 / 8) * 128, sboA = 128, lboB = 8192, sboB = 1024;
+          const int c = c0 + g;
+          const int kx = colkx[par][c];
+          const bool slotcol = kx >= 0 && kx != it.kx0 + c;   // merged Nyquist column: global memory
+          const float kc = J.ks1 == 2 ? koth : colk[c];
+          const C *src = stg + n1s[h] * SPC + c + shift;
+          const long long gb = (long long)it.box * a.bstride + (long long)it.other * a.otherstride + kx;
 #pragma unroll
-        for (int p = 0; p < 3; ++p) {
-          const unsigned char *A = p == 0 ? sAl : sAh;
-          const unsigned char *B = p == 1 ? Bl : Bh;
-#pragma unroll
-          for (int ks = 0; ks < 4; ++ks)
-            tc::mma_f16(taddr + 128u * bb, tc::smem_desc(A + 2 * ks * lboA, lboA, sboA),
-                        tma::desc_sw128(B + 2 * ks * sboB, lboB, sboB), idesc, (p | ks) ? 1u : 0u);
+          for (int n2 = 0; n2 < N2; ++n2) {
+            const int n = 64 * n2 + n1s[h];
+            C v = mkc<C>(0.f, 0.f);
+            if (kx >= 0 && ((rin >> (h * N2 + n2)) & 1u)) {
+              v = slotcol ? J.in1[gb + (long long)n * a.rowstride] : src[64 * n2 * SPC];
+              if (mult1) {
+                const float bk = J.b1 * (J.ks1 == 1 ? krow[n] : kc);
+                v = mkc<C>(v.x * J.a1 - v.y * bk, v.y * J.a1 + v.x * bk);
+              }
+            }
+            z[h][g][n2] = v;
+          }
         }
-        tc::mma_commit(&mmab[bb]);
-        ++mma_issued;
+      if (two) {
+        // ---- second input of a two-input job, staged after the first
+        __syncthreads();
+        if (warp == 0) {
+          issue_load(i, 1);
+          if (lane == 0) ++loads_issued;
+        }
+        if (t == 0) wait_load();
+        __syncthreads();
+        if (abort_s) {
+          aborted = true;
+          break;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            const int c = c0 + g;
+            const int kx = colkx[par][c];
+            const bool slotcol = kx >= 0 && kx != it.kx0 + c;
+            const float kc = J.ks2 == 2 ? koth : colk[c];
+            const C *src = stg + n1s[h] * SPC + c + shift;
+            const long long gb = (long long)it.box * a.bstride + (long long)it.other * a.otherstride + kx;
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) {
+              const int n = 64 * n2 + n1s[h];
+              if (kx >= 0 && ((rin >> (h * N2 + n2)) & 1u)) {
+                const C w2 = slotcol ? J.in2[gb + (long long)n * a.rowstride] : src[64 * n2 * SPC];
+                const float bk = J.b2 * (J.ks2 == 1 ? krow[n] : kc);
+                z[h][g][n2] = mkc<C>(z[h][g][n2].x + (w2.x * J.a2 - w2.y * bk),
+                                     z[h][g][n2].y + (w2.y * J.a2 + w2.x * bk));
+              }
+            }
+          }
       }
-    }
-    // ---- drain the previous tile
-    if (i >= 1) {
-      const int pb = (i - 1) & 1;
-      if (t == 0) {
-        if (tc::mbar_wait_bounded(&mmab[pb], (uint32_t)((i - 1) >> 1) & 1u, kTmaWaitLimit)) ++mma_seen;
+      __syncthreads();   // B0: the staging tile is consumed
+      if (warp == 0 && i + 1 < my_n) {
+        issue_load(i + 1, 0);
+        if (lane == 0) ++loads_issued;
+      }
+      // ---- N2-point DFT, twiddle, column maxima
+      float cmax[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) cmax[g] = 0.f;
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          dft<N2, C, INV>(z[h][g]);
+          float m = fmaxf(fabsf(z[h][g][0].x), fabsf(z[h][g][0].y));
+#pragma unroll
+          for (int k2 = 1; k2 < N2; ++k2) {
+            const C tw = tws[(k2 - 1) * 64 + n1s[h]];
+            z[h][g][k2] = INV ? cmulc(z[h][g][k2], tw) : cmul(z[h][g][k2], tw);
+            m = fmaxf(m, fmaxf(fabsf(z[h][g][k2].x), fabsf(z[h][g][k2].y)));
+          }
+          cmax[g] = fmaxf(cmax[g], m);
+        }
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        // the warp's four n1 of this column group are lanes cg + 8 jq
+        float m = fmaxf(cmax[g], __shfl_xor_sync(0xffffffffu, cmax[g], 8));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 16));
+        if (jq == 0) atomicMax(&pm[par][c0 + g], __float_as_uint(m));
+      }
+      if (t == 0 && i > 0) {   // MMA(i - 1) done: the accumulator and B are free
+        if (tc::mbar_wait_bounded(&mmab, (uint32_t)(i - 1) & 1u, kTmaWaitLimit)) ++mma_seen;
         else abort_s = 1;
       }
       tc::fence_before_sync();
-      __syncthreads();   // #3
+      __syncthreads();   // B: column maxima complete, MMA(i - 1) complete
       tc::fence_after_sync();
       if (abort_s) {
         aborted = true;
         break;
       }
-      const TmaItem it = prev;
-      const TmaJob &J = a.job[it.job];
-      const int q = warp & 3, g4 = warp >> 2;
-      const uint32_t ta = taddr + ((uint32_t)(32 * q) << 16) + 128u * pb + 32u * g4;
-      float v[32];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-          "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-          : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
-            "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15]),
-            "=f"(v[16]), "=f"(v[17]), "=f"(v[18]), "=f"(v[19]), "=f"(v[20]), "=f"(v[21]), "=f"(v[22]), "=f"(v[23]),
-            "=f"(v[24]), "=f"(v[25]), "=f"(v[26]), "=f"(v[27]), "=f"(v[28]), "=f"(v[29]), "=f"(v[30]), "=f"(v[31])
-          : "r"(ta)
-          : "memory");
-      tc::tmem_ld_wait();
-      const bool odd = lane & 1;
-      const int k1 = 16 * q + (lane >> 1);
-      const unsigned *pmd = pm[(i - 1) % 3];
-      float w[16];
-#pragma unroll
-      for (int jj = 0; jj < 16; ++jj) {
-        const float tpart = __shfl_xor_sync(0xffffffffu, v[2 * jj + 1], 1);
-        const int c = (16 * g4 + jj) % TCW;
-        const float us = __int_as_float((127 + tc_exp(pmd[c])) << 23);   // 2^e
-        w[jj] = (odd ? tpart + v[2 * jj] : v[2 * jj] - tpart) * us;
+    } else {
+      // after the last tile: wait for its MMAs before draining
+      if (t == 0 && i > 0) {
+        if (tc::mbar_wait_bounded(&mmab, (uint32_t)(i - 1) & 1u, kTmaWaitLimit)) ++mma_seen;
+        else abort_s = 1;
       }
-      // even lane: pencils 0..7 (re own, im from the odd lane); odd lane: 8..15
-      float r[8];
+      tc::fence_before_sync();
+      __syncthreads();
+      tc::fence_after_sync();
+      if (abort_s) {
+        aborted = true;
+        break;
+      }
+    }
+    // ---- drain tile i - 1 (accumulator: its MMAs are complete)
+    if (i >= 1) {
+      const TmaItem it = prev;
+      C *obase = a.job[it.job].out + ((long long)it.box * a.bso + (long long)it.other * a.oso);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) r[k] = __shfl_xor_sync(0xffffffffu, odd ? w[k] : w[8 + k], 1);
-      const int jbase = 16 * g4 + (odd ? 8 : 0);
-      const long long obase = (long long)it.box * a.bso + (long long)it.other * a.oso;
+      for (int sb = 0; sb < 2; ++sb) {
+        const int col0 = 64 * (warp >> 2) + 32 * sb;   // accumulator columns of this block
+        const uint32_t ta = taddr + ((uint32_t)(32 * q4) << 16) + (uint32_t)col0;
+        float v[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
+              "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15]),
+              "=f"(v[16]), "=f"(v[17]), "=f"(v[18]), "=f"(v[19]), "=f"(v[20]), "=f"(v[21]), "=f"(v[22]),
+              "=f"(v[23]), "=f"(v[24]), "=f"(v[25]), "=f"(v[26]), "=f"(v[27]), "=f"(v[28]), "=f"(v[29]),
+              "=f"(v[30]), "=f"(v[31])
+            : "r"(ta)
+            : "memory");
+        tc::tmem_ld_wait();
+        // unscale factors of the block's 16 pencils j = col0 / 2 + jj, column j % TCW
+        float us[16];
+        const float *ut = usc[par ^ 1];
+        if constexpr (TCW >= 16) {
+          const int cb = (col0 / 2) % TCW;
 #pragma unroll
-      for (int k = 0; k < 8; k += 2) {
-        const int j = jbase + k;
-        const int k2 = j / TCW, c = j % TCW;   // c even: the pair (c, c + 1) shares the output row
-        const int row = k2 + N2 * k1;
-        if (!a.krout.keep(row)) continue;
-        const C y0 = odd ? mkc<C>(r[k], w[8 + k]) : mkc<C>(w[k], r[k]);
-        const C y1 = odd ? mkc<C>(r[k + 1], w[9 + k]) : mkc<C>(w[k + 1], r[k + 1]);
-        const int kx0c = it.kx0 + c;
-        const int kxa = tma_col(a, kx0c), kxb = tma_col(a, kx0c + 1);
-        const bool va = kxa < a.ncols && a.kcol.keep(kxa), vb = kxb < a.ncols && a.kcol.keep(kxb);
-        C *orow = J.out + obase + (long long)row * a.rso;
-        if (va && vb && kxa == kx0c && kxb == kx0c + 1) {
-          *reinterpret_cast<float4 *>(orow + kx0c) = make_float4(y0.x, y0.y, y1.x, y1.y);
+          for (int k = 0; k < 16; k += 4) {
+            const float4 q = *reinterpret_cast<const float4 *>(ut + cb + k);
+            us[k] = q.x, us[k + 1] = q.y, us[k + 2] = q.z, us[k + 3] = q.w;
+          }
         } else {
-          if (va) orow[kxa] = y0;
-          if (vb) orow[kxb] = y1;
+#pragma unroll
+          for (int k = 0; k < 8; k += 4) {
+            const float4 q = *reinterpret_cast<const float4 *>(ut + k);
+            us[k] = us[k + 8] = q.x, us[k + 1] = us[k + 9] = q.y, us[k + 2] = us[k + 10] = q.z,
+                        us[k + 3] = us[k + 11] = q.w;
+          }
+        }
+        float w[16];
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+          const float tp = __shfl_xor_sync(0xffffffffu, v[2 * jj + 1], 1);
+          w[jj] = (odd ? tp + v[2 * jj] : v[2 * jj] - tp) * us[jj];
+        }
+        // even lane: pencils 0..7 of the block (re own, im from the odd lane); odd lane: 8..15
+        float r[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) r[k] = __shfl_xor_sync(0xffffffffu, odd ? w[k] : w[8 + k], 1);
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+          if (!((rout >> (4 * sb + k / 2)) & 1u)) continue;
+          const int j = col0 / 2 + (odd ? 8 : 0) + k;
+          const int c = j % TCW;   // even: the pair (c, c + 1) shares the output row
+          const C y0 = odd ? mkc<C>(r[k], w[8 + k]) : mkc<C>(w[k], r[k]);
+          const C y1 = odd ? mkc<C>(r[k + 1], w[9 + k]) : mkc<C>(w[k + 1], r[k + 1]);
+          const int kxa = colkx[par ^ 1][c], kxb = colkx[par ^ 1][c + 1];
+          C *orow = obase + roff[4 * sb + k / 2];
+          if (kxa >= 0 && kxb >= 0 && kxa == it.kx0 + c && kxb == it.kx0 + c + 1) {
+            *reinterpret_cast<float4 *>(orow + kxa) = make_float4(y0.x, y0.y, y1.x, y1.y);
+          } else {
+            if (kxa >= 0) orow[kxa] = y0;
+            if (kxb >= 0) orow[kxb] = y1;
+          }
         }
       }
     }
-    if (i < my_n) prev = tma_item<TCW>(a, blockIdx.x + (unsigned)i * nb);
+    if (i < my_n) {
+      // ---- scale, split into f16 hi + lo, store the B operand (its last
+      //      reader, MMA(i - 1), is complete)
+      if (t < TCW) usc[par][t] = __int_as_float((127 + tc_exp(pm[par][t])) << 23);   // 2^e, for the drain
+      float sc[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) sc[g] = __int_as_float((127 - tc_exp(pm[par][c0 + g])) << 23);   // 2^-e
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          __align__(16) __half2 hv[G], lv[G];
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            const float2 x = make_float2(z[h][g][k2].x * sc[g], z[h][g][k2].y * sc[g]);
+            hv[g] = __float22half2_rn(x);
+            const float2 hb = __half22float2(hv[g]);
+            lv[g] = __float22half2_rn(make_float2(x.x - hb.x, x.y - hb.y));
+          }
+          const int off = tma::b_offset(n1s[h], 2 * (k2 * TCW + c0));
+          if constexpr (G == 4) {
+            *reinterpret_cast<uint4 *>(sBh + off) = *reinterpret_cast<const uint4 *>(hv);
+            *reinterpret_cast<uint4 *>(sBl + off) = *reinterpret_cast<const uint4 *>(lv);
+          } else if constexpr (G == 2) {
+            *reinterpret_cast<uint2 *>(sBh + off) = *reinterpret_cast<const uint2 *>(hv);
+            *reinterpret_cast<uint2 *>(sBl + off) = *reinterpret_cast<const uint2 *>(lv);
+          } else {
+            *reinterpret_cast<__half2 *>(sBh + off) = hv[0];
+            *reinterpret_cast<__half2 *>(sBl + off) = lv[0];
+          }
+        }
+      tc::fence_proxy_async();
+      tc::fence_before_sync();
+      __syncthreads();   // C: operands written; the drain's TMEM reads are complete
+      if (t == 0) {
+        tc::fence_after_sync();
+        // 3 x 4 MMAs (K = 16 each) into the accumulator: Al Bh, Ah Bl, then Ah Bh
+        constexpr uint32_t lboA = (128 / 8) * 128, sboA = 128, lboB = 8192, sboB = 1024;
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          const unsigned char *A = p == 0 ? sAl : sAh;
+          const unsigned char *B = p == 1 ? sBl : sBh;
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks)
+            tc::mma_f16(taddr, tc::smem_desc(A + 2 * ks * lboA, lboA, sboA),
+                        tma::desc_sw128(B + 2 * ks * sboB, lboB, sboB), idesc, (p | ks) ? 1u : 0u);
+        }
+        tc::mma_commit(&mmab);
+        ++mma_issued;
+      }
+      prev = tma_item<TCW>(a, blockIdx.x + (unsigned)i * nb);
+    }
   }
   if (aborted && t == 0) {
     // wait (bounded) for the copies and MMAs still in flight before TMEM is freed
-    for (int k = loads_seen; k < loads_issued; ++k)
-      tc::mbar_wait_bounded(&full[NST == 2 ? (k & 1) : 0], (uint32_t)(k / NST) & 1u, kTmaWaitLimit);
-    for (int k = mma_seen; k < mma_issued; ++k)
-      tc::mbar_wait_bounded(&mmab[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitLimit);
+    for (int k = loads_seen; k < loads_issued; ++k) tc::mbar_wait_bounded(&full, (uint32_t)k & 1u, kTmaWaitLimit);
+    for (int k = mma_seen; k < mma_issued; ++k) tc::mbar_wait_bounded(&mmab, (uint32_t)k & 1u, kTmaWaitLimit);
     atomicExch(status, 1);
   }
   tc::fence_before_sync();

@@ -118,6 +118,10 @@ cudaError_t Launcher<T, N>::strided_tma(const TmaArgs &a, bool inv, const void *
     const unsigned nb = (unsigned)(a.total < nctas ? a.total : nctas);
     const __half *A = reinterpret_cast<const __half *>(adft) + (inv ? 2 * 128 * 64 : 0);
     cudaError_t e;
+    // two CTAs of ~105 KB per SM: ask for the largest shared-memory carveout
+    if ((e = cudaFuncSetAttribute(inv ? k_strided_tma<N, true> : k_strided_tma<N, false>,
+                                  cudaFuncAttributePreferredSharedMemoryCarveout, 100)) != cudaSuccess)
+      return e;
     if (inv) {
       if ((e = set_smem(k_strided_tma<N, true>, PL::SMEM)) != cudaSuccess) return e;
       k_strided_tma<N, true><<<nb, PL::THREADS, PL::SMEM, st>>>(a, A, status);
