@@ -103,7 +103,7 @@ struct dnsbox_ctx {
   // kernel schedule of the right-hand side (chosen by dnsbox_autotune, or the
   // defaults): passes A, B, D 0 = TMA-staged tensor-core kernel, 1 = the
   // cp.async-fed one; pass E1 0 = SIMT, 1 = TMA-staged tensor-core kernel;
-  // x pass 0 = default, 1 = block, 2 = warp
+  // x pass 0 = default, 1 = block, 2 = warp, 3 = warp with 128 registers
   int sched_tc[4] = {0, 0, 0, 0};
   int sched_x = 0;
   char *adj = nullptr;                   // adjoint arena

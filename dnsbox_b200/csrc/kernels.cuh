@@ -536,8 +536,11 @@ __device__ __forceinline__ void xline_w_tail(typename CT<T>::type *s, const Xlin
   }
 }
 
-template <typename T, int N>
-__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
+// MINB > 0 asks the register allocator for MINB resident blocks per SM (at
+// most 128 registers for the FP32 N = 256 blocks of four warps: 16 warps per
+// SM instead of the 12 that its default allocation leaves room for).
+template <typename T, int N, int MINB = 0>
+__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb, MINB)
     k_xline_nl_w(const __grid_constant__ XlineNLArgs<T> a) {
   using C = typename CT<T>::type;
   using PL = typename XlineWarp<T, N>::Plan;

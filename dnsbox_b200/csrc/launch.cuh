@@ -22,7 +22,8 @@ template <typename T, int N> struct Launcher {
   static cudaError_t strided_tma(const TmaArgs &a, bool inv, const void *adft, int *status, int nctas,
                                  cudaStream_t st);
   static bool has_tma();
-  // variant: 0 the default kernel for N, 1 the block kernel, 2 the warp kernel (where it exists)
+  // variant: 0 the default kernel for N, 1 the block kernel, 2 the warp kernel, 3 the warp kernel held
+  // to the registers of four resident blocks per SM (2 and 3 where the warp kernel exists)
   static cudaError_t xline_nl(const XlineNLArgs<T> &a, int variant, cudaStream_t st);
   static bool has_xline_warp();
   static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);
@@ -148,10 +149,15 @@ cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaS
     constexpr int LDC = N + N / XlineWarp<T, N>::Plan::R[0];
     const size_t smem = (size_t)WPB * 6 * LDC * sizeof(C);
     cudaError_t e;
-    if ((e = set_smem(k_xline_nl_w<T, N>, smem)) != cudaSuccess) return e;
     const long long pairs = (a.nlines + 1) / 2;
     const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
-    k_xline_nl_w<T, N><<<nb, 32 * WPB, smem, st>>>(a);
+    if (variant == 3) {
+      if ((e = set_smem(k_xline_nl_w<T, N, 4>, smem)) != cudaSuccess) return e;
+      k_xline_nl_w<T, N, 4><<<nb, 32 * WPB, smem, st>>>(a);
+    } else {
+      if ((e = set_smem(k_xline_nl_w<T, N>, smem)) != cudaSuccess) return e;
+      k_xline_nl_w<T, N><<<nb, 32 * WPB, smem, st>>>(a);
+    }
     return cudaGetLastError();
     }
   }

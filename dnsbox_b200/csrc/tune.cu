@@ -7,8 +7,8 @@
 // differently across sizes are made by timing: for each of the tensor-core
 // strided passes (A inverse z, B inverse y, D forward y) the TMA-staged or
 // the cp.async-fed kernel, for the forward z pass (E1) the SIMT or the
-// TMA-staged tensor-core kernel, and for the fused x pass the block or the
-// warp kernel.  Each uniform candidate schedule advances a copy of the caller's
+// TMA-staged tensor-core kernel, and for the fused x pass the block kernel or
+// the warp kernel with its default or a four-blocks-per-SM register budget.  Each uniform candidate schedule advances a copy of the caller's
 // state for a few steps with pass timing on (CUDA events on the context's
 // stream); every pass keeps its fastest kernel; the chosen schedule is timed
 // once more.  The context's clock, time step and step history are restored,
@@ -127,7 +127,7 @@ extern "C" int dnsbox_set_schedule(dnsbox_ctx *ctx, const dnsbox_schedule *s) {
   if (!ctx || !s) return set_err(DNSBOX_ERR_ARG, "null argument");
   for (int i = 0; i < 4; ++i)
     if (s->tc_kernel[i] != 0 && s->tc_kernel[i] != 1) return set_err(DNSBOX_ERR_ARG, "tc_kernel must be 0 or 1");
-  if (s->x_kernel < 0 || s->x_kernel > 2) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0, 1 or 2");
+  if (s->x_kernel < 0 || s->x_kernel > 3) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0 .. 3");
   apply(ctx, *s);
   return DNSBOX_OK;
 }
@@ -149,7 +149,7 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
     if (Ops<float>::has_tma(p.nz)) e1_opts.push_back(1);
   }
   std::vector<int> x_opts = {0};
-  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1};
+  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1, 3};
   const dnsbox_schedule saved_sched = current(ctx);
   Saved sv;
   RET(save(ctx, sv));
