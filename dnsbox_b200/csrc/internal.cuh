@@ -361,15 +361,17 @@ template <typename T>
 static int run_strided(dnsbox_ctx *c, int axis, bool inv, StridedArgs<T> a, int kind = DNSBOX_PASS_OTHER,
                        bool allow_tc = true, const void *tma_base = nullptr, int tma_slots = 0) {
   const int n = axis == 2 ? c->p.nz : c->p.ny;
+  const int si = kind == DNSBOX_PASS_Z_INV ? 0 : kind == DNSBOX_PASS_Y_INV ? 1 : kind == DNSBOX_PASS_Y_FWD ? 2
+               : kind == DNSBOX_PASS_Z_FWD ? 3 : -1;
   if constexpr (sizeof(T) == 4) {
-    const int si = kind == DNSBOX_PASS_Z_INV ? 0 : kind == DNSBOX_PASS_Y_INV ? 1 : kind == DNSBOX_PASS_Y_FWD ? 2
-                 : kind == DNSBOX_PASS_Z_FWD ? 3 : -1;
-    // passes A, B, D: TMA unless scheduled on the cp.async kernel; E1: TMA when scheduled
+    // passes A, B, D: TMA unless scheduled on the cp.async or the SIMT kernel;
+    // E1: TMA when scheduled
     const bool want = si >= 0 && (si == 3 ? c->sched_tc[3] == 1 : c->sched_tc[si] == 0);
     if (allow_tc && tma_base && c->tc && c->tma_on && Ops<T>::has_tma(n) && want)
       return run_strided_tma(c, axis, inv, a, tma_base, tma_slots, kind);
   }
-  const bool tc = allow_tc && c->tc && Ops<T>::has_tc(n);
+  const bool simt = si >= 0 && si < 3 && c->sched_tc[si] == 2;
+  const bool tc = allow_tc && c->tc && Ops<T>::has_tc(n) && !simt;
   const int width = tc ? 4096 / n : TileCols<T>::v;
   if (a.kcol.a) {
     a.ntx_lo = (a.kcol.a + width - 1) / width;

@@ -6,7 +6,8 @@
 // transforms are the library's own kernels, and the choices that measured
 // differently across sizes are made by timing: for each of the tensor-core
 // strided passes (A inverse z, B inverse y, D forward y) the TMA-staged or
-// the cp.async-fed kernel, for the forward z pass (E1) the SIMT or the
+// the cp.async-fed tensor-core kernel or the FP32 SIMT kernel (the form's
+// accuracy bars hold for all three), for the forward z pass (E1) the SIMT or the
 // TMA-staged tensor-core kernel, and for the fused x pass the block kernel or
 // the warp kernel with its default or a four-blocks-per-SM register budget.  Each uniform candidate schedule advances a copy of the caller's
 // state for a few steps with pass timing on (CUDA events on the context's
@@ -125,8 +126,9 @@ extern "C" int dnsbox_get_schedule(const dnsbox_ctx *ctx, dnsbox_schedule *out) 
 
 extern "C" int dnsbox_set_schedule(dnsbox_ctx *ctx, const dnsbox_schedule *s) {
   if (!ctx || !s) return set_err(DNSBOX_ERR_ARG, "null argument");
-  for (int i = 0; i < 4; ++i)
-    if (s->tc_kernel[i] != 0 && s->tc_kernel[i] != 1) return set_err(DNSBOX_ERR_ARG, "tc_kernel must be 0 or 1");
+  for (int i = 0; i < 3; ++i)
+    if (s->tc_kernel[i] < 0 || s->tc_kernel[i] > 2) return set_err(DNSBOX_ERR_ARG, "tc_kernel[0..2] must be 0 .. 2");
+  if (s->tc_kernel[3] != 0 && s->tc_kernel[3] != 1) return set_err(DNSBOX_ERR_ARG, "tc_kernel[3] must be 0 or 1");
   if (s->x_kernel < 0 || s->x_kernel > 3) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0 .. 3");
   apply(ctx, *s);
   return DNSBOX_OK;
@@ -148,6 +150,8 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
     if (tz || ty) tc_opts.push_back(1);
     if (Ops<float>::has_tma(p.nz)) e1_opts.push_back(1);
   }
+  if (ctx->tc && !fp64 && (Ops<float>::has_tc(p.nz) || Ops<float>::has_tc(p.ny)))
+    tc_opts.push_back(2);   // the FP32 SIMT kernel
   std::vector<int> x_opts = {0};
   if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1, 3};
   const dnsbox_schedule saved_sched = current(ctx);

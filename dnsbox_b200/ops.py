@@ -35,6 +35,7 @@ from .grid import nspec as _nspec
 
 PRECISION = {"fp64": 0, "fp32": 1, "tc_split": 2}
 STEPPER = {"heun": 0, "ab2": 1, "semi_implicit": 2}
+TC_KERNELS = ("tma", "cp.async", "simt")   # per strided pass of the tensor-core form
 AB2_MODE = {"reference": 0, "standard": 1}
 SPECTRUM_MODE = {"mpi": 0, "single": 1}
 ADJ_PHAT = {"intent": 0, "literal": 1}
@@ -326,7 +327,7 @@ class Box:
     # ---------------------------------------------------------- kernel schedule
     @staticmethod
     def _sched_dict(sc):
-        return {"tc_kernel": ["tma" if v == 0 else "cp.async" for v in sc.tc_kernel[:3]],
+        return {"tc_kernel": [TC_KERNELS[v] for v in sc.tc_kernel[:3]],
                 "z_fwd_kernel": "tma" if sc.tc_kernel[3] else "simt",
                 "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-16w"}[sc.x_kernel], "tuned": bool(sc.tuned),
                 "ms_default": sc.ms_default, "ms_tuned": sc.ms_tuned}
@@ -337,9 +338,13 @@ class Box:
         return self._sched_dict(sc)
 
     def set_schedule(self, tc_kernel=(0, 0, 0), x_kernel=0, z_fwd_tma=False):
+        """tc_kernel: per pass A, B, D of the tensor-core form, 0 / "tma", 1 /
+        "cp.async" or 2 / "simt"; x_kernel 0 .. 3; z_fwd_tma: pass E1 on the
+        TMA tensor-core kernel."""
         sc = _lib.Schedule()
         for i in range(3):
-            sc.tc_kernel[i] = int(tc_kernel[i])
+            v = tc_kernel[i]
+            sc.tc_kernel[i] = TC_KERNELS.index(v) if isinstance(v, str) else int(v)
         sc.tc_kernel[3] = int(bool(z_fwd_tma))
         sc.x_kernel = int(x_kernel)
         _lib.check(self._lib.dnsbox_set_schedule(self._h, ctypes.byref(sc)))

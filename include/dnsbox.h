@@ -302,11 +302,13 @@ int dnsbox_ensemble_destroy(dnsbox_ensemble *ens);
 /* ---- kernel schedule and its autotuner ---------------------------------------
  * No reference counterpart as code: the reference leaves transform planning to
  * p3dfft / FFTW (variables.f90:154).  The schedule picks, per tensor-core
- * strided pass of the right-hand side, the TMA-staged or the cp.async-fed
- * kernel, and for the fused x pass the block or the warp kernel. */
+ * strided pass of the right-hand side of the tensor-core form, the TMA-staged
+ * or the cp.async-fed tensor-core kernel or the FP32 SIMT kernel, and for the
+ * fused x pass the block or the warp kernel. */
 typedef struct dnsbox_schedule {
   int32_t tc_kernel[4];   /* passes A (inverse z), B (inverse y), D (forward y): 0 TMA-staged tensor-core
-                             kernel, 1 cp.async-fed one; [3] pass E1 (forward z): 0 SIMT, 1 TMA-staged */
+                             kernel, 1 cp.async-fed one, 2 FP32 SIMT kernel; [3] pass E1 (forward z):
+                             0 SIMT, 1 TMA-staged tensor-core kernel */
   int32_t x_kernel;       /* fused x pass: 0 default for the size, 1 block kernel, 2 warp kernel,
                              3 warp kernel held to 128 registers (16 warps per SM) */
   int32_t tuned;          /* 1 when chosen by dnsbox_autotune */
