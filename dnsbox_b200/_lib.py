@@ -130,6 +130,7 @@ SIGNATURES = {
                                               ctypes.POINTER(_VP)]),
     "dnsbox_ensemble_run": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dnsbox_ensemble_destroy": (ctypes.c_int, [_VP]),
+    "dnsbox_ensemble_pruned": (ctypes.c_int, [_VP]),
     "dnsbox_profile_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dnsbox_sync": (ctypes.c_int, [_VP]),
     "dnsbox_get_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(Schedule)]),

@@ -556,14 +556,16 @@ __global__ void k_convert(const A *src, B *dst, long long n) {
 // Sets *flag when any component of a state (3 fields nh apart) is nonzero
 // (or not a number) at a mode outside the kept set of the pruning rule.
 template <typename C>
-__global__ void k_cut_check(const C *u, long long nh, int nxh, int ny, AxisKeep kx, AxisKeep ky, AxisKeep kz,
-                            int *flag) {
-  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nh;
+__global__ void k_cut_check(const C *u, long long nh, long long fstride, int nxh, int ny, AxisKeep kx, AxisKeep ky,
+                            AxisKeep kz, int *flag) {
+  // m runs over the modes of every box (fstride = nbatch * nh per component)
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < fstride;
        m += (long long)gridDim.x * blockDim.x) {
-    const int ix = (int)(m % nxh), iy = (int)((m / nxh) % ny), iz = (int)(m / ((long long)nxh * ny));
+    const long long mb = m % nh;
+    const int ix = (int)(mb % nxh), iy = (int)((mb / nxh) % ny), iz = (int)(mb / ((long long)nxh * ny));
     if (kx.keep(ix) && ky.keep(iy) && kz.keep(iz)) continue;
     for (int c = 0; c < 3; ++c) {
-      const C v = u[c * nh + m];
+      const C v = u[c * fstride + m];
       if (!(v.x == 0 && v.y == 0)) {
         *flag = 1;
         return;
@@ -1032,15 +1034,22 @@ template <typename T> static int step_once(dnsbox_ctx *c, void *uh) {
 
 // Decides whether this call may use the pruned passes: the state must vanish
 // exactly on the 2/3-rule cut set (the stepper then keeps it so).
-template <typename T> static int prune_decide(dnsbox_ctx *c, const void *uh) {
+// The check of every box of the context writes c->cut_flag (nonzero: some
+// box has content on the cut set); queued on c->stream.
+template <typename T> static int cut_check_async(dnsbox_ctx *c, const void *uh) {
   using C = typename CT<T>::type;
-  c->prune_now = 0;
-  if (!c->prune_ok || c->p.no_prune || c->nbatch > 1) return DNSBOX_OK;
   CK(cudaMemsetAsync(c->cut_flag, 0, sizeof(int), c->stream));
-  k_cut_check<C><<<grid_for((long long)c->nh), 256, 0, c->stream>>>(reinterpret_cast<const C *>(uh), (long long)c->nh,
-                                                                     c->nxh, c->p.ny, c->keep[0], c->keep[1],
-                                                                     c->keep[2], c->cut_flag);
+  k_cut_check<C><<<grid_for((long long)c->fstride), 256, 0, c->stream>>>(
+      reinterpret_cast<const C *>(uh), (long long)c->nh, (long long)c->fstride, c->nxh, c->p.ny, c->keep[0],
+      c->keep[1], c->keep[2], c->cut_flag);
   CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+template <typename T> static int prune_decide(dnsbox_ctx *c, const void *uh) {
+  c->prune_now = 0;
+  if (!c->prune_ok || c->p.no_prune) return DNSBOX_OK;
+  RET(cut_check_async<T>(c, uh));
   int *flag = reinterpret_cast<int *>(c->hstage + 62);
   CK(cudaMemcpyAsync(flag, c->cut_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1882,16 +1891,20 @@ extern "C" int dnsbox_diag_read(dnsbox_ctx *ctx, int nrecent, dnsbox_diag *host)
 extern "C" int dnsbox_batch_size(const dnsbox_ctx *ctx) { return ctx ? ctx->nbatch : -1; }
 
 // ------------------------------------------------------------------ ensemble
-// The graph is captured and replayed on a private stream (the legacy default
-// stream cannot be captured); events order it after the contexts' stream on
-// entry and make that stream wait for it on exit.
+// The graphs are captured and replayed on a private stream (the legacy
+// default stream cannot be captured); events order them after the contexts'
+// stream on entry and make that stream wait for them on exit.  Two graphs:
+// the full passes, and (when every context allows it) the pruned passes,
+// which a replay may use while every state vanishes on its 2/3-rule cut set
+// -- the steps keep it so, and dnsbox_ensemble_run checks it once per call.
 struct dnsbox_ensemble {
   std::vector<dnsbox_ctx *> ctxs;
   std::vector<void *> states;
   cudaStream_t user = 0, own = nullptr;
   cudaEvent_t in = nullptr, out = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph[2] = {nullptr, nullptr};   // [0] full passes, [1] pruned passes
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  int last_pruned = 0;
   // capture: one branch stream per context, forked from and joined into `own`,
   // so that the graph runs the contexts' steps as independent branches
   std::vector<cudaStream_t> branch;
@@ -1903,11 +1916,21 @@ static int step_any(dnsbox_ctx *c, void *u) {
   return c->fp64 ? step_once<double>(c, u) : step_once<float>(c, u);
 }
 
+static int prune_decide_any(dnsbox_ctx *c, void *u) {
+  return c->fp64 ? prune_decide<double>(c, u) : prune_decide<float>(c, u);
+}
+
+static int cut_check_any(dnsbox_ctx *c, void *u) {
+  return c->fp64 ? cut_check_async<double>(c, u) : cut_check_async<float>(c, u);
+}
+
 static void ensemble_free(dnsbox_ensemble *e) {
   if (!e) return;
   if (e->own) cudaStreamSynchronize(e->own);
-  if (e->exec) cudaGraphExecDestroy(e->exec);
-  if (e->graph) cudaGraphDestroy(e->graph);
+  for (int g = 0; g < 2; ++g) {
+    if (e->exec[g]) cudaGraphExecDestroy(e->exec[g]);
+    if (e->graph[g]) cudaGraphDestroy(e->graph[g]);
+  }
   if (e->in) cudaEventDestroy(e->in);
   if (e->out) cudaEventDestroy(e->out);
   if (e->fork) cudaEventDestroy(e->fork);
@@ -1916,8 +1939,42 @@ static void ensemble_free(dnsbox_ensemble *e) {
   for (cudaStream_t b : e->branch)
     if (b) cudaStreamDestroy(b);
   if (e->own) cudaStreamDestroy(e->own);
-  for (auto *c : e->ctxs) c->stream = e->user;
+  for (auto *c : e->ctxs) {
+    c->stream = e->user;
+    c->prune_now = 0;
+  }
   delete e;
+}
+
+// Captures one step of every context (pruned passes where `pruned`) into
+// e->graph[g] / e->exec[g].
+static int ensemble_capture(dnsbox_ensemble *e, int g, bool pruned) {
+  const int n = (int)e->ctxs.size();
+  for (auto *c : e->ctxs) {
+    c->stream = e->own;
+    c->prune_now = pruned ? 1 : 0;
+  }
+  CK(cudaStreamBeginCapture(e->own, cudaStreamCaptureModeThreadLocal));
+  int rc = DNSBOX_OK;
+  cudaError_t cerr = cudaEventRecord(e->fork, e->own);
+  for (int i = 0; i < n && rc == DNSBOX_OK && cerr == cudaSuccess; ++i) {
+    if ((cerr = cudaStreamWaitEvent(e->branch[i], e->fork, 0)) != cudaSuccess) break;
+    e->ctxs[i]->stream = e->branch[i];
+    rc = step_any(e->ctxs[i], e->states[i]);
+    if (rc == DNSBOX_OK && (cerr = cudaEventRecord(e->joins[i], e->branch[i])) == cudaSuccess)
+      cerr = cudaStreamWaitEvent(e->own, e->joins[i], 0);
+  }
+  if (rc == DNSBOX_OK && cerr != cudaSuccess) rc = set_err(DNSBOX_ERR_CUDA, "ensemble capture: %s", cudaGetErrorString(cerr));
+  const cudaError_t err = cudaStreamEndCapture(e->own, &e->graph[g]);
+  for (auto *c : e->ctxs) {
+    c->host_step -= 1;   // the captured step has not run
+    c->stream = e->user;
+    c->prune_now = 0;
+  }
+  if (rc != DNSBOX_OK) return rc;
+  if (err != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(err));
+  CK(cudaGraphInstantiate(&e->exec[g], e->graph[g], 0));
+  return DNSBOX_OK;
 }
 
 extern "C" int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *states, int n, dnsbox_ensemble **out) {
@@ -1939,6 +1996,10 @@ extern "C" int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *stat
     ensemble_free(e);
     return set_err(DNSBOX_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
   };
+  auto fail_rc = [&](int rc) {
+    ensemble_free(e);
+    return rc;
+  };
   cudaError_t err;
   if ((err = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking)) != cudaSuccess) return fail(err, "stream");
   if ((err = cudaEventCreateWithFlags(&e->in, cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
@@ -1950,61 +2011,63 @@ extern "C" int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *stat
     if ((err = cudaStreamCreateWithFlags(&e->branch[i], cudaStreamNonBlocking)) != cudaSuccess) return fail(err, "stream");
     if ((err = cudaEventCreateWithFlags(&e->joins[i], cudaEventDisableTiming)) != cudaSuccess) return fail(err, "event");
   }
-  for (auto *c : e->ctxs) {
-    c->stream = e->user;
-    c->prune_now = 0;   // the captured step uses the full passes (no per-call state check inside a graph)
-  }
+  for (auto *c : e->ctxs) c->stream = e->user;
   // one eager step on the contexts' stream, so the captured step is a steady
   // one (the first step's forced dt update and the AB2 start-up are host-side
-  // decisions)
+  // decisions); it decides pruning per context as dnsbox_step does
+  bool all_pruned = true;
   for (int i = 0; i < n; ++i) {
-    const int rc = step_any(e->ctxs[i], e->states[i]);
-    if (rc != DNSBOX_OK) {
-      ensemble_free(e);
-      return rc;
-    }
+    int rc = prune_decide_any(e->ctxs[i], e->states[i]);
+    if (rc == DNSBOX_OK) rc = step_any(e->ctxs[i], e->states[i]);
+    if (rc != DNSBOX_OK) return fail_rc(rc);
+    all_pruned = all_pruned && e->ctxs[i]->prune_now;
+    e->ctxs[i]->prune_now = 0;
   }
   if ((err = cudaEventRecord(e->in, e->user)) != cudaSuccess) return fail(err, "event record");
   if ((err = cudaStreamWaitEvent(e->own, e->in, 0)) != cudaSuccess) return fail(err, "stream wait");
-  for (auto *c : e->ctxs) c->stream = e->own;
-  if ((err = cudaStreamBeginCapture(e->own, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
-    return fail(err, "cudaStreamBeginCapture");
-  int rc = DNSBOX_OK;
-  cudaError_t cerr = cudaEventRecord(e->fork, e->own);
-  for (int i = 0; i < n && rc == DNSBOX_OK && cerr == cudaSuccess; ++i) {
-    if ((cerr = cudaStreamWaitEvent(e->branch[i], e->fork, 0)) != cudaSuccess) break;
-    e->ctxs[i]->stream = e->branch[i];
-    rc = step_any(e->ctxs[i], e->states[i]);
-    if (rc == DNSBOX_OK && (cerr = cudaEventRecord(e->joins[i], e->branch[i])) == cudaSuccess)
-      cerr = cudaStreamWaitEvent(e->own, e->joins[i], 0);
-  }
-  if (rc == DNSBOX_OK && cerr != cudaSuccess) rc = set_err(DNSBOX_ERR_CUDA, "ensemble capture: %s", cudaGetErrorString(cerr));
-  err = cudaStreamEndCapture(e->own, &e->graph);
-  for (auto *c : e->ctxs) c->host_step -= 1;   // the captured step has not run
-  if (rc != DNSBOX_OK) {
-    ensemble_free(e);
-    return rc;
-  }
-  if (err != cudaSuccess) return fail(err, "cudaStreamEndCapture");
-  if ((err = cudaGraphInstantiate(&e->exec, e->graph, 0)) != cudaSuccess) return fail(err, "cudaGraphInstantiate");
-  for (auto *c : e->ctxs) c->stream = e->user;
+  int rc = ensemble_capture(e, 0, false);
+  if (rc == DNSBOX_OK && all_pruned) rc = ensemble_capture(e, 1, true);
+  if (rc != DNSBOX_OK) return fail_rc(rc);
   *out = e;
   return DNSBOX_OK;
 }
 
+// The pruned graph when every state still vanishes on its cut set (one check
+// kernel per context and one 4-byte read per call), else the full graph.
 extern "C" int dnsbox_ensemble_run(dnsbox_ensemble *e, int nsteps) {
   if (!e || nsteps < 0) return set_err(DNSBOX_ERR_ARG, "invalid argument");
   CK(cudaSetDevice(e->ctxs[0]->p.device));
+  int g = 0;
+  if (e->exec[1] && nsteps > 0) {
+    const int n = (int)e->ctxs.size();
+    for (int i = 0; i < n; ++i) {
+      dnsbox_ctx *c = e->ctxs[i];
+      RET(cut_check_any(c, e->states[i]));   // on the user stream, after the caller's work
+    }
+    // each context's check writes its own flag; they are folded on the host
+    int clean = 1;
+    for (int i = 0; i < n; ++i) {
+      dnsbox_ctx *c = e->ctxs[i];
+      int *flag = reinterpret_cast<int *>(c->hstage + 62);
+      CK(cudaMemcpyAsync(flag, c->cut_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(e->user));
+    for (int i = 0; i < n; ++i) clean = clean && *reinterpret_cast<int *>(e->ctxs[i]->hstage + 62) == 0;
+    g = clean ? 1 : 0;
+  }
+  e->last_pruned = g;
   CK(cudaEventRecord(e->in, e->user));
   CK(cudaStreamWaitEvent(e->own, e->in, 0));
   for (int i = 0; i < nsteps; ++i) {
-    CK(cudaGraphLaunch(e->exec, e->own));
+    CK(cudaGraphLaunch(e->exec[g], e->own));
     for (auto *c : e->ctxs) c->host_step += 1;
   }
   CK(cudaEventRecord(e->out, e->own));
   CK(cudaStreamWaitEvent(e->user, e->out, 0));
   return DNSBOX_OK;
 }
+
+extern "C" int dnsbox_ensemble_pruned(const dnsbox_ensemble *e) { return e ? e->last_pruned : -1; }
 
 extern "C" int dnsbox_ensemble_destroy(dnsbox_ensemble *e) {
   if (!e) return DNSBOX_OK;

@@ -33,7 +33,7 @@ Key key_of(const dnsbox_ctx *c) {
 }
 
 void apply(dnsbox_ctx *c, const dnsbox_schedule &s) {
-  for (int i = 0; i < 4; ++i) c->sched_tc[i] = s.tc_kernel[i] ? 1 : 0;
+  for (int i = 0; i < 4; ++i) c->sched_tc[i] = s.tc_kernel[i];   // checked by dnsbox_set_schedule
   c->sched_x = s.x_kernel;
 }
 

@@ -41,6 +41,10 @@ class Ensemble:
     def run(self, nsteps: int):
         _lib.check(self._lib.dnsbox_ensemble_run(self._h, int(nsteps)))
 
+    def pruned(self) -> bool:
+        """Whether the last run replayed the pruned passes."""
+        return self._lib.dnsbox_ensemble_pruned(self._h) == 1
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             self._lib.dnsbox_ensemble_destroy(self._h)

@@ -293,10 +293,17 @@ int dnsbox_diag_read(dnsbox_ctx *ctx, int nrecent, dnsbox_diag *diag_host);
  * first context's stream (all contexts are switched to it), each context's
  * step an independent branch of the graph (the branches may run
  * concurrently).  Every state is first advanced by one step eagerly, so the
- * captured step is a steady one. */
+ * captured step is a steady one.  When every state vanishes on its 2/3-rule
+ * cut set, a second graph of the pruned passes (as dnsbox_step uses them) is
+ * captured beside the full one. */
 int dnsbox_ensemble_create(dnsbox_ctx *const *ctxs, void *const *states_dev, int n, dnsbox_ensemble **out);
-/* Replays the captured step nsteps times (asynchronous). */
+/* Replays the captured step nsteps times: the pruned graph when it exists and
+ * every state still vanishes on its cut set (checked once per call, which
+ * waits for the work queued before it on the first context's stream), else
+ * the full graph.  The replays themselves are asynchronous. */
 int dnsbox_ensemble_run(dnsbox_ensemble *ens, int nsteps);
+/* 1 when the last dnsbox_ensemble_run replayed the pruned graph. */
+int dnsbox_ensemble_pruned(const dnsbox_ensemble *ens);
 int dnsbox_ensemble_destroy(dnsbox_ensemble *ens);
 
 /* ---- kernel schedule and its autotuner ---------------------------------------

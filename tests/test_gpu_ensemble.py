@@ -145,3 +145,64 @@ def test_sharded_config2_equals_unsharded():
                 seen.add(gi)
         e.close()
     assert seen == set(range(96))
+
+
+@pytest.mark.parametrize("n,prec", [(32, "fp64"), (48, "fp32"), (96, "fp32"), (128, "tc_split")])
+def test_batched_pruned_passes_equal_full_passes(n, prec):
+    """A batched context prunes the 2/3-rule zeros as a single box does: with
+    per-box CFL control and forcing, the pruned steps equal the full ones bit
+    for bit (states and step records)."""
+    from dnsbox_b200.ops import Box
+    nb, ns = 3, 4
+    nus = [2e-3, 4e-3, 8e-3]
+    kw = dict(kCutOff=2.5, Pin=0.1, bandlim=True, courant_min=0.5, courant_max=0.5, dt_max=1e-2, dt=1e-3)
+    out = []
+    for prune in (True, False):
+        box = Box(n, nbatch=nb, nu=nus[0], precision=prec, prune=prune, **kw)
+        box.set_batch_nu(nus)
+        u = box.zeros()
+        for b in range(nb):
+            u[:, b] = box.from_numpy(ic.random_field(n, seed=20 + b, k0=3.0))
+        recs = box.step(u, ns)
+        out.append((u.cpu(), recs, box.step_pruned()))
+        box.close()
+    (up, rp, pp), (uf, rf, pf) = out
+    assert pp and not pf
+    assert torch.equal(up, uf)
+    for i in range(ns):
+        for b in range(nb):
+            assert rp[i][b]["ekin"] == rf[i][b]["ekin"] and rp[i][b]["dt"] == rf[i][b]["dt"]
+
+
+def test_ensemble_pruned_graph_and_full_fallback():
+    """The ensemble replays the pruned graph while every state vanishes on its
+    cut set, and the full graph once a state has content there; both equal the
+    eager steps of the same contexts bit for bit."""
+    from dnsbox_b200.ensemble import Ensemble, config2_nus, make_group
+    spec = [(16, 2), (32, 3)]
+    groups, eager = [], []
+    for gi, (n, nb) in enumerate(spec):
+        nus = config2_nus(nb, seed=2000 + n)
+        groups.append(make_group(n, nb, seeds=range(10 * gi, 10 * gi + nb), nus=nus, dt=1e-3))
+        eager.append(make_group(n, nb, seeds=range(10 * gi, 10 * gi + nb), nus=nus, dt=1e-3))
+    ens = Ensemble(groups)
+    ens.run(2)
+    assert ens.pruned()
+    for box, u in eager:
+        box.step(u, 3, diag=False)
+        assert box.step_pruned()
+    torch.cuda.synchronize()
+    for (gb, gu), (eb, eu) in zip(groups, eager):
+        assert torch.equal(gu, eu)
+    # content on the cut set of one box (kz = 12 of n = 32 lies past the 2/3 cut)
+    for _, u in (groups[1], eager[1]):
+        u[0, 1, 12, 0, 0] = 1e-3
+    ens.run(2)
+    assert not ens.pruned()
+    eager[1][0].step(eager[1][1], 2, diag=False)
+    assert not eager[1][0].step_pruned()
+    eager[0][0].step(eager[0][1], 2, diag=False)
+    torch.cuda.synchronize()
+    for (gb, gu), (eb, eu) in zip(groups, eager):
+        assert torch.equal(gu, eu)
+    ens.close()
