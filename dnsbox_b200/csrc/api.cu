@@ -890,7 +890,7 @@ int run_strided_tma(dnsbox_ctx *c, int axis, bool inv, const StridedArgs<float> 
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_err(DNSBOX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   Prof pr(c, kind);
-  CK(Ops<float>::strided_tma(n, t, inv, c->adft, c->tc_status, 2 * c->nsm, c->stream));   // two CTAs per SM
+  CK(Ops<float>::strided_tma(n, t, inv, c->adft, c->tc_status, c->tma_ctas_per_sm * c->nsm, c->stream));
   return DNSBOX_OK;
 }
 
@@ -1134,6 +1134,9 @@ static int alloc_dft64(dnsbox_ctx *c) {
   const char *br = getenv("DNSBOX_TMA_BOX_ROWS");
   const int brv = br ? atoi(br) : 32;
   c->tma_box_rows = (brv == 8 || brv == 16 || brv == 32 || brv == 64) ? brv : 32;
+  // resident CTAs per SM of the TMA passes (1 or 2; DNSBOX_TMA_CTAS_PER_SM)
+  const char *cps = getenv("DNSBOX_TMA_CTAS_PER_SM");
+  c->tma_ctas_per_sm = (cps && atoi(cps) == 1) ? 1 : 2;
   return DNSBOX_OK;
 }
 

@@ -34,7 +34,7 @@ DNSBOX_PLAN(24, 24, 8, 3)
 DNSBOX_PLAN(32, 8, 8, 4)
 DNSBOX_PLAN(48, 12, 4, 4, 3)
 DNSBOX_PLAN(64, 8, 8, 8)
-DNSBOX_PLAN(96, 24, 8, 4, 3)
+DNSBOX_PLAN(96, 12, 4, 4, 2, 3)
 DNSBOX_PLAN(128, 16, 16, 8)
 DNSBOX_PLAN(192, 24, 8, 8, 3)
 DNSBOX_PLAN(256, 16, 16, 16)

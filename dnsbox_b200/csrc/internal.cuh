@@ -100,6 +100,7 @@ struct dnsbox_ctx {
   int nsm = 0;                           // streaming multiprocessors of the device
   int tma_on = 0;                        // the right-hand side uses the TMA-staged tensor-core passes
   int tma_box_rows = 32;                 // rows per TMA box of their staged tiles
+  int tma_ctas_per_sm = 2;               // resident CTAs per SM of the TMA passes
   // kernel schedule of the right-hand side (chosen by dnsbox_autotune, or the
   // defaults): passes A, B, D 0 = TMA-staged tensor-core kernel, 1 = the
   // cp.async-fed one; pass E1 0 = SIMT, 1 = TMA-staged tensor-core kernel;
