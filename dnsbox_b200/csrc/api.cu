@@ -906,7 +906,9 @@ int tc_check(dnsbox_ctx *c) {
   if (*flag) {
     CK(cudaMemsetAsync(c->tc_status, 0, sizeof(int), c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    return set_err(DNSBOX_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core MMA or staged copy)");
+    const int code = *flag;
+    return set_err(DNSBOX_ERR_TIMEOUT, "a bounded device wait gave up (%s)",
+                   code == 2 ? "staged TMA copy" : code == 3 ? "tensor-core MMA of a TMA pass" : "tensor-core MMA");
   }
   return DNSBOX_OK;
 }
@@ -1134,9 +1136,11 @@ static int alloc_dft64(dnsbox_ctx *c) {
   const char *br = getenv("DNSBOX_TMA_BOX_ROWS");
   const int brv = br ? atoi(br) : 32;
   c->tma_box_rows = (brv == 8 || brv == 16 || brv == 32 || brv == 64) ? brv : 32;
-  // resident CTAs per SM of the TMA passes (1 or 2; DNSBOX_TMA_CTAS_PER_SM)
+  // resident CTAs per SM of the TMA passes (DNSBOX_TMA_CTAS_PER_SM = 2 for
+  // two; one by default: with two per SM, repeated 256^3 pruned steps gave an
+  // occasional wrong result that one CTA per SM never showed)
   const char *cps = getenv("DNSBOX_TMA_CTAS_PER_SM");
-  c->tma_ctas_per_sm = (cps && atoi(cps) == 1) ? 1 : 2;
+  c->tma_ctas_per_sm = (cps && atoi(cps) == 2) ? 2 : 1;
   return DNSBOX_OK;
 }
 

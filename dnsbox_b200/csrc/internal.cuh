@@ -100,12 +100,12 @@ struct dnsbox_ctx {
   int nsm = 0;                           // streaming multiprocessors of the device
   int tma_on = 0;                        // the right-hand side uses the TMA-staged tensor-core passes
   int tma_box_rows = 32;                 // rows per TMA box of their staged tiles
-  int tma_ctas_per_sm = 2;               // resident CTAs per SM of the TMA passes
+  int tma_ctas_per_sm = 1;               // resident CTAs per SM of the TMA passes
   // kernel schedule of the right-hand side (chosen by dnsbox_autotune, or the
   // defaults): passes A, B, D 0 = TMA-staged tensor-core kernel, 1 = the
   // cp.async-fed one; pass E1 0 = SIMT, 1 = TMA-staged tensor-core kernel;
   // x pass 0 = default, 1 = block, 2 = warp, 3 = warp with 128 registers
-  int sched_tc[4] = {0, 0, 0, 0};
+  int sched_tc[4] = {1, 1, 1, 0};         // passes A, B, D: 0 TMA, 1 cp.async, 2 SIMT; E1: 0 SIMT, 1 TMA
   int sched_x = 0;
   char *adj = nullptr;                   // adjoint arena
   size_t adj_bytes = 0;

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, TmaPlan<N>::CTAS_PER_SM)
   bool aborted = false;
   auto wait_load = [&]() {   // thread 0
     if (tc::mbar_wait_bounded(&full, (uint32_t)loads_seen & 1u, kTmaWaitLimit)) ++loads_seen;
-    else abort_s = 1;
+    else abort_s = 2;   // the status code says which wait gave up: 2 staged copy, 3 MMA
   };
   for (int i = 0; i <= my_n; ++i) {
     const int par = i & 1;
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, TmaPlan<N>::CTAS_PER_SM)
       }
       if (t == 0 && i > 0) {   // MMA(i - 1) done: the accumulator and B are free
         if (tc::mbar_wait_bounded(&mmab, (uint32_t)(i - 1) & 1u, kTmaWaitLimit)) ++mma_seen;
-        else abort_s = 1;
+        else abort_s = 3;
       }
       tc::fence_before_sync();
       __syncthreads();   // B: column maxima complete, MMA(i - 1) complete
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, TmaPlan<N>::CTAS_PER_SM)
       // after the last tile: wait for its MMAs before draining
       if (t == 0 && i > 0) {
         if (tc::mbar_wait_bounded(&mmab, (uint32_t)(i - 1) & 1u, kTmaWaitLimit)) ++mma_seen;
-        else abort_s = 1;
+        else abort_s = 3;
       }
       tc::fence_before_sync();
       __syncthreads();
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(TmaPlan<N>::THREADS, TmaPlan<N>::CTAS_PER_SM)
     // wait (bounded) for the copies and MMAs still in flight before TMEM is freed
     for (int k = loads_seen; k < loads_issued; ++k) tc::mbar_wait_bounded(&full, (uint32_t)k & 1u, kTmaWaitLimit);
     for (int k = mma_seen; k < mma_issued; ++k) tc::mbar_wait_bounded(&mmab, (uint32_t)k & 1u, kTmaWaitLimit);
-    atomicExch(status, 1);
+    atomicExch(status, abort_s);
   }
   tc::fence_before_sync();
   __syncthreads();

@@ -5,11 +5,13 @@
 // (variables.f90:154, p3dfft_setup measuring FFTW plans).  Here the
 // transforms are the library's own kernels, and the choices that measured
 // differently across sizes are made by timing: for each of the tensor-core
-// strided passes (A inverse z, B inverse y, D forward y) the TMA-staged or
-// the cp.async-fed tensor-core kernel or the FP32 SIMT kernel (the form's
-// accuracy bars hold for all three), for the forward z pass (E1) the SIMT or the
-// TMA-staged tensor-core kernel, and for the fused x pass the block kernel or
-// the warp kernel with its default or a four-blocks-per-SM register budget.  Each uniform candidate schedule advances a copy of the caller's
+// strided passes (A inverse z, B inverse y, D forward y) of the tensor-core
+// form the cp.async-fed tensor-core kernel or the FP32 SIMT kernel (the
+// form's accuracy bars hold for both), and for the fused x pass the block
+// kernel or the warp kernel with its default or a four-blocks-per-SM
+// register budget.  The TMA-staged tensor-core kernels (passes A, B, D and
+// E1) stay selectable by dnsbox_set_schedule but are not candidates: they
+// measured slower than both others at every size.  Each uniform candidate schedule advances a copy of the caller's
 // state for a few steps with pass timing on (CUDA events on the context's
 // stream); every pass keeps its fastest kernel; the chosen schedule is timed
 // once more.  The context's clock, time step and step history are restored,
@@ -143,13 +145,9 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
   const dnsbox_params &p = ctx->p;
   const bool fp64 = ctx->fp64;
   // candidate kernels
-  std::vector<int> tc_opts = {0}, e1_opts = {0};
-  if (ctx->tc && !fp64 && ctx->tma_on) {
-    const bool tz = Ops<float>::has_tma(p.nz) && Ops<float>::has_tc(p.nz);
-    const bool ty = Ops<float>::has_tma(p.ny) && Ops<float>::has_tc(p.ny);
-    if (tz || ty) tc_opts.push_back(1);
-    if (Ops<float>::has_tma(p.nz)) e1_opts.push_back(1);
-  }
+  // the TMA-staged kernels are not candidates: slower than both others at
+  // every measured size (and one CTA per SM by default)
+  std::vector<int> tc_opts = {1}, e1_opts = {0};
   if (ctx->tc && !fp64 && (Ops<float>::has_tc(p.nz) || Ops<float>::has_tc(p.ny)))
     tc_opts.push_back(2);   // the FP32 SIMT kernel
   std::vector<int> x_opts = {0};
@@ -205,7 +203,7 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
         if (r.s.x_kernel == xv) sum += r.pass[DNSBOX_PASS_X_NL], ++n;
       if (n && sum / n < bestx) bestx = sum / n, best.x_kernel = xv;
     }
-    best.ms_default = runs.empty() ? 0.0 : runs[0].step;   // TMA passes, default x kernel
+    best.ms_default = runs.empty() ? 0.0 : runs[0].step;   // cp.async passes, default x kernel
     double pass_tmp[DNSBOX_NPASS];
     rc = trial(ctx, best, uh, scratch, bytes, sv, nsteps, pass_tmp, &best.ms_tuned);
     // keep the default when the combination measures slower than it

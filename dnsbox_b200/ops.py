@@ -326,8 +326,8 @@ class Box:
 
     # ---------------------------------------------------------- kernel schedule
     @staticmethod
-    def _sched_dict(sc):
-        return {"tc_kernel": [TC_KERNELS[v] for v in sc.tc_kernel[:3]],
+    def _sched_dict(sc, tc=True):
+        return {"tc_kernel": [TC_KERNELS[v] if tc else "simt" for v in sc.tc_kernel[:3]],
                 "z_fwd_kernel": "tma" if sc.tc_kernel[3] else "simt",
                 "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-16w"}[sc.x_kernel], "tuned": bool(sc.tuned),
                 "ms_default": sc.ms_default, "ms_tuned": sc.ms_tuned}
@@ -335,7 +335,7 @@ class Box:
     def schedule(self) -> dict:
         sc = _lib.Schedule()
         _lib.check(self._lib.dnsbox_get_schedule(self._h, ctypes.byref(sc)))
-        return self._sched_dict(sc)
+        return self._sched_dict(sc, self.precision == "tc_split")
 
     def set_schedule(self, tc_kernel=(0, 0, 0), x_kernel=0, z_fwd_tma=False):
         """tc_kernel: per pass A, B, D of the tensor-core form, 0 / "tma", 1 /
@@ -356,7 +356,7 @@ class Box:
         self._sync_stream()
         sc = _lib.Schedule()
         _lib.check(self._lib.dnsbox_autotune(self._h, _ptr(uh), int(nsteps), ctypes.byref(sc)))
-        return self._sched_dict(sc)
+        return self._sched_dict(sc, self.precision == "tc_split")
 
     def implicit_iterations(self) -> int:
         """Fixed-point iterations of the last semi-implicit step."""
