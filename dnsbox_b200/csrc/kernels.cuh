@@ -419,23 +419,21 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
 // sequence runs the two-stage radix-16 plan on 16 threads, so a warp
 // transforms two sequences at once with one shared-memory exchange each; at
 // N = 512 a sequence runs the three-stage plan on all 32 threads.
-// NARROW (N = 256): every sequence on all 32 threads with the 8-value plan
-// (one sequence per round, half the registers of the 16-value plan).
-template <typename T, int N, bool NARROW = false> struct XlineWarp {
+template <typename T, int N> struct XlineWarp {
   static constexpr bool on = N == 256 || N == 512;
   static constexpr int wpb = sizeof(T) == 8 ? (N >= 512 ? 1 : 2) : (N >= 1024 ? 1 : (N >= 512 ? 2 : 4));
-  using Plan = typename std::conditional<N == 256 && !NARROW, FftPlan<256>, WarpPlan<N>>::type;
+  using Plan = typename std::conditional<N == 256, FftPlan<256>, WarpPlan<N>>::type;
 };
 
 // Second half of the warp-granular fused x pass for one line pair (la, lb):
 // the inverse transforms are in the warp's tile s (column-major, skewed);
 // (omega x u) * s, the three forward transforms, the unpacking into the
 // output half lines and the CFL maxima of the pair.
-template <typename T, int N, bool NARROW = false>
+template <typename T, int N>
 __device__ __forceinline__ void xline_w_tail(typename CT<T>::type *s, const XlineNLArgs<T> &a, long long la,
                                              long long lb, int lane, long long pout) {
   using C = typename CT<T>::type;
-  using PL = typename XlineWarp<T, N, NARROW>::Plan;
+  using PL = typename XlineWarp<T, N>::Plan;
   using EN = FftEndsP<PL>;
   using AD = AddrSkew<PL::R[0]>;
   constexpr int E = PL::E;
@@ -538,14 +536,11 @@ __device__ __forceinline__ void xline_w_tail(typename CT<T>::type *s, const Xlin
   }
 }
 
-// MINB > 0 asks the register allocator for MINB resident blocks per SM (at
-// most 128 registers for the FP32 N = 256 blocks of four warps: 16 warps per
-// SM instead of the 12 that its default allocation leaves room for).
-template <typename T, int N, int MINB = 0, bool NARROW = false>
-__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb, MINB)
+template <typename T, int N>
+__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
     k_xline_nl_w(const __grid_constant__ XlineNLArgs<T> a) {
   using C = typename CT<T>::type;
-  using PL = typename XlineWarp<T, N, NARROW>::Plan;
+  using PL = typename XlineWarp<T, N>::Plan;
   using EN = FftEndsP<PL>;
   using AD = AddrSkew<PL::R[0]>;
   constexpr int E = PL::E;
@@ -597,7 +592,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb, MINB)
 #pragma unroll
     for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
   }
-  xline_w_tail<T, N, NARROW>(s, a, la, lb, lane, pout);
+  xline_w_tail<T, N>(s, a, la, lb, lane, pout);
 }
 
 // Plain x-line transforms of nf fields (blockIdx.y = field).

@@ -143,18 +143,6 @@ template <typename T, int N>
 cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaStream_t st) {
   using C = typename CT<T>::type;
   if constexpr (XlineWarp<T, N>::on) {
-    if (variant == 4 && N == 256) {
-      // one sequence per round on all 32 threads (8-value plan)
-      constexpr int WPB = XlineWarp<T, N, true>::wpb;
-      constexpr int LDC = N + N / XlineWarp<T, N, true>::Plan::R[0];
-      const size_t smem = (size_t)WPB * 6 * LDC * sizeof(C);
-      cudaError_t e;
-      const long long pairs = (a.nlines + 1) / 2;
-      const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
-      if ((e = set_smem(k_xline_nl_w<T, N, 0, true>, smem)) != cudaSuccess) return e;
-      k_xline_nl_w<T, N, 0, true><<<nb, 32 * WPB, smem, st>>>(a);
-      return cudaGetLastError();
-    }
     if (variant != 1) {
     // warp-granular kernel: one warp per line pair
     constexpr int WPB = XlineWarp<T, N>::wpb;
@@ -163,23 +151,8 @@ cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaS
     cudaError_t e;
     const long long pairs = (a.nlines + 1) / 2;
     const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
-    if (variant == 3) {
-      if ((e = set_smem(k_xline_nl_w<T, N, 4>, smem)) != cudaSuccess) return e;
-      k_xline_nl_w<T, N, 4><<<nb, 32 * WPB, smem, st>>>(a);
-    } else if (variant == 4) {
-      // persistent: the resident blocks of every SM, striding over the pairs
-      auto kern = k_xline_nl_w<T, N, 0, true>;
-      if ((e = set_smem(kern, smem)) != cudaSuccess) return e;
-      int dev = 0, nsm = 0, per_sm = 0;
-      if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-      if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * WPB, smem)) != cudaSuccess) return e;
-      const unsigned cap = (unsigned)(per_sm > 0 ? per_sm : 1) * (unsigned)nsm;
-      kern<<<nb < cap ? nb : cap, 32 * WPB, smem, st>>>(a);
-    } else {
-      if ((e = set_smem(k_xline_nl_w<T, N>, smem)) != cudaSuccess) return e;
-      k_xline_nl_w<T, N><<<nb, 32 * WPB, smem, st>>>(a);
-    }
+    if ((e = set_smem(k_xline_nl_w<T, N>, smem)) != cudaSuccess) return e;
+    k_xline_nl_w<T, N><<<nb, 32 * WPB, smem, st>>>(a);
     return cudaGetLastError();
     }
   }

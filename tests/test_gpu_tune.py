@@ -19,7 +19,7 @@ def rel(a, b):
 @pytest.mark.parametrize("prec", ["tc_split", "fp32"])
 def test_every_schedule_matches_the_oracle(prec):
     from dnsbox_b200.ops import Box
-    n = 256   # the size with every x-pass kernel
+    n = 256   # the size with all four x-pass kernels
     kw = dict(nu=2e-3, kCutOff=2.5, Pin=0.1, bandlim=True)
     uh = ic.random_field(n, seed=12, k0=3.0)
     want = O.rhs_nonlinear(O.Grid(O.Params(nx=n, ny=n, nz=n, **kw)), uh)
@@ -28,7 +28,7 @@ def test_every_schedule_matches_the_oracle(prec):
     # each kernel on each of passes A, B, D (TMA 0, cp.async 1, SIMT 2)
     tcs = [(0, 0, 0), (1, 1, 1), (2, 2, 2), (0, 1, 2), (2, 0, 1), (1, 2, 0)] if prec == "tc_split" else [(0, 0, 0)]
     for tc in tcs:
-        for xk in (0, 1, 2, 3, 4):
+        for xk in (0, 1, 2):
             for zt in ((False, True) if prec == "tc_split" else (False,)):
                 b.set_schedule(tc, xk, zt)
                 got, _ = b.rhs_nonlinear(u)
