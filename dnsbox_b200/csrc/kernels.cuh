@@ -175,6 +175,18 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
   const int kx = strided_col(a, kx0 + col);
   const bool valid = act && kx < a.ncols && a.kcol.keep(kx);
   const long long base = (long long)other * a.otherstride + kx + (long long)blockIdx.y * a.bstride;
+  // the job's row multipliers T(b k_row(n)) (ks == 1), once per block
+  // instead of once per element: the same values as apply_mult forms
+  __shared__ T bks[2][N];
+  const bool mult1 = !(J.a1 == 1.0 && J.b1 == 0.0);
+  if ((mult1 && J.ks1 == 1) || (J.in2 && J.ks2 == 1)) {
+    for (int n = threadIdx.x; n < N; n += blockDim.x) {
+      const double k = k_full(n, N, a.alpha_row);
+      bks[0][n] = T(J.b1 * k);
+      bks[1][n] = T(J.b2 * k);
+    }
+    __syncthreads();
+  }
   C v[E];
   if (valid) {
     // all E loads of the first stage are independent and issued together
@@ -185,19 +197,22 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
     // wavenumber of the column (0) or of the tile's other-axis index (2)
     const double kcol = k_half(kx, a.nx, a.alpha_x);
     const double koth = a.n_other ? k_full(other, a.n_other, a.alpha_other) : 0.0;
-    if (!(J.a1 == 1.0 && J.b1 == 0.0)) {
-      const double kc = J.ks1 == 2 ? koth : kcol;
+    if (mult1) {
+      const T aa = T(J.a1), bkc = T(J.b1 * (J.ks1 == 2 ? koth : kcol));
 #pragma unroll
-      for (int i = 0; i < E; ++i)
-        v[i] = apply_mult<T>(v[i], J.a1, J.b1, J.ks1 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc);
+      for (int i = 0; i < E; ++i) {
+        const T bk = J.ks1 == 1 ? bks[0][EN::in_row(p, i)] : bkc;
+        v[i] = mkc<C>(v[i].x * aa - v[i].y * bk, v[i].y * aa + v[i].x * bk);
+      }
     }
     if (J.in2) {
       const C *in2 = J.in2 + base;
-      const double kc = J.ks2 == 2 ? koth : kcol;
+      const T aa = T(J.a2), bkc = T(J.b2 * (J.ks2 == 2 ? koth : kcol));
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const C w = a.krin.keep(EN::in_row(p, i)) ? in2[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
-        v[i] = cadd(v[i], apply_mult<T>(w, J.a2, J.b2, J.ks2 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc));
+        const T bk = J.ks2 == 1 ? bks[1][EN::in_row(p, i)] : bkc;
+        v[i] = cadd(v[i], mkc<C>(w.x * aa - w.y * bk, w.y * aa + w.x * bk));
       }
     }
   } else {
