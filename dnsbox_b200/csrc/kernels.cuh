@@ -611,6 +611,103 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
 }
 
 // Plain x-line transforms of nf fields (blockIdx.y = field).
+// 16- and 8-byte asynchronous global -> shared copies (cp.async), commit and
+// wait for all but the newest group.
+__device__ __forceinline__ void cpa16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// The warp kernel with its inputs staged by cp.async: the two half lines of
+// each sequence of round r + 1 are copied (16-byte chunks of the kept prefix,
+// plus the lone Nyquist element when pruned) into that sequence's own tile
+// column while round r transforms, then read from shared memory with the
+// Hermitian mirror.  Every half-line element is fetched from global memory
+// once, in whole coalesced chunks, and no registers hold the next round's
+// inputs.  Needs 16-byte aligned input rows (even pitch in FP32).
+template <typename T, int N>
+__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
+    k_xline_nl_ws(const __grid_constant__ XlineNLArgs<T> a) {
+  using C = typename CT<T>::type;
+  using PL = typename XlineWarp<T, N>::Plan;
+  using EN = FftEndsP<PL>;
+  using AD = AddrSkew<PL::R[0]>;
+  constexpr int E = PL::E;
+  constexpr int P = N / E;                       // threads per sequence
+  constexpr int SPW = 32 / P;                    // sequences a warp transforms at once
+  constexpr int RI = 6 / SPW;                    // rounds of inverse transforms
+  constexpr int LDC = N + N / PL::R[0];          // column length with the skew
+  constexpr int WPB = XlineWarp<T, N>::wpb;
+  constexpr int H = N / 2 + 1;
+  constexpr int CPC = 16 / (int)sizeof(C);       // complex values per 16-byte chunk
+  constexpr int HS = (H + CPC - 1) / CPC * CPC;  // staged half-line length
+  static_assert(2 * HS <= LDC, "both staged half lines of a sequence fit its column");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C *s = reinterpret_cast<C *>(smem_raw) + (size_t)warp * 6 * LDC;
+  const long long la = 2 * ((long long)blockIdx.x * WPB + warp), lb = la + 1;
+  if (la >= a.nlines) return;
+  const C *f1s[6] = {a.U, a.U, a.W, a.OX, a.OX, a.OZ};
+  const C *f2s[6] = {a.V, a.V, a.W, a.OY, a.OY, a.OZ};
+  const long long l1s[6] = {la, lb, la, la, lb, la};
+  const long long l2s[6] = {la, lb, lb, la, lb, lb};
+  const int p = lane % P, h = lane / P;   // position in the sequence, sequence slot
+  const long long pin = a.pin ? a.pin : a.nxh, pout = a.pout ? a.pout : a.nxh;
+  // the kept prefix [0, L) of a half line, and the Nyquist element N/2 beyond it when pruned
+  const int L = a.kxa ? a.kxa : H;
+  const int nch = L / CPC;
+  auto stage = [&](int r) {
+#pragma unroll
+    for (int hh = 0; hh < SPW; ++hh) {
+      const int q = SPW * r + hh;
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const C *src = w ? f2s[q] + l2s[q] * pin : f1s[q] + l1s[q] * pin;
+        C *dst = s + q * LDC + w * HS;
+        for (int c = lane; c < nch; c += 32) cpa16(dst + c * CPC, src + c * CPC);
+        if (lane == 0) {
+          if constexpr (CPC == 2) {
+            if (L & 1) cpa8(dst + L - 1, src + L - 1);
+            if (a.kxa) cpa8(dst + N / 2, src + N / 2);
+          } else {
+            if (a.kxa) cpa16(dst + N / 2, src + N / 2);
+          }
+        }
+      }
+    }
+    cpa_commit();
+  };
+  stage(0);
+#pragma unroll 1
+  for (int r = 0; r < RI; ++r) {
+    const int q = SPW * r + h;
+    if (r + 1 < RI) stage(r + 1);
+    else cpa_commit();   // an empty group: round r's copies are the older one
+    cpa_wait_prev();
+    __syncwarp();        // every lane's copies of round r are visible
+    const C *X1 = s + q * LDC, *X2 = X1 + HS;
+    C v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int n = EN::in_row(p, i);
+      const int kk = n <= N / 2 ? n : N - n;
+      const bool kp = xkeep(a.kxa, kk, N);
+      v[i] = pack_pair<C, N>(n, kp ? X1[kk] : mkc<C>(0, 0), kp ? X2[kk] : mkc<C>(0, 0));
+    }
+    __syncwarp();        // column q is read before the transform overwrites it
+    fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, p, true, a.tw);
+#pragma unroll
+    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
+  }
+  xline_w_tail<T, N>(s, a, la, lb, lane, pout);
+}
+
 template <typename T> struct XlineArgs {
   using C = typename CT<T>::type;
   const void *in[6];

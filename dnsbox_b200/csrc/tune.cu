@@ -8,7 +8,7 @@
 // strided passes (A inverse z, B inverse y, D forward y) of the tensor-core
 // form the cp.async-fed tensor-core kernel or the FP32 SIMT kernel (the
 // form's accuracy bars hold for both), and for the fused x pass the block
-// kernel or the warp kernel.  The TMA-staged tensor-core kernels (passes A, B, D and
+// kernel or the warp kernel with register-prefetched or cp.async-staged inputs.  The TMA-staged tensor-core kernels (passes A, B, D and
 // E1) stay selectable by dnsbox_set_schedule but are not candidates: they
 // measured slower than both others at every size.  Each uniform candidate schedule advances a copy of the caller's
 // state for a few steps with pass timing on (CUDA events on the context's
@@ -130,7 +130,7 @@ extern "C" int dnsbox_set_schedule(dnsbox_ctx *ctx, const dnsbox_schedule *s) {
   for (int i = 0; i < 3; ++i)
     if (s->tc_kernel[i] < 0 || s->tc_kernel[i] > 2) return set_err(DNSBOX_ERR_ARG, "tc_kernel[0..2] must be 0 .. 2");
   if (s->tc_kernel[3] != 0 && s->tc_kernel[3] != 1) return set_err(DNSBOX_ERR_ARG, "tc_kernel[3] must be 0 or 1");
-  if (s->x_kernel < 0 || s->x_kernel > 2) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0 .. 2");
+  if (s->x_kernel < 0 || s->x_kernel > 3) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0 .. 3");
   apply(ctx, *s);
   return DNSBOX_OK;
 }
@@ -150,7 +150,7 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
   if (ctx->tc && !fp64 && (Ops<float>::has_tc(p.nz) || Ops<float>::has_tc(p.ny)))
     tc_opts.push_back(2);   // the FP32 SIMT kernel
   std::vector<int> x_opts = {0};
-  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1};
+  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1, 3};
   const dnsbox_schedule saved_sched = current(ctx);
   Saved sv;
   RET(save(ctx, sv));
