@@ -132,11 +132,13 @@ __host__ __device__ __forceinline__ int strided_col(const StridedArgs<T> &a, int
 // Resident CTAs of a strided launch to ask the register allocator for: FP32
 // blocks of up to 256 threads whose plans hold at most 16 values a thread
 // are held to 64 registers a thread (the load-latency-bound passes gain more
-// from the extra warps than they lose to the tighter allocation); 0 leaves
+// from the extra warps than they lose to the tighter allocation), FP64
+// blocks of 128 threads to 128 registers (16 warps per SM); 0 leaves
 // the choice to the compiler.
 template <typename T, int N> struct StridedMinCtas {
   static constexpr int NT = round32(TileCols<T>::v * (N / FftPlan<N>::E));
-  static constexpr int v = (sizeof(T) == 4 && NT <= 256 && FftPlan<N>::E <= 16) ? 1024 / NT : 0;
+  static constexpr int v = (sizeof(T) == 4 && NT <= 256 && FftPlan<N>::E <= 16) ? 1024 / NT
+                         : (sizeof(T) == 8 && NT == 128 && FftPlan<N>::E <= 16) ? 4 : 0;
 };
 
 // Column origin and other-axis index of tile t of the (possibly pruned) grid.
