@@ -179,12 +179,51 @@ template <int R, typename C, bool INV> __device__ __forceinline__ void dft(C *v)
   else static_assert(R == 2, "unsupported radix");
 }
 
+// ----------------------------------------------------------- twiddle sources
+// W_N^(r j TS) of stage S of plan PL (r in [1, R), j in [0, NS)).  TwGlobal
+// reads the N-point table exp(-2 pi i k / N) through the read-only cache;
+// TwShared reads per-stage [r - 1][j] tables in shared memory, so that the
+// lanes of a warp with consecutive j read consecutive words (one shared
+// wavefront instead of a scatter of L1 sectors), filled by tw_fill.
+template <class PL, int S> __host__ __device__ constexpr int tw_off() {
+  int o = 0;
+  for (int t = 1; t < S; ++t) o += (PL::R[t] - 1) * PL::ns(t);
+  return o;
+}
+template <class PL> __host__ __device__ constexpr int tw_size() { return tw_off<PL, PL::NST>(); }
+
+template <typename C> struct TwGlobal {
+  const C *__restrict__ tw;
+  template <class PL, int S> __device__ __forceinline__ C get(int r, int j) const {
+    constexpr int TS = PL::N / (PL::ns(S) * PL::R[S]);
+    return __ldg(&tw[r * j * TS]);
+  }
+};
+template <typename C> struct TwShared {
+  const C *t;
+  template <class PL, int S> __device__ __forceinline__ C get(int r, int j) const {
+    return t[tw_off<PL, S>() + (r - 1) * PL::ns(S) + j];
+  }
+};
+// Fills the shared tables of plan PL from the global N-point table (all
+// threads of the block take part; the caller synchronises afterwards).
+template <typename C, class PL, int S = 1>
+__device__ __forceinline__ void tw_fill(C *t, const C *__restrict__ tw, int tid, int nthreads) {
+  if constexpr (S < PL::NST) {
+    constexpr int NS = PL::ns(S), R = PL::R[S], TS = PL::N / (NS * R);
+    for (int i = tid; i < (R - 1) * NS; i += nthreads) {
+      const int r = 1 + i / NS, j = i % NS;
+      t[tw_off<PL, S>() + i] = tw[r * j * TS];
+    }
+    tw_fill<C, PL, S + 1>(t, tw, tid, nthreads);
+  }
+}
+
 // ----------------------------------------------------------------- stages
 // One Stockham stage on column `col` of the tile; p in [0, N/E).  All threads
 // of the block call it (barriers inside); `active` masks idle threads.
-template <typename C, class PL, int S, bool INV, bool WARP, class AD = AddrRM>
-__device__ __forceinline__ void fft_stage_p(C *s, int LD, int col, int p, bool active,
-                                            const C *__restrict__ tw) {
+template <typename C, class PL, int S, bool INV, bool WARP, class AD = AddrRM, class TW = TwGlobal<C>>
+__device__ __forceinline__ void fft_stage_p(C *s, int LD, int col, int p, bool active, const TW &tw) {
   constexpr int N = PL::N;
   constexpr int R = PL::R[S];
   constexpr int NS = PL::ns(S);
@@ -208,10 +247,9 @@ __device__ __forceinline__ void fft_stage_p(C *s, int LD, int col, int p, bool a
       const int b = p + m * P;
       const int j = b % NS;
       if constexpr (NS > 1) {
-        constexpr int TS = N / (NS * R);
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const C w = __ldg(&tw[r * j * TS]);
+          const C w = tw.template get<PL, S>(r, j);
           v[m][r] = INV ? cmulc(v[m][r], w) : cmul(v[m][r], w);
         }
       }
@@ -226,7 +264,7 @@ __device__ __forceinline__ void fft_stage_p(C *s, int LD, int col, int p, bool a
 
 template <typename C, int N, int S, bool INV>
 __device__ __forceinline__ void fft_stage(C *s, int LD, int col, int p, bool active, const C *__restrict__ tw) {
-  fft_stage_p<C, FftPlan<N>, S, INV, false>(s, LD, col, p, active, tw);
+  fft_stage_p<C, FftPlan<N>, S, INV, false>(s, LD, col, p, active, TwGlobal<C>{tw});
 }
 
 template <typename C, int N, bool INV, int S = 0>
@@ -286,9 +324,9 @@ __device__ __forceinline__ void fft_first_regs_p(C *v, C *s, int LD, int col, in
 
 // Last stage from shared memory into registers (v in out_row order).  The
 // caller owns the barrier that must follow before shared memory is reused.
-template <typename C, class PL, bool INV, class AD = AddrRM>
+template <typename C, class PL, bool INV, class AD = AddrRM, class TW = TwGlobal<C>>
 __device__ __forceinline__ void fft_last_regs_p(C *v, const C *s, int LD, int col, int p, bool active,
-                                                const C *__restrict__ tw) {
+                                                const TW &tw) {
   constexpr int N = PL::N;
   constexpr int S = PL::NST - 1;
   constexpr int R = PL::R[S];
@@ -303,10 +341,9 @@ __device__ __forceinline__ void fft_last_regs_p(C *v, const C *s, int LD, int co
 #pragma unroll
     for (int r = 0; r < R; ++r) v[m * R + r] = s[AD::at(b + r * NB, col, LD)];
     const int j = b % NS;
-    constexpr int TS = N / (NS * R);
 #pragma unroll
     for (int r = 1; r < R; ++r) {
-      const C w = __ldg(&tw[r * j * TS]);
+      const C w = tw.template get<PL, S>(r, j);
       v[m * R + r] = INV ? cmulc(v[m * R + r], w) : cmul(v[m * R + r], w);
     }
     dft<R, C, INV>(v + m * R);
@@ -314,26 +351,30 @@ __device__ __forceinline__ void fft_last_regs_p(C *v, const C *s, int LD, int co
 }
 
 // Stages 1 .. NST-2 in shared memory.
-template <typename C, class PL, bool INV, bool WARP, class AD = AddrRM, int S = 1>
-__device__ __forceinline__ void fft_middle_p(C *s, int LD, int col, int p, bool active, const C *__restrict__ tw) {
+template <typename C, class PL, bool INV, bool WARP, class AD = AddrRM, int S = 1, class TW = TwGlobal<C>>
+__device__ __forceinline__ void fft_middle_p(C *s, int LD, int col, int p, bool active, const TW &tw) {
   if constexpr (S + 1 < PL::NST) {
-    fft_stage_p<C, PL, S, INV, WARP, AD>(s, LD, col, p, active, tw);
-    fft_middle_p<C, PL, INV, WARP, AD, S + 1>(s, LD, col, p, active, tw);
+    fft_stage_p<C, PL, S, INV, WARP, AD, TW>(s, LD, col, p, active, tw);
+    fft_middle_p<C, PL, INV, WARP, AD, S + 1, TW>(s, LD, col, p, active, tw);
   }
 }
 
 // Whole transform with v holding the first stage's inputs on entry and the
 // last stage's outputs on exit.  Shared memory (N x LD tile) is scratch;
 // ends with a barrier (block or warp) so the tile may be reused.
+template <typename C, class PL, bool INV, bool WARP, class AD = AddrRM, class TW>
+__device__ __forceinline__ void fft_regs_t(C *v, C *s, int LD, int col, int p, bool active, const TW &tw) {
+  fft_first_regs_p<C, PL, INV, WARP, AD>(v, s, LD, col, p, active);
+  if constexpr (PL::NST > 1) {
+    fft_middle_p<C, PL, INV, WARP, AD, 1, TW>(s, LD, col, p, active, tw);
+    fft_last_regs_p<C, PL, INV, AD, TW>(v, s, LD, col, p, active, tw);
+    fft_sync<WARP>();
+  }
+}
 template <typename C, class PL, bool INV, bool WARP, class AD = AddrRM>
 __device__ __forceinline__ void fft_regs_p(C *v, C *s, int LD, int col, int p, bool active,
                                            const C *__restrict__ tw) {
-  fft_first_regs_p<C, PL, INV, WARP, AD>(v, s, LD, col, p, active);
-  if constexpr (PL::NST > 1) {
-    fft_middle_p<C, PL, INV, WARP, AD>(s, LD, col, p, active, tw);
-    fft_last_regs_p<C, PL, INV, AD>(v, s, LD, col, p, active, tw);
-    fft_sync<WARP>();
-  }
+  fft_regs_t<C, PL, INV, WARP, AD>(v, s, LD, col, p, active, TwGlobal<C>{tw});
 }
 
 template <typename C, int N, bool INV>

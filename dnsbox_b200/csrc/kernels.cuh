@@ -436,11 +436,38 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
 // sequence runs the two-stage radix-16 plan on 16 threads, so a warp
 // transforms two sequences at once with one shared-memory exchange each; at
 // N = 512 a sequence runs the three-stage plan on all 32 threads.
+// In FP32 the twiddles come from per-stage tables in shared memory (one
+// wavefront per lane-varying read instead of a scatter of L1 sectors, which
+// left the kernel bound by L1 throughput); FP64 keeps the global table, whose
+// shared copy would cost a resident block.
 template <typename T, int N> struct XlineWarp {
   static constexpr bool on = N == 256 || N == 512;
   static constexpr int wpb = sizeof(T) == 8 ? (N >= 512 ? 1 : 2) : (N >= 1024 ? 1 : (N >= 512 ? 2 : 4));
   using Plan = typename std::conditional<N == 256, FftPlan<256>, WarpPlan<N>>::type;
+  static constexpr bool full3 = 32 / (N / Plan::E) == 2 && sizeof(T) == 4;   // see xline_w_tail
+  static constexpr bool smtw = on && sizeof(T) == 4;
+  static constexpr int twn = smtw ? tw_size<Plan>() + (full3 ? tw_size<WarpPlan<N>>() : 0) : 0;
+  // twiddle tables of the block after its warps' tiles; all threads fill them
+  __device__ static __forceinline__ typename CT<T>::type *tables(unsigned char *smem, const typename CT<T>::type *tw) {
+    using C = typename CT<T>::type;
+    C *t = reinterpret_cast<C *>(smem) + (size_t)wpb * 6 * (N + N / Plan::R[0]);
+    if constexpr (smtw) {
+      tw_fill<C, Plan>(t, tw, threadIdx.x, blockDim.x);
+      if constexpr (full3) tw_fill<C, WarpPlan<N>>(t + tw_size<Plan>(), tw, threadIdx.x, blockDim.x);
+      __syncthreads();
+    }
+    return t;
+  }
 };
+
+// The x pass's transform of `v` on column `col` with the kernel's twiddle source.
+template <typename T, class PL, bool INV, class AD, int N>
+__device__ __forceinline__ void xw_fft(typename CT<T>::type *v, typename CT<T>::type *s, int LD, int col, int p,
+                                       bool active, const typename CT<T>::type *tw, const typename CT<T>::type *twt) {
+  using C = typename CT<T>::type;
+  if constexpr (XlineWarp<T, N>::smtw) fft_regs_t<C, PL, INV, true, AD>(v, s, LD, col, p, active, TwShared<C>{twt});
+  else fft_regs_p<C, PL, INV, true, AD>(v, s, LD, col, p, active, tw);
+}
 
 // Second half of the warp-granular fused x pass for one line pair (la, lb):
 // the inverse transforms are in the warp's tile s (column-major, skewed);
@@ -448,7 +475,8 @@ template <typename T, int N> struct XlineWarp {
 // output half lines and the CFL maxima of the pair.
 template <typename T, int N>
 __device__ __forceinline__ void xline_w_tail(typename CT<T>::type *s, const XlineNLArgs<T> &a, long long la,
-                                             long long lb, int lane, long long pout) {
+                                             long long lb, int lane, long long pout,
+                                             const typename CT<T>::type *twt) {
   using C = typename CT<T>::type;
   using PL = typename XlineWarp<T, N>::Plan;
   using EN = FftEndsP<PL>;
@@ -489,7 +517,7 @@ __device__ __forceinline__ void xline_w_tail(typename CT<T>::type *s, const Xlin
   // FP32 with two per warp, sequence 2 runs on all 32 lanes with the 32-thread
   // plan (same column, skew and twiddle table) instead of on one half-warp
   // (in FP64 that form measured slower)
-  constexpr bool FULL3 = SPW == 2 && sizeof(T) == 4;
+  constexpr bool FULL3 = XlineWarp<T, N>::full3;
   constexpr int RF = FULL3 ? 1 : (3 + SPW - 1) / SPW;
 #pragma unroll 1
   for (int r = 0; r < RF; ++r) {
@@ -502,7 +530,7 @@ __device__ __forceinline__ void xline_w_tail(typename CT<T>::type *s, const Xlin
       for (int i = 0; i < E; ++i) v[i] = s[AD::at(EN::in_row(p, i), qc, LDC)];
     }
     __syncwarp();
-    fft_regs_p<C, PL, false, true, AD>(v, s, LDC, qc, p, act, a.tw);
+    xw_fft<T, PL, false, AD, N>(v, s, LDC, qc, p, act, a.tw, twt);
     if (act) {
 #pragma unroll
       for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), qc, LDC)] = v[i];
@@ -516,7 +544,7 @@ __device__ __forceinline__ void xline_w_tail(typename CT<T>::type *s, const Xlin
 #pragma unroll
     for (int i = 0; i < WP::E; ++i) w[i] = s[AD::at(EW::in_row(lane, i), 2, LDC)];
     __syncwarp();
-    fft_regs_p<C, WP, false, true, AD>(w, s, LDC, 2, lane, true, a.tw);
+    xw_fft<T, WP, false, AD, N>(w, s, LDC, 2, lane, true, a.tw, twt + tw_size<PL>());
 #pragma unroll
     for (int i = 0; i < WP::E; ++i) s[AD::at(EW::out_row(lane, i), 2, LDC)] = w[i];
   }
@@ -568,6 +596,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   C *s = reinterpret_cast<C *>(smem_raw) + (size_t)warp * 6 * LDC;
+  const C *twt = XlineWarp<T, N>::tables(smem_raw, a.tw);   // (a block barrier in FP32)
   const long long la = 2 * ((long long)blockIdx.x * WPB + warp), lb = la + 1;
   if (la >= a.nlines) return;
   const C *f1s[6] = {a.U, a.U, a.W, a.OX, a.OX, a.OZ};
@@ -605,11 +634,11 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
         x2[i] = kp ? g2[kk] : mkc<C>(0, 0);
       }
     }
-    fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, p, true, a.tw);
+    xw_fft<T, PL, true, AD, N>(v, s, LDC, q, p, true, a.tw, twt);
 #pragma unroll
     for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
   }
-  xline_w_tail<T, N>(s, a, la, lb, lane, pout);
+  xline_w_tail<T, N>(s, a, la, lb, lane, pout, twt);
 }
 
 // Plain x-line transforms of nf fields (blockIdx.y = field).
@@ -653,6 +682,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   C *s = reinterpret_cast<C *>(smem_raw) + (size_t)warp * 6 * LDC;
+  const C *twt = XlineWarp<T, N>::tables(smem_raw, a.tw);   // (a block barrier in FP32)
   const long long la = 2 * ((long long)blockIdx.x * WPB + warp), lb = la + 1;
   if (la >= a.nlines) return;
   const C *f1s[6] = {a.U, a.U, a.W, a.OX, a.OX, a.OZ};
@@ -703,11 +733,11 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
       v[i] = pack_pair<C, N>(n, kp ? X1[kk] : mkc<C>(0, 0), kp ? X2[kk] : mkc<C>(0, 0));
     }
     __syncwarp();        // column q is read before the transform overwrites it
-    fft_regs_p<C, PL, true, true, AD>(v, s, LDC, q, p, true, a.tw);
+    xw_fft<T, PL, true, AD, N>(v, s, LDC, q, p, true, a.tw, twt);
 #pragma unroll
     for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
   }
-  xline_w_tail<T, N>(s, a, la, lb, lane, pout);
+  xline_w_tail<T, N>(s, a, la, lb, lane, pout, twt);
 }
 
 template <typename T> struct XlineArgs {

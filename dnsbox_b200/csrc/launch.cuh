@@ -147,7 +147,7 @@ cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaS
     // warp-granular kernel: one warp per line pair
     constexpr int WPB = XlineWarp<T, N>::wpb;
     constexpr int LDC = N + N / XlineWarp<T, N>::Plan::R[0];
-    const size_t smem = (size_t)WPB * 6 * LDC * sizeof(C);
+    const size_t smem = ((size_t)WPB * 6 * LDC + XlineWarp<T, N>::twn) * sizeof(C);
     cudaError_t e;
     const long long pairs = (a.nlines + 1) / 2;
     const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
