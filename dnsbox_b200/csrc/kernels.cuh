@@ -132,13 +132,12 @@ __host__ __device__ __forceinline__ int strided_col(const StridedArgs<T> &a, int
 // Resident CTAs of a strided launch to ask the register allocator for: FP32
 // blocks of up to 256 threads whose plans hold at most 16 values a thread
 // are held to 64 registers a thread (the load-latency-bound passes gain more
-// from the extra warps than they lose to the tighter allocation), FP64
-// blocks of 128 threads to 128 registers (16 warps per SM); 0 leaves
+// from the extra warps than they lose to the tighter allocation); 0 leaves
 // the choice to the compiler.
 template <typename T, int N> struct StridedMinCtas {
   static constexpr int NT = round32(TileCols<T>::v * (N / FftPlan<N>::E));
   static constexpr int v = (sizeof(T) == 4 && NT <= 256 && FftPlan<N>::E <= 16) ? 1024 / NT
-                         : (sizeof(T) == 8 && NT == 128 && FftPlan<N>::E <= 16) ? 4 : 0;
+                         : 0;
 };
 
 // Column origin and other-axis index of tile t of the (possibly pruned) grid.
@@ -177,11 +176,13 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
   const int kx = strided_col(a, kx0 + col);
   const bool valid = act && kx < a.ncols && a.kcol.keep(kx);
   const long long base = (long long)other * a.otherstride + kx + (long long)blockIdx.y * a.bstride;
-  // the job's row multipliers T(b k_row(n)) (ks == 1), once per block
-  // instead of once per element: the same values as apply_mult forms
-  __shared__ T bks[2][N];
+  // FP32: the job's row multipliers T(b k_row(n)) (ks == 1), once per block
+  // instead of once per element (the same values as apply_mult forms; FP64
+  // evaluates them per element, which keeps its kernel at 128 registers)
+  constexpr bool TAB = sizeof(T) == 4;
+  __shared__ T bks[2][TAB ? N : 1];
   const bool mult1 = !(J.a1 == 1.0 && J.b1 == 0.0);
-  if ((mult1 && J.ks1 == 1) || (J.in2 && J.ks2 == 1)) {
+  if (TAB && ((mult1 && J.ks1 == 1) || (J.in2 && J.ks2 == 1))) {
     for (int n = threadIdx.x; n < N; n += blockDim.x) {
       const double k = k_full(n, N, a.alpha_row);
       bks[0][n] = T(J.b1 * k);
@@ -199,22 +200,40 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
     // wavenumber of the column (0) or of the tile's other-axis index (2)
     const double kcol = k_half(kx, a.nx, a.alpha_x);
     const double koth = a.n_other ? k_full(other, a.n_other, a.alpha_other) : 0.0;
-    if (mult1) {
-      const T aa = T(J.a1), bkc = T(J.b1 * (J.ks1 == 2 ? koth : kcol));
+    if constexpr (TAB) {
+      if (mult1) {
+        const T aa = T(J.a1), bkc = T(J.b1 * (J.ks1 == 2 ? koth : kcol));
 #pragma unroll
-      for (int i = 0; i < E; ++i) {
-        const T bk = J.ks1 == 1 ? bks[0][EN::in_row(p, i)] : bkc;
-        v[i] = mkc<C>(v[i].x * aa - v[i].y * bk, v[i].y * aa + v[i].x * bk);
+        for (int i = 0; i < E; ++i) {
+          const T bk = J.ks1 == 1 ? bks[0][EN::in_row(p, i)] : bkc;
+          v[i] = mkc<C>(v[i].x * aa - v[i].y * bk, v[i].y * aa + v[i].x * bk);
+        }
       }
-    }
-    if (J.in2) {
-      const C *in2 = J.in2 + base;
-      const T aa = T(J.a2), bkc = T(J.b2 * (J.ks2 == 2 ? koth : kcol));
+      if (J.in2) {
+        const C *in2 = J.in2 + base;
+        const T aa = T(J.a2), bkc = T(J.b2 * (J.ks2 == 2 ? koth : kcol));
 #pragma unroll
-      for (int i = 0; i < E; ++i) {
-        const C w = a.krin.keep(EN::in_row(p, i)) ? in2[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
-        const T bk = J.ks2 == 1 ? bks[1][EN::in_row(p, i)] : bkc;
-        v[i] = cadd(v[i], mkc<C>(w.x * aa - w.y * bk, w.y * aa + w.x * bk));
+        for (int i = 0; i < E; ++i) {
+          const C w = a.krin.keep(EN::in_row(p, i)) ? in2[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
+          const T bk = J.ks2 == 1 ? bks[1][EN::in_row(p, i)] : bkc;
+          v[i] = cadd(v[i], mkc<C>(w.x * aa - w.y * bk, w.y * aa + w.x * bk));
+        }
+      }
+    } else {
+      if (mult1) {
+        const double kc = J.ks1 == 2 ? koth : kcol;
+#pragma unroll
+        for (int i = 0; i < E; ++i)
+          v[i] = apply_mult<T>(v[i], J.a1, J.b1, J.ks1 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc);
+      }
+      if (J.in2) {
+        const C *in2 = J.in2 + base;
+        const double kc = J.ks2 == 2 ? koth : kcol;
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+          const C w = a.krin.keep(EN::in_row(p, i)) ? in2[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
+          v[i] = cadd(v[i], apply_mult<T>(w, J.a2, J.b2, J.ks2 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc));
+        }
       }
     }
   } else {
