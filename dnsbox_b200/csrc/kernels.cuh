@@ -625,33 +625,48 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
   const int p = lane % P, h = lane / P;   // position in the sequence, sequence slot
   const long long pin = a.pin ? a.pin : a.nxh, pout = a.pout ? a.pout : a.nxh;
   // inverse transforms: round r transforms sequences SPW r + h; the loads of
-  // the next round are issued before this round's transform
+  // the next round are issued before this round's transform.  A lane loads
+  // only its rows n = p + P i <= N/2 (i < E/2, and i = E/2 at p = 0); row
+  // N - n of the Hermitian mirror is row n' = (P - p) + P (E - 1 - i) of lane
+  // P - p (lane p = 0: its own row P (E - i)), taken by a shuffle, so every
+  // half-line element is read from global memory once.
+  static_assert(PL::R[0] == E, "first-stage rows n = p + P i");
   C x1[E], x2[E];
+  auto load = [&](const C *g1, const C *g2) {
 #pragma unroll
-  for (int i = 0; i < E; ++i) {
-    const int n = EN::in_row(p, i);
-    const int kk = n <= N / 2 ? n : N - n;
-    const bool kp = xkeep(a.kxa, kk, N);
-    x1[i] = kp ? f1s[h][l1s[h] * pin + kk] : mkc<C>(0, 0);
-    x2[i] = kp ? f2s[h][l2s[h] * pin + kk] : mkc<C>(0, 0);
-  }
+    for (int i = 0; i <= E / 2; ++i) {
+      const int n = p + P * i;   // <= N / 2 for i < E / 2 and for p = 0
+      const bool kp = (i < E / 2 || p == 0) && xkeep(a.kxa, n, N);
+      x1[i] = kp ? g1[n] : mkc<C>(0, 0);
+      x2[i] = kp ? g2[n] : mkc<C>(0, 0);
+    }
+  };
+  const int mirror = (lane & ~(P - 1)) | ((P - p) & (P - 1));   // lane of the mirror rows
+  auto mirror_fill = [&]() {
+#pragma unroll
+    for (int i = E / 2; i < E; ++i) {
+      const int j = E - 1 - i;
+      C m1 = mkc<C>(__shfl_sync(0xffffffffu, x1[j].x, mirror), __shfl_sync(0xffffffffu, x1[j].y, mirror));
+      C m2 = mkc<C>(__shfl_sync(0xffffffffu, x2[j].x, mirror), __shfl_sync(0xffffffffu, x2[j].y, mirror));
+      if (p == 0) {   // rows 0 and N/2 are its own loads; N - P i = P (E - i)
+        m1 = i == E / 2 ? x1[i] : x1[E - i];
+        m2 = i == E / 2 ? x2[i] : x2[E - i];
+      }
+      x1[i] = m1;
+      x2[i] = m2;
+    }
+  };
+  load(f1s[h] + l1s[h] * pin, f2s[h] + l2s[h] * pin);
 #pragma unroll 1
   for (int r = 0; r < 6 / SPW; ++r) {
     const int q = SPW * r + h;
     C v[E];
+    mirror_fill();
 #pragma unroll
     for (int i = 0; i < E; ++i) v[i] = pack_pair<C, N>(EN::in_row(p, i), x1[i], x2[i]);
     if (r + 1 < 6 / SPW) {
       const int qn = q + SPW;
-      const C *g1 = f1s[qn] + l1s[qn] * pin, *g2 = f2s[qn] + l2s[qn] * pin;
-#pragma unroll
-      for (int i = 0; i < E; ++i) {
-        const int n = EN::in_row(p, i);
-        const int kk = n <= N / 2 ? n : N - n;
-        const bool kp = xkeep(a.kxa, kk, N);
-        x1[i] = kp ? g1[kk] : mkc<C>(0, 0);
-        x2[i] = kp ? g2[kk] : mkc<C>(0, 0);
-      }
+      load(f1s[qn] + l1s[qn] * pin, f2s[qn] + l2s[qn] * pin);
     }
     xw_fft<T, PL, true, AD, N>(v, s, LDC, q, p, true, a.tw, twt);
 #pragma unroll
