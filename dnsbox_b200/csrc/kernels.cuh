@@ -467,9 +467,10 @@ template <typename T, int N> struct XlineWarp {
   static constexpr bool smtw = on && sizeof(T) == 4;
   static constexpr int twn = smtw ? tw_size<Plan>() + (full3 ? tw_size<WarpPlan<N>>() : 0) : 0;
   // twiddle tables of the block after its warps' tiles; all threads fill them
-  __device__ static __forceinline__ typename CT<T>::type *tables(unsigned char *smem, const typename CT<T>::type *tw) {
+  __device__ static __forceinline__ typename CT<T>::type *tables(unsigned char *smem, const typename CT<T>::type *tw,
+                                                                  int cols = 6) {
     using C = typename CT<T>::type;
-    C *t = reinterpret_cast<C *>(smem) + (size_t)wpb * 6 * (N + N / Plan::R[0]);
+    C *t = reinterpret_cast<C *>(smem) + (size_t)wpb * cols * (N + N / Plan::R[0]);
     if constexpr (smtw) {
       tw_fill<C, Plan>(t, tw, threadIdx.x, blockDim.x);
       if constexpr (full3) tw_fill<C, WarpPlan<N>>(t + tw_size<Plan>(), tw, threadIdx.x, blockDim.x);
@@ -676,102 +677,136 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
 }
 
 // Plain x-line transforms of nf fields (blockIdx.y = field).
-// 16- and 8-byte asynchronous global -> shared copies (cp.async), commit and
-// wait for all but the newest group.
-__device__ __forceinline__ void cpa16(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cpa8(void *dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cpa_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
-// The warp kernel with its inputs staged by cp.async: the two half lines of
-// each sequence of round r + 1 are copied (16-byte chunks of the kept prefix,
-// plus the lone Nyquist element when pruned) into that sequence's own tile
-// column while round r transforms, then read from shared memory with the
-// Hermitian mirror.  Every half-line element is fetched from global memory
-// once, in whole coalesced chunks, and no registers hold the next round's
-// inputs.  Needs 16-byte aligned input rows (even pitch in FP32).
-template <typename T, int N>
-__global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
-    k_xline_nl_ws(const __grid_constant__ XlineNLArgs<T> a) {
+// Fused x pass at N = 256 with the fields of a line in registers (FP32).
+// Half-warp h owns line la + h and packs its six real lines as three
+// sequences, U + iV, W + i OZ and OX + i OY, transformed one per round on
+// its 16 lanes.  With the two-stage radix-16 plan a lane's first-stage
+// input rows and last-stage output rows are the same, n = p + 16 i, so after
+// the three rounds every lane holds u, v, w and the vorticity at its 16
+// rows: the cross product and the CFL maxima need no shared memory, and the
+// products px + i py are already the forward transform's inputs.  The third
+// forward sequence, pz(a) + i pz(b), is formed by one shuffle across the
+// halves and transformed by both (each stores its line's half).  Shared
+// memory holds only each sequence's one exchange (two columns per warp) and
+// the twiddle tables.  Hermitian-mirror rows, on input and output, come from
+// the partner lane by shuffle.
+template <typename T>
+__global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb)
+    k_xline_nl_r(const __grid_constant__ XlineNLArgs<T> a) {
+  constexpr int N = 256;
   using C = typename CT<T>::type;
   using PL = typename XlineWarp<T, N>::Plan;
   using EN = FftEndsP<PL>;
   using AD = AddrSkew<PL::R[0]>;
   constexpr int E = PL::E;
-  constexpr int P = N / E;                       // threads per sequence
-  constexpr int SPW = 32 / P;                    // sequences a warp transforms at once
-  constexpr int RI = 6 / SPW;                    // rounds of inverse transforms
-  constexpr int LDC = N + N / PL::R[0];          // column length with the skew
+  constexpr int P = N / E;
+  static_assert(P == 16 && E == 16 && PL::NST == 2 && PL::R[0] == 16 && PL::R[1] == 16,
+                "rows n = p + 16 i at both ends of the transform");
+  constexpr int LDC = N + N / PL::R[0];
   constexpr int WPB = XlineWarp<T, N>::wpb;
-  constexpr int H = N / 2 + 1;
-  constexpr int CPC = 16 / (int)sizeof(C);       // complex values per 16-byte chunk
-  constexpr int HS = (H + CPC - 1) / CPC * CPC;  // staged half-line length
-  static_assert(2 * HS <= LDC, "both staged half lines of a sequence fit its column");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C *s = reinterpret_cast<C *>(smem_raw) + (size_t)warp * 6 * LDC;
-  const C *twt = XlineWarp<T, N>::tables(smem_raw, a.tw);   // (a block barrier in FP32)
-  const long long la = 2 * ((long long)blockIdx.x * WPB + warp), lb = la + 1;
+  const int p = lane & 15, h = lane >> 4;
+  C *s = reinterpret_cast<C *>(smem_raw) + (size_t)warp * 2 * LDC;
+  const C *twt = XlineWarp<T, N>::tables(smem_raw, a.tw, 2);   // (a block barrier in FP32)
+  const long long la = 2 * ((long long)blockIdx.x * WPB + warp);
   if (la >= a.nlines) return;
-  const C *f1s[6] = {a.U, a.U, a.W, a.OX, a.OX, a.OZ};
-  const C *f2s[6] = {a.V, a.V, a.W, a.OY, a.OY, a.OZ};
-  const long long l1s[6] = {la, lb, la, la, lb, la};
-  const long long l2s[6] = {la, lb, lb, la, lb, lb};
-  const int p = lane % P, h = lane / P;   // position in the sequence, sequence slot
+  const long long line = la + h;
   const long long pin = a.pin ? a.pin : a.nxh, pout = a.pout ? a.pout : a.nxh;
-  // the kept prefix [0, L) of a half line, and the Nyquist element N/2 beyond it when pruned
-  const int L = a.kxa ? a.kxa : H;
-  const int nch = L / CPC;
-  auto stage = [&](int r) {
+  const T sc = T(a.s);
+  const int mirror = (lane & 16) | ((16 - p) & 15);
+  // rows n = p + 16 i <= N / 2 of the two half lines of a sequence
+  C x1[E / 2 + 1], x2[E / 2 + 1];
+  auto load = [&](const C *g1, const C *g2) {
 #pragma unroll
-    for (int hh = 0; hh < SPW; ++hh) {
-      const int q = SPW * r + hh;
-#pragma unroll
-      for (int w = 0; w < 2; ++w) {
-        const C *src = w ? f2s[q] + l2s[q] * pin : f1s[q] + l1s[q] * pin;
-        C *dst = s + q * LDC + w * HS;
-        for (int c = lane; c < nch; c += 32) cpa16(dst + c * CPC, src + c * CPC);
-        if (lane == 0) {
-          if constexpr (CPC == 2) {
-            if (L & 1) cpa8(dst + L - 1, src + L - 1);
-            if (a.kxa) cpa8(dst + N / 2, src + N / 2);
-          } else {
-            if (a.kxa) cpa16(dst + N / 2, src + N / 2);
-          }
-        }
-      }
+    for (int i = 0; i <= E / 2; ++i) {
+      const int n = p + P * i;
+      const bool kp = (i < E / 2 || p == 0) && xkeep(a.kxa, n, N);
+      x1[i] = kp ? g1[n] : mkc<C>(0, 0);
+      x2[i] = kp ? g2[n] : mkc<C>(0, 0);
     }
-    cpa_commit();
   };
-  stage(0);
-#pragma unroll 1
-  for (int r = 0; r < RI; ++r) {
-    const int q = SPW * r + h;
-    if (r + 1 < RI) stage(r + 1);
-    else cpa_commit();   // an empty group: round r's copies are the older one
-    cpa_wait_prev();
-    __syncwarp();        // every lane's copies of round r are visible
-    const C *X1 = s + q * LDC, *X2 = X1 + HS;
+  // value at row N - (p + 16 i) of a lane's rows from w (own rows): the partner
+  // lane's row p' + 16 (15 - i), or (p = 0) its own row 16 (16 - i)
+  auto shfl_c = [&](C c, int src) {
+    return mkc<C>(__shfl_sync(0xffffffffu, c.x, src), __shfl_sync(0xffffffffu, c.y, src));
+  };
+  const C *f1s[3] = {a.U, a.W, a.OX};
+  const C *f2s[3] = {a.V, a.OZ, a.OY};
+  C o[3][E];   // inverse transforms: (u, v), (w, oz), (ox, oy) at rows p + 16 i
+  load(f1s[0] + line * pin, f2s[0] + line * pin);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
     C v[E];
 #pragma unroll
     for (int i = 0; i < E; ++i) {
-      const int n = EN::in_row(p, i);
-      const int kk = n <= N / 2 ? n : N - n;
-      const bool kp = xkeep(a.kxa, kk, N);
-      v[i] = pack_pair<C, N>(n, kp ? X1[kk] : mkc<C>(0, 0), kp ? X2[kk] : mkc<C>(0, 0));
+      const int n = p + P * i;
+      C y1, y2;
+      if (i < E / 2) {
+        y1 = x1[i], y2 = x2[i];
+      } else {
+        y1 = shfl_c(x1[E - 1 - i], mirror);
+        y2 = shfl_c(x2[E - 1 - i], mirror);
+        if (p == 0) {
+          y1 = i == E / 2 ? x1[E / 2] : x1[E - i];
+          y2 = i == E / 2 ? x2[E / 2] : x2[E - i];
+        }
+      }
+      v[i] = pack_pair<C, N>(n, y1, y2);
     }
-    __syncwarp();        // column q is read before the transform overwrites it
-    xw_fft<T, PL, true, AD, N>(v, s, LDC, q, p, true, a.tw, twt);
+    if (r < 2) load(f1s[r + 1] + line * pin, f2s[r + 1] + line * pin);
+    xw_fft<T, PL, true, AD, N>(v, s, LDC, h, p, true, a.tw, twt);
 #pragma unroll
-    for (int i = 0; i < E; ++i) s[AD::at(EN::out_row(p, i), q, LDC)] = v[i];
+    for (int i = 0; i < E; ++i) o[r][i] = v[i];
   }
-  xline_w_tail<T, N>(s, a, la, lb, lane, pout, twt);
+  // (omega x u) s at the lane's rows, and the CFL maxima
+  T m0 = 0, m1 = 0, m2 = 0;
+  C f[E];
+  T pz[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const T u = o[0][i].x, v = o[0][i].y, w = o[1][i].x, oz = o[1][i].y, ox = o[2][i].x, oy = o[2][i].y;
+    f[i] = mkc<C>((oy * w - oz * v) * sc, (oz * u - ox * w) * sc);
+    pz[i] = (ox * v - oy * u) * sc;
+    m0 = fmax(m0, fabs(u));
+    m1 = fmax(m1, fabs(v));
+    m2 = fmax(m2, fabs(w));
+  }
+  // forward transforms and the unpacking of two real transforms per sequence:
+  // X1[k] = (Z[k] + conj Z[N-k]) / 2, X2[k] = (Z[k] - conj Z[N-k]) / 2i at k = p + 16 i <= N/2
+  auto unpack_store = [&](const C *z, C *d1, C *d2) {
+#pragma unroll
+    for (int i = 0; i <= E / 2; ++i) {
+      const int k = p + P * i;
+      C zn = shfl_c(z[(E - 1 - i) & (E - 1)], mirror);
+      if (p == 0) zn = z[(E - i) & (E - 1)];
+      const C zk = z[i];
+      if ((i < E / 2 || p == 0) && xkeep(a.kxa, k, N)) {
+        if (d1) d1[k] = mkc<C>(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
+        if (d2) d2[k] = mkc<C>(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
+      }
+    }
+  };
+  xw_fft<T, PL, false, AD, N>(f, s, LDC, h, p, true, a.tw, twt);
+  unpack_store(f, a.NX + line * pout, a.NY + line * pout);
+  // pz(a) + i pz(b) on both halves (the same sequence)
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const T other = __shfl_xor_sync(0xffffffffu, pz[i], 16);
+    f[i] = h == 0 ? mkc<C>(pz[i], other) : mkc<C>(other, pz[i]);
+  }
+  xw_fft<T, PL, false, AD, N>(f, s, LDC, h, p, true, a.tw, twt);
+  unpack_store(f, h == 0 ? a.NZ + line * pout : nullptr, h == 1 ? a.NZ + line * pout : nullptr);
+  // CFL maxima of the pair (both lines lie in one box: ny*nz is even)
+  m0 = warp_max(m0);
+  m1 = warp_max(m1);
+  m2 = warp_max(m2);
+  if (lane == 0 && a.st) {
+    double *um = a.st[la / a.lines_per_box].umax;
+    atomic_max_nonneg(um + 0, (double)m0 * a.s);
+    atomic_max_nonneg(um + 1, (double)m1 * a.s);
+    atomic_max_nonneg(um + 2, (double)m2 * a.s);
+  }
 }
 
 template <typename T> struct XlineArgs {

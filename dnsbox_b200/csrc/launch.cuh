@@ -151,18 +151,17 @@ cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaS
     cudaError_t e;
     const long long pairs = (a.nlines + 1) / 2;
     const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
-    // staged inputs need 16-byte aligned rows: aligned fields and (FP32) an even pitch
-    const long long pin = a.pin ? a.pin : a.nxh;
-    bool aligned = sizeof(C) == 16 || pin % 2 == 0;
-    const C *const fields[6] = {a.U, a.V, a.W, a.OX, a.OY, a.OZ};
-    for (int f = 0; f < 6; ++f) aligned = aligned && (reinterpret_cast<uintptr_t>(fields[f]) & 15) == 0;
-    if (variant == 3 && aligned) {
-      if ((e = set_smem(k_xline_nl_ws<T, N>, smem)) != cudaSuccess) return e;
-      k_xline_nl_ws<T, N><<<nb, 32 * WPB, smem, st>>>(a);
-    } else {
-      if ((e = set_smem(k_xline_nl_w<T, N>, smem)) != cudaSuccess) return e;
-      k_xline_nl_w<T, N><<<nb, 32 * WPB, smem, st>>>(a);
+    if constexpr (N == 256 && sizeof(T) == 4) {
+      if (variant == 3) {
+        // fields of a line in registers: two exchange columns per warp
+        const size_t smem_r = ((size_t)WPB * 2 * LDC + XlineWarp<T, N>::twn) * sizeof(C);
+        if ((e = set_smem(k_xline_nl_r<T>, smem_r)) != cudaSuccess) return e;
+        k_xline_nl_r<T><<<nb, 32 * WPB, smem_r, st>>>(a);
+        return cudaGetLastError();
+      }
     }
+    if ((e = set_smem(k_xline_nl_w<T, N>, smem)) != cudaSuccess) return e;
+    k_xline_nl_w<T, N><<<nb, 32 * WPB, smem, st>>>(a);
     return cudaGetLastError();
     }
   }

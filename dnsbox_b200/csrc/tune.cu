@@ -8,7 +8,8 @@
 // strided passes (A inverse z, B inverse y, D forward y) of the tensor-core
 // form the cp.async-fed tensor-core kernel or the FP32 SIMT kernel (the
 // form's accuracy bars hold for both), and for the fused x pass the block
-// kernel or the warp kernel with register-prefetched or cp.async-staged inputs.  The TMA-staged tensor-core kernels (passes A, B, D and
+// kernel or the warp kernel, and at 256 in FP32 the warp kernel that keeps each line's fields in
+// registers.  The TMA-staged tensor-core kernels (passes A, B, D and
 // E1) stay selectable by dnsbox_set_schedule but are not candidates: they
 // measured slower than both others at every size.  Each uniform candidate schedule advances a copy of the caller's
 // state for a few steps with pass timing on (CUDA events on the context's
@@ -150,7 +151,8 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
   if (ctx->tc && !fp64 && (Ops<float>::has_tc(p.nz) || Ops<float>::has_tc(p.ny)))
     tc_opts.push_back(2);   // the FP32 SIMT kernel
   std::vector<int> x_opts = {0};
-  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1, 3};
+  if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1};
+  if (!fp64 && p.nx == 256) x_opts.push_back(3);
   const dnsbox_schedule saved_sched = current(ctx);
   Saved sv;
   RET(save(ctx, sv));

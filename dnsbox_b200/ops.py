@@ -329,7 +329,7 @@ class Box:
     def _sched_dict(sc, tc=True):
         return {"tc_kernel": [TC_KERNELS[v] if tc else "simt" for v in sc.tc_kernel[:3]],
                 "z_fwd_kernel": "tma" if sc.tc_kernel[3] else "simt",
-                "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-staged"}[sc.x_kernel], "tuned": bool(sc.tuned),
+                "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-registers"}[sc.x_kernel], "tuned": bool(sc.tuned),
                 "ms_default": sc.ms_default, "ms_tuned": sc.ms_tuned}
 
     def schedule(self) -> dict:
