@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
 // Plain x-line transforms of nf fields (blockIdx.y = field).
 // Fused x pass at N = 256 with the fields of a line in registers (FP32).
 // Half-warp h owns line la + h and packs its six real lines as three
-// sequences, U + iV, W + i OZ and OX + i OY, transformed one per round on
+// sequences, U + iV, W + i 2^e OZ and OX + i OY, transformed one per round on
 // its 16 lanes.  With the two-stage radix-16 plan a lane's first-stage
 // input rows and last-stage output rows are the same, n = p + 16 i, so after
 // the three rounds every lane holds u, v, w and the vorticity at its 16
@@ -717,13 +717,14 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb)
   const int mirror = (lane & 16) | ((16 - p) & 15);
   // rows n = p + 16 i <= N / 2 of the two half lines of a sequence
   C x1[E / 2 + 1], x2[E / 2 + 1];
-  auto load = [&](const C *g1, const C *g2) {
+  auto load = [&](const C *g1, const C *g2, T up2) {
 #pragma unroll
     for (int i = 0; i <= E / 2; ++i) {
       const int n = p + P * i;
       const bool kp = (i < E / 2 || p == 0) && xkeep(a.kxa, n, N);
       x1[i] = kp ? g1[n] : mkc<C>(0, 0);
-      x2[i] = kp ? g2[n] : mkc<C>(0, 0);
+      const C y = kp ? g2[n] : mkc<C>(0, 0);
+      x2[i] = mkc<C>(y.x * up2, y.y * up2);
     }
   };
   // value at row N - (p + 16 i) of a lane's rows from w (own rows): the partner
@@ -733,8 +734,13 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb)
   };
   const C *f1s[3] = {a.U, a.W, a.OX};
   const C *f2s[3] = {a.V, a.OZ, a.OY};
-  C o[3][E];   // inverse transforms: (u, v), (w, oz), (ox, oy) at rows p + 16 i
-  load(f1s[0] + line * pin, f2s[0] + line * pin);
+  // The vorticity fields carry the factor s of the spectral curl, the
+  // velocity fields do not: W and OZ share a sequence, so OZ is brought to
+  // W's magnitude by the power of two nearest 1/s (exact both ways) before
+  // the transform, which would otherwise round it relative to W.
+  const T up = (T)exp2(rint(-log2(a.s))), down = T(1) / up;
+  C o[3][E];   // inverse transforms: (u, v), (w, 2^e oz), (ox, oy) at rows p + 16 i
+  load(f1s[0] + line * pin, f2s[0] + line * pin, T(1));
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     C v[E];
@@ -754,7 +760,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb)
       }
       v[i] = pack_pair<C, N>(n, y1, y2);
     }
-    if (r < 2) load(f1s[r + 1] + line * pin, f2s[r + 1] + line * pin);
+    if (r < 2) load(f1s[r + 1] + line * pin, f2s[r + 1] + line * pin, r == 0 ? up : T(1));
     xw_fft<T, PL, true, AD, N>(v, s, LDC, h, p, true, a.tw, twt);
 #pragma unroll
     for (int i = 0; i < E; ++i) o[r][i] = v[i];
@@ -765,7 +771,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb)
   T pz[E];
 #pragma unroll
   for (int i = 0; i < E; ++i) {
-    const T u = o[0][i].x, v = o[0][i].y, w = o[1][i].x, oz = o[1][i].y, ox = o[2][i].x, oy = o[2][i].y;
+    const T u = o[0][i].x, v = o[0][i].y, w = o[1][i].x, oz = o[1][i].y * down, ox = o[2][i].x, oy = o[2][i].y;
     f[i] = mkc<C>((oy * w - oz * v) * sc, (oz * u - ox * w) * sc);
     pz[i] = (ox * v - oy * u) * sc;
     m0 = fmax(m0, fabs(u));
