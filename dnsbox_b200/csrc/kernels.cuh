@@ -690,8 +690,9 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, N>::wpb)
 // memory holds only each sequence's one exchange (two columns per warp) and
 // the twiddle tables.  Hermitian-mirror rows, on input and output, come from
 // the partner lane by shuffle.
-template <typename T>
-__global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb)
+// MINB > 0: that many resident blocks per SM asked of the register allocator.
+template <typename T, int MINB = 0>
+__global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb, MINB)
     k_xline_nl_r(const __grid_constant__ XlineNLArgs<T> a) {
   constexpr int N = 256;
   using C = typename CT<T>::type;

@@ -152,11 +152,13 @@ cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaS
     const long long pairs = (a.nlines + 1) / 2;
     const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
     if constexpr (N == 256 && sizeof(T) == 4) {
-      if (variant == 3) {
-        // fields of a line in registers: two exchange columns per warp
+      if (variant == 3 || variant == 4) {
+        // fields of a line in registers: two exchange columns per warp (4: held to
+        // 128 registers for four blocks per SM)
         const size_t smem_r = ((size_t)WPB * 2 * LDC + XlineWarp<T, N>::twn) * sizeof(C);
-        if ((e = set_smem(k_xline_nl_r<T>, smem_r)) != cudaSuccess) return e;
-        k_xline_nl_r<T><<<nb, 32 * WPB, smem_r, st>>>(a);
+        auto kern = variant == 3 ? k_xline_nl_r<T> : k_xline_nl_r<T, 4>;
+        if ((e = set_smem(kern, smem_r)) != cudaSuccess) return e;
+        kern<<<nb, 32 * WPB, smem_r, st>>>(a);
         return cudaGetLastError();
       }
     }

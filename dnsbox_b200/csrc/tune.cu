@@ -131,7 +131,7 @@ extern "C" int dnsbox_set_schedule(dnsbox_ctx *ctx, const dnsbox_schedule *s) {
   for (int i = 0; i < 3; ++i)
     if (s->tc_kernel[i] < 0 || s->tc_kernel[i] > 2) return set_err(DNSBOX_ERR_ARG, "tc_kernel[0..2] must be 0 .. 2");
   if (s->tc_kernel[3] != 0 && s->tc_kernel[3] != 1) return set_err(DNSBOX_ERR_ARG, "tc_kernel[3] must be 0 or 1");
-  if (s->x_kernel < 0 || s->x_kernel > 3) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0 .. 3");
+  if (s->x_kernel < 0 || s->x_kernel > 4) return set_err(DNSBOX_ERR_ARG, "x_kernel must be 0 .. 4");
   apply(ctx, *s);
   return DNSBOX_OK;
 }
@@ -152,7 +152,7 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
     tc_opts.push_back(2);   // the FP32 SIMT kernel
   std::vector<int> x_opts = {0};
   if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1};
-  if (!fp64 && p.nx == 256) x_opts.push_back(3);
+  if (!fp64 && p.nx == 256) x_opts.insert(x_opts.end(), {3, 4});
   const dnsbox_schedule saved_sched = current(ctx);
   Saved sv;
   RET(save(ctx, sv));

@@ -329,7 +329,7 @@ class Box:
     def _sched_dict(sc, tc=True):
         return {"tc_kernel": [TC_KERNELS[v] if tc else "simt" for v in sc.tc_kernel[:3]],
                 "z_fwd_kernel": "tma" if sc.tc_kernel[3] else "simt",
-                "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-registers"}[sc.x_kernel], "tuned": bool(sc.tuned),
+                "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-registers", 4: "warp-registers-128"}[sc.x_kernel], "tuned": bool(sc.tuned),
                 "ms_default": sc.ms_default, "ms_tuned": sc.ms_tuned}
 
     def schedule(self) -> dict:
@@ -339,7 +339,7 @@ class Box:
 
     def set_schedule(self, tc_kernel=(0, 0, 0), x_kernel=0, z_fwd_tma=False):
         """tc_kernel: per pass A, B, D of the tensor-core form, 0 / "tma", 1 /
-        "cp.async" or 2 / "simt"; x_kernel 0 .. 3; z_fwd_tma: pass E1 on the
+        "cp.async" or 2 / "simt"; x_kernel 0 .. 4; z_fwd_tma: pass E1 on the
         TMA tensor-core kernel."""
         sc = _lib.Schedule()
         for i in range(3):

@@ -28,7 +28,7 @@ def test_every_schedule_matches_the_oracle(prec):
     # each kernel on each of passes A, B, D (TMA 0, cp.async 1, SIMT 2)
     tcs = [(0, 0, 0), (1, 1, 1), (2, 2, 2), (0, 1, 2), (2, 0, 1), (1, 2, 0)] if prec == "tc_split" else [(0, 0, 0)]
     for tc in tcs:
-        for xk in (0, 1, 2, 3):
+        for xk in (0, 1, 2, 3, 4):
             for zt in ((False, True) if prec == "tc_split" else (False,)):
                 b.set_schedule(tc, xk, zt)
                 got, _ = b.rhs_nonlinear(u)
