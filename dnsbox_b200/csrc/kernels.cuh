@@ -816,124 +816,6 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb, MINB)
   }
 }
 
-// Fused x pass at N = 512 with the fields of a line in registers (FP32):
-// a block of two 64-thread groups, group g owning line la + g.  With the
-// three-stage radix-8 plan (8 values a thread) a thread's first-stage input
-// rows and last-stage output rows are both n = p + 64 i, so the three
-// inverse sequences U + iV, W + i 2^e OZ, OX + i OY of a line, the cross
-// product and the forward inputs stay in registers as in k_xline_nl_r; the
-// Hermitian-mirror rows of the inputs are read from global memory, and the
-// unpacking of the forward transforms goes through the group's exchange
-// column.  Block barriers serve both groups (they run the same sequence).
-template <typename T>
-__global__ void __launch_bounds__(128) k_xline_nl_r512(const __grid_constant__ XlineNLArgs<T> a) {
-  constexpr int N = 512, H = N / 2 + 1;
-  using C = typename CT<T>::type;
-  using PL = FftPlan<N>;
-  using AD = AddrSkew<PL::R[0]>;
-  constexpr int E = PL::E;
-  constexpr int P = N / E;
-  static_assert(P == 64 && E == 8 && PL::R[0] == E && PL::R[PL::NST - 1] == E,
-                "rows n = p + 64 i at both ends of the transform");
-  constexpr int LDC = N + N / PL::R[0];
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *s = reinterpret_cast<C *>(smem_raw);    // two exchange columns
-  C *twt = s + 2 * LDC;                      // per-stage twiddle tables
-  tw_fill<C, PL>(twt, a.tw, threadIdx.x, blockDim.x);
-  __syncthreads();
-  const int g = threadIdx.x >> 6, p = threadIdx.x & 63;
-  const long long la = 2 * (long long)blockIdx.x;
-  if (la >= a.nlines) return;   // whole blocks (nlines is even)
-  const long long line = la + g;
-  const long long pin = a.pin ? a.pin : a.nxh, pout = a.pout ? a.pout : a.nxh;
-  const T sc = T(a.s);
-  const T up = (T)exp2(rint(-log2(a.s))), down = T(1) / up;   // see k_xline_nl_r
-  const TwShared<C> tw{twt};
-  const C *f1s[3] = {a.U, a.W, a.OX};
-  const C *f2s[3] = {a.V, a.OZ, a.OY};
-  C x1[E], x2[E];
-  auto load = [&](const C *g1, const C *g2, T up2) {
-#pragma unroll
-    for (int i = 0; i < E; ++i) {
-      const int n = p + P * i;
-      const int kk = n <= N / 2 ? n : N - n;
-      const bool kp = xkeep(a.kxa, kk, N);
-      x1[i] = kp ? g1[kk] : mkc<C>(0, 0);
-      const C y = kp ? g2[kk] : mkc<C>(0, 0);
-      x2[i] = mkc<C>(y.x * up2, y.y * up2);
-    }
-  };
-  C o[3][E];
-  load(f1s[0] + line * pin, f2s[0] + line * pin, T(1));
-#pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    C v[E];
-#pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = pack_pair<C, N>(p + P * i, x1[i], x2[i]);
-    if (r < 2) load(f1s[r + 1] + line * pin, f2s[r + 1] + line * pin, r == 0 ? up : T(1));
-    fft_regs_t<C, PL, true, false, AD>(v, s, LDC, g, p, true, tw);
-#pragma unroll
-    for (int i = 0; i < E; ++i) o[r][i] = v[i];
-  }
-  T m0 = 0, m1 = 0, m2 = 0;
-  C f[E];
-  T pz[E];
-#pragma unroll
-  for (int i = 0; i < E; ++i) {
-    const T u = o[0][i].x, v = o[0][i].y, w = o[1][i].x, oz = o[1][i].y * down, ox = o[2][i].x, oy = o[2][i].y;
-    f[i] = mkc<C>((oy * w - oz * v) * sc, (oz * u - ox * w) * sc);
-    pz[i] = (ox * v - oy * u) * sc;
-    m0 = fmax(m0, fabs(u));
-    m1 = fmax(m1, fabs(v));
-    m2 = fmax(m2, fabs(w));
-  }
-  // forward transform, then X1 / X2 of the two real transforms at k = p + 64 j
-  // (j <= 4) from the group's column: Z[k] and Z[N - k]
-  auto unpack_store = [&](C *d1, C *d2) {
-    C *col = s + g * LDC;
-#pragma unroll
-    for (int i = 0; i < E; ++i) col[AD::at(p + P * i, 0, LDC)] = f[i];
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j <= N / 2 / P; ++j) {
-      const int k = p + P * j;
-      if (k < H && xkeep(a.kxa, k, N)) {
-        const C zk = col[AD::at(k, 0, LDC)], zn = col[AD::at((N - k) % N, 0, LDC)];
-        if (d1) d1[k] = mkc<C>(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
-        if (d2) d2[k] = mkc<C>(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
-      }
-    }
-    __syncthreads();
-  };
-  fft_regs_t<C, PL, false, false, AD>(f, s, LDC, g, p, true, tw);
-  unpack_store(a.NX + line * pout, a.NY + line * pout);
-  // pz(a) + i pz(b): the partner group's pz through the columns
-  {
-    T *pzs = reinterpret_cast<T *>(s);   // 2 x N reals (within the two columns)
-#pragma unroll
-    for (int i = 0; i < E; ++i) pzs[g * N + p + P * i] = pz[i];
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < E; ++i) {
-      const T other = pzs[(1 - g) * N + p + P * i];
-      f[i] = g == 0 ? mkc<C>(pz[i], other) : mkc<C>(other, pz[i]);
-    }
-    __syncthreads();
-  }
-  fft_regs_t<C, PL, false, false, AD>(f, s, LDC, g, p, true, tw);
-  unpack_store(g == 0 ? a.NZ + line * pout : nullptr, g == 1 ? a.NZ + line * pout : nullptr);
-  // CFL maxima of the pair (both lines lie in one box: ny*nz is even)
-  m0 = warp_max(m0);
-  m1 = warp_max(m1);
-  m2 = warp_max(m2);
-  if ((threadIdx.x & 31) == 0 && a.st) {
-    double *um = a.st[la / a.lines_per_box].umax;
-    atomic_max_nonneg(um + 0, (double)m0 * a.s);
-    atomic_max_nonneg(um + 1, (double)m1 * a.s);
-    atomic_max_nonneg(um + 2, (double)m2 * a.s);
-  }
-}
-
 template <typename T> struct XlineArgs {
   using C = typename CT<T>::type;
   const void *in[6];

@@ -151,16 +151,6 @@ cudaError_t Launcher<T, N>::xline_nl(const XlineNLArgs<T> &a, int variant, cudaS
     cudaError_t e;
     const long long pairs = (a.nlines + 1) / 2;
     const unsigned nb = (unsigned)((pairs + WPB - 1) / WPB);
-    if constexpr (N == 512 && sizeof(T) == 4) {
-      if (variant == 3) {
-        // fields of a line in registers: two 64-thread line groups per block
-        constexpr int LD5 = N + N / FftPlan<N>::R[0];
-        const size_t smem_r = ((size_t)2 * LD5 + tw_size<FftPlan<N>>()) * sizeof(C);
-        if ((e = set_smem(k_xline_nl_r512<T>, smem_r)) != cudaSuccess) return e;
-        k_xline_nl_r512<T><<<(unsigned)pairs, 128, smem_r, st>>>(a);
-        return cudaGetLastError();
-      }
-    }
     if constexpr (N == 256 && sizeof(T) == 4) {
       if (variant == 3 || variant == 4) {
         // fields of a line in registers: two exchange columns per warp (4: held to

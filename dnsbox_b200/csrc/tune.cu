@@ -153,7 +153,6 @@ extern "C" int dnsbox_autotune(dnsbox_ctx *ctx, const void *uh, int nsteps, dnsb
   std::vector<int> x_opts = {0};
   if (fp64 ? Ops<double>::has_xline_warp(p.nx) : Ops<float>::has_xline_warp(p.nx)) x_opts = {2, 1};
   if (!fp64 && p.nx == 256) x_opts.insert(x_opts.end(), {3, 4});
-  if (!fp64 && p.nx == 512) x_opts.push_back(3);
   const dnsbox_schedule saved_sched = current(ctx);
   Saved sv;
   RET(save(ctx, sv));

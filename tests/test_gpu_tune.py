@@ -64,21 +64,3 @@ def test_autotune_keeps_state_clock_and_caches(prec):
     b.close()
     c.close()
 
-
-def test_x_kernels_at_512_agree():
-    """At 512 in FP32 the register x kernel (schedule choice 3) against the
-    warp kernel (2), whose 256^3 parity with the oracle the test above checks:
-    the same right-hand side within the FP32 bar."""
-    from dnsbox_b200.ops import Box
-    n = 512
-    kw = dict(nu=8e-4, kCutOff=2.5, Pin=0.1, bandlim=True)
-    b = Box(n, precision="fp32", **kw)
-    from dnsbox_b200.ic import random_field_gpu
-    u = random_field_gpu(b, seed=4, k0=3.0)
-    out = {}
-    for xk in (2, 3):
-        b.set_schedule((2, 2, 2), xk, False)
-        got, _ = b.rhs_nonlinear(u)
-        out[xk] = got.to(torch.complex128)
-    assert float((out[3] - out[2]).abs().norm() / out[2].abs().norm()) < 2e-6
-    b.close()
