@@ -962,8 +962,16 @@ template <typename T> struct FinishArgs {
 // launch does not visit as zero.  Each lane batches the global operands of
 // two modes before any store.  MODE (a FinishMode) is a template parameter so
 // that only the operands of the update in use occupy registers.
+// Resident blocks per SM asked of the register allocator: the FP32
+// corrector and AB2 finishes (115-120 registers, two blocks) are held to
+// three blocks.
+template <typename T, int MODE> struct FinishMinB {
+  static constexpr int v = (sizeof(T) == 4 && (MODE == 2 || MODE == 3)) ? 3 : 0;
+};
+
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_finish_rows(const __grid_constant__ FinishArgs<T> a, int nrows) {
+__global__ void __launch_bounds__(256, FinishMinB<T, MODE>::v)
+    k_finish_rows(const __grid_constant__ FinishArgs<T> a, int nrows) {
   using C = typename CT<T>::type;
   constexpr int CH = 2;
   const int lane = threadIdx.x & 31;
