@@ -265,7 +265,7 @@ def force_tc(box, prec, sched):
     if not prec.endswith("@tc"):
         return sched
     tc = tuple("cp.async" if v == "simt" else v for v in sched["tc_kernel"])
-    box.set_schedule(tc, {"default": 0, "block": 1, "warp": 2, "warp-registers": 3, "warp-registers-128": 4}[sched["x_kernel"]],
+    box.set_schedule(tc, sched["x_kernel"],
                      sched["z_fwd_kernel"] == "tma")
     return dict(box.schedule(), tuned=False)
 

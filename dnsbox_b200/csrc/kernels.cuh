@@ -718,14 +718,13 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb, MINB)
   const int mirror = (lane & 16) | ((16 - p) & 15);
   // rows n = p + 16 i <= N / 2 of the two half lines of a sequence
   C x1[E / 2 + 1], x2[E / 2 + 1];
-  auto load = [&](const C *g1, const C *g2, T up2) {
+  auto load = [&](const C *g1, const C *g2) {
 #pragma unroll
     for (int i = 0; i <= E / 2; ++i) {
       const int n = p + P * i;
       const bool kp = (i < E / 2 || p == 0) && xkeep(a.kxa, n, N);
       x1[i] = kp ? g1[n] : mkc<C>(0, 0);
-      const C y = kp ? g2[n] : mkc<C>(0, 0);
-      x2[i] = mkc<C>(y.x * up2, y.y * up2);
+      x2[i] = kp ? g2[n] : mkc<C>(0, 0);
     }
   };
   // value at row N - (p + 16 i) of a lane's rows from w (own rows): the partner
@@ -735,16 +734,38 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb, MINB)
   };
   const C *f1s[3] = {a.U, a.W, a.OX};
   const C *f2s[3] = {a.V, a.OZ, a.OY};
-  // The vorticity fields carry the factor s of the spectral curl, the
-  // velocity fields do not: W and OZ share a sequence, so OZ is brought to
-  // W's magnitude by the power of two nearest 1/s (exact both ways) before
-  // the transform, which would otherwise round it relative to W.
-  const T up = (T)exp2(rint(-log2(a.s))), down = T(1) / up;
+  // W and OZ share a sequence, and the vorticity is larger than the velocity
+  // by the factor s of the spectral curl and by the wavenumbers of the field:
+  // the transform would round OZ's part relative to W's, so each line's OZ is
+  // first brought to its W's magnitude by a power of two (exact both ways),
+  // the exponent difference of the two half lines' largest components.
+  T up = 1, down = 1;
   C o[3][E];   // inverse transforms: (u, v), (w, 2^e oz), (ox, oy) at rows p + 16 i
-  load(f1s[0] + line * pin, f2s[0] + line * pin, T(1));
+  load(f1s[0] + line * pin, f2s[0] + line * pin);
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     C v[E];
+    if (r == 1) {
+      T mw = 0, mo = 0;
+#pragma unroll
+      for (int i = 0; i <= E / 2; ++i) {
+        mw = fmax(mw, fmax(fabs(x1[i].x), fabs(x1[i].y)));
+        mo = fmax(mo, fmax(fabs(x2[i].x), fabs(x2[i].y)));
+      }
+#pragma unroll
+      for (int o = 8; o; o >>= 1) {   // the 16 lanes of this line
+        mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+        mo = fmax(mo, __shfl_xor_sync(0xffffffffu, mo, o));
+      }
+      int ew = 0, eo = 0;
+      frexp(mw, &ew);
+      frexp(mo, &eo);
+      const int d = mw > 0 && mo > 0 ? max(-96, min(96, ew - eo)) : 0;
+      up = ldexp(T(1), d);
+      down = ldexp(T(1), -d);
+#pragma unroll
+      for (int i = 0; i <= E / 2; ++i) x2[i] = mkc<C>(x2[i].x * up, x2[i].y * up);
+    }
 #pragma unroll
     for (int i = 0; i < E; ++i) {
       const int n = p + P * i;
@@ -761,7 +782,7 @@ __global__ void __launch_bounds__(32 * XlineWarp<T, 256>::wpb, MINB)
       }
       v[i] = pack_pair<C, N>(n, y1, y2);
     }
-    if (r < 2) load(f1s[r + 1] + line * pin, f2s[r + 1] + line * pin, r == 0 ? up : T(1));
+    if (r < 2) load(f1s[r + 1] + line * pin, f2s[r + 1] + line * pin);
     xw_fft<T, PL, true, AD, N>(v, s, LDC, h, p, true, a.tw, twt);
 #pragma unroll
     for (int i = 0; i < E; ++i) o[r][i] = v[i];

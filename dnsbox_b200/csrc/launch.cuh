@@ -22,8 +22,9 @@ template <typename T, int N> struct Launcher {
   static cudaError_t strided_tma(const TmaArgs &a, bool inv, const void *adft, int *status, int nctas,
                                  cudaStream_t st);
   static bool has_tma();
-  // variant: 0 the default kernel for N, 1 the block kernel, 2 the warp kernel, 3 the warp kernel held
-  // to the registers of four resident blocks per SM (2 and 3 where the warp kernel exists)
+  // variant: 0 the default kernel for N, 1 the block kernel, 2 the warp kernel, 3 the warp kernel with
+  // each line's fields in registers (N = 256, FP32), 4 the same held to the registers of four resident
+  // blocks per SM; 3 and 4 run the warp kernel at other sizes
   static cudaError_t xline_nl(const XlineNLArgs<T> &a, int variant, cudaStream_t st);
   static bool has_xline_warp();
   static cudaError_t xline_c2r(const XlineArgs<T> &a, int nf, cudaStream_t st);

@@ -36,6 +36,7 @@ from .grid import nspec as _nspec
 PRECISION = {"fp64": 0, "fp32": 1, "tc_split": 2}
 STEPPER = {"heun": 0, "ab2": 1, "semi_implicit": 2}
 TC_KERNELS = ("tma", "cp.async", "simt")   # per strided pass of the tensor-core form
+X_KERNELS = ("default", "block", "warp", "warp-registers", "warp-registers-128")   # the fused x pass
 AB2_MODE = {"reference": 0, "standard": 1}
 SPECTRUM_MODE = {"mpi": 0, "single": 1}
 ADJ_PHAT = {"intent": 0, "literal": 1}
@@ -329,7 +330,7 @@ class Box:
     def _sched_dict(sc, tc=True):
         return {"tc_kernel": [TC_KERNELS[v] if tc else "simt" for v in sc.tc_kernel[:3]],
                 "z_fwd_kernel": "tma" if sc.tc_kernel[3] else "simt",
-                "x_kernel": {0: "default", 1: "block", 2: "warp", 3: "warp-registers", 4: "warp-registers-128"}[sc.x_kernel], "tuned": bool(sc.tuned),
+                "x_kernel": X_KERNELS[sc.x_kernel], "tuned": bool(sc.tuned),
                 "ms_default": sc.ms_default, "ms_tuned": sc.ms_tuned}
 
     def schedule(self) -> dict:
@@ -339,14 +340,14 @@ class Box:
 
     def set_schedule(self, tc_kernel=(0, 0, 0), x_kernel=0, z_fwd_tma=False):
         """tc_kernel: per pass A, B, D of the tensor-core form, 0 / "tma", 1 /
-        "cp.async" or 2 / "simt"; x_kernel 0 .. 4; z_fwd_tma: pass E1 on the
+        "cp.async" or 2 / "simt"; x_kernel 0 .. 4 (or its name); z_fwd_tma: pass E1 on the
         TMA tensor-core kernel."""
         sc = _lib.Schedule()
         for i in range(3):
             v = tc_kernel[i]
             sc.tc_kernel[i] = TC_KERNELS.index(v) if isinstance(v, str) else int(v)
         sc.tc_kernel[3] = int(bool(z_fwd_tma))
-        sc.x_kernel = int(x_kernel)
+        sc.x_kernel = X_KERNELS.index(x_kernel) if isinstance(x_kernel, str) else int(x_kernel)
         _lib.check(self._lib.dnsbox_set_schedule(self._h, ctypes.byref(sc)))
 
     def autotune(self, uh: torch.Tensor, nsteps: int = 4) -> dict:

@@ -318,7 +318,8 @@ typedef struct dnsbox_schedule {
                              (forward z): 0 SIMT (the default), 1 TMA-staged tensor-core kernel */
   int32_t x_kernel;       /* fused x pass: 0 default for the size, 1 block kernel, 2 warp kernel,
                              3 (N = 256, FP32) warp kernel with each line's fields in registers,
-                             4 the same held to 128 registers (four blocks per SM) */
+                             4 the same held to 128 registers (four blocks per SM); 3 and 4 run the
+                             warp kernel at other sizes */
   int32_t tuned;          /* 1 when chosen by dnsbox_autotune */
   double ms_default;      /* step time of the default schedule in the tuning run (ms) */
   double ms_tuned;        /* step time of the chosen schedule (ms) */
