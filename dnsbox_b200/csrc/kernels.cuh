@@ -170,7 +170,12 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
   const int tile = blockIdx.x / a.njobs;
   int kx0, other;
   strided_tile(a, tile, TC, kx0, other);
-  const StridedJob<T> &J = a.job[job];
+  // the job's fields, read from the parameter bank once (an indexed
+  // parameter read each time they are used measured as a busy ADU pipe)
+  const C *const in1p = a.job[job].in1, *const in2p = a.job[job].in2;
+  C *const outp = a.job[job].out;
+  const double ja1 = a.job[job].a1, jb1 = a.job[job].b1, ja2 = a.job[job].a2, jb2 = a.job[job].b2;
+  const int ks1 = a.job[job].ks1, ks2 = a.job[job].ks2;
   const bool act = threadIdx.x < NF;
   const int col = threadIdx.x % TC, p = threadIdx.x / TC;
   const int kx = strided_col(a, kx0 + col);
@@ -181,19 +186,19 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
   // evaluates them per element, which keeps its kernel at 128 registers)
   constexpr bool TAB = sizeof(T) == 4;
   __shared__ T bks[2][TAB ? N : 1];
-  const bool mult1 = !(J.a1 == 1.0 && J.b1 == 0.0);
-  if (TAB && ((mult1 && J.ks1 == 1) || (J.in2 && J.ks2 == 1))) {
+  const bool mult1 = !(ja1 == 1.0 && jb1 == 0.0);
+  if (TAB && ((mult1 && ks1 == 1) || (in2p && ks2 == 1))) {
     for (int n = threadIdx.x; n < N; n += blockDim.x) {
       const double k = k_full(n, N, a.alpha_row);
-      bks[0][n] = T(J.b1 * k);
-      bks[1][n] = T(J.b2 * k);
+      bks[0][n] = T(jb1 * k);
+      bks[1][n] = T(jb2 * k);
     }
     __syncthreads();
   }
   C v[E];
   if (valid) {
     // all E loads of the first stage are independent and issued together
-    const C *in1 = J.in1 + base;
+    const C *in1 = in1p + base;
 #pragma unroll
     for (int i = 0; i < E; ++i)
       v[i] = a.krin.keep(EN::in_row(p, i)) ? in1[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
@@ -202,37 +207,37 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
     const double koth = a.n_other ? k_full(other, a.n_other, a.alpha_other) : 0.0;
     if constexpr (TAB) {
       if (mult1) {
-        const T aa = T(J.a1), bkc = T(J.b1 * (J.ks1 == 2 ? koth : kcol));
+        const T aa = T(ja1), bkc = T(jb1 * (ks1 == 2 ? koth : kcol));
 #pragma unroll
         for (int i = 0; i < E; ++i) {
-          const T bk = J.ks1 == 1 ? bks[0][EN::in_row(p, i)] : bkc;
+          const T bk = ks1 == 1 ? bks[0][EN::in_row(p, i)] : bkc;
           v[i] = mkc<C>(v[i].x * aa - v[i].y * bk, v[i].y * aa + v[i].x * bk);
         }
       }
-      if (J.in2) {
-        const C *in2 = J.in2 + base;
-        const T aa = T(J.a2), bkc = T(J.b2 * (J.ks2 == 2 ? koth : kcol));
+      if (in2p) {
+        const C *in2 = in2p + base;
+        const T aa = T(ja2), bkc = T(jb2 * (ks2 == 2 ? koth : kcol));
 #pragma unroll
         for (int i = 0; i < E; ++i) {
           const C w = a.krin.keep(EN::in_row(p, i)) ? in2[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
-          const T bk = J.ks2 == 1 ? bks[1][EN::in_row(p, i)] : bkc;
+          const T bk = ks2 == 1 ? bks[1][EN::in_row(p, i)] : bkc;
           v[i] = cadd(v[i], mkc<C>(w.x * aa - w.y * bk, w.y * aa + w.x * bk));
         }
       }
     } else {
       if (mult1) {
-        const double kc = J.ks1 == 2 ? koth : kcol;
+        const double kc = ks1 == 2 ? koth : kcol;
 #pragma unroll
         for (int i = 0; i < E; ++i)
-          v[i] = apply_mult<T>(v[i], J.a1, J.b1, J.ks1 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc);
+          v[i] = apply_mult<T>(v[i], ja1, jb1, ks1 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc);
       }
-      if (J.in2) {
-        const C *in2 = J.in2 + base;
-        const double kc = J.ks2 == 2 ? koth : kcol;
+      if (in2p) {
+        const C *in2 = in2p + base;
+        const double kc = ks2 == 2 ? koth : kcol;
 #pragma unroll
         for (int i = 0; i < E; ++i) {
           const C w = a.krin.keep(EN::in_row(p, i)) ? in2[(long long)EN::in_row(p, i) * a.rowstride] : mkc<C>(0, 0);
-          v[i] = cadd(v[i], apply_mult<T>(w, J.a2, J.b2, J.ks2 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc));
+          v[i] = cadd(v[i], apply_mult<T>(w, ja2, jb2, ks2 == 1 ? k_full(EN::in_row(p, i), N, a.alpha_row) : kc));
         }
       }
     }
@@ -243,7 +248,7 @@ __global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), 
   fft_regs<C, N, INV>(v, s, TC, col, p, act, a.tw);
   if (valid) {
     const long long rso = out_rowstride(a);
-    C *out = J.out + ((long long)other * out_otherstride(a) + kx + (long long)blockIdx.y * out_bstride(a));
+    C *out = outp + ((long long)other * out_otherstride(a) + kx + (long long)blockIdx.y * out_bstride(a));
 #pragma unroll
     for (int i = 0; i < E; ++i)
       if (a.krout.keep(EN::out_row(p, i))) out[(long long)EN::out_row(p, i) * rso] = v[i];
