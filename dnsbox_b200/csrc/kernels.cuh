@@ -129,15 +129,22 @@ __host__ __device__ __forceinline__ int strided_col(const StridedArgs<T> &a, int
   return (a.nyq_tile < 0 && kx == a.kcol.a) ? (a.kcol.n >> 1) : kx;
 }
 
+// Columns per CTA of the SIMT strided kernel: the host's tile width, or (FP32,
+// N >= 512, whose plans give 64 threads per column) half a tile, so that a
+// CTA has 512 threads instead of 1024 and two fit an SM side by side.
+template <typename T, int N> struct StridedCols {
+  static constexpr int v = (sizeof(T) == 4 && N >= 512) ? TileCols<T>::v / 2 : TileCols<T>::v;
+};
+
 // Resident CTAs of a strided launch to ask the register allocator for: FP32
 // blocks of up to 256 threads whose plans hold at most 16 values a thread
 // are held to 64 registers a thread (the load-latency-bound passes gain more
 // from the extra warps than they lose to the tighter allocation); 0 leaves
 // the choice to the compiler.
 template <typename T, int N> struct StridedMinCtas {
-  static constexpr int NT = round32(TileCols<T>::v * (N / FftPlan<N>::E));
+  static constexpr int NT = round32(StridedCols<T, N>::v * (N / FftPlan<N>::E));
   static constexpr int v = (sizeof(T) == 4 && NT <= 256 && FftPlan<N>::E <= 16) ? 1024 / NT
-                         : 0;
+                         : (sizeof(T) == 4 && NT == 512) ? 2 : 0;
 };
 
 // Column origin and other-axis index of tile t of the (possibly pruned) grid.
@@ -157,19 +164,24 @@ __device__ __forceinline__ C apply_mult(C v, double a, double b, double k) {
 }
 
 template <typename T, int N, bool INV>
-__global__ void __launch_bounds__(round32(TileCols<T>::v *(N / FftPlan<N>::E)), StridedMinCtas<T, N>::v)
+__global__ void __launch_bounds__(round32(StridedCols<T, N>::v *(N / FftPlan<N>::E)), StridedMinCtas<T, N>::v)
     k_strided(const __grid_constant__ StridedArgs<T> a) {
   using C = typename CT<T>::type;
   using EN = FftEnds<N>;
-  constexpr int TC = TileCols<T>::v;
+  constexpr int TC = StridedCols<T, N>::v;    // columns of this CTA
+  constexpr int SPLIT = TileCols<T>::v / TC;  // CTAs per tile of the host's grid
   constexpr int E = EN::E;
-  constexpr int NF = TC * (N / E);   // FFT threads: column fastest, 128 B per row
+  constexpr int NF = TC * (N / E);   // FFT threads: column fastest
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s = reinterpret_cast<C *>(smem_raw);
-  const int job = blockIdx.x % a.njobs;
-  const int tile = blockIdx.x / a.njobs;
+  // block (tile, job, part): the parts of a tile are adjacent blocks, so they
+  // read the two halves of the same 128-byte row segments at about one time
+  const int part = blockIdx.x % SPLIT, tj = blockIdx.x / SPLIT;
+  const int job = tj % a.njobs;
+  const int tile = tj / a.njobs;
   int kx0, other;
-  strided_tile(a, tile, TC, kx0, other);
+  strided_tile(a, tile, TileCols<T>::v, kx0, other);
+  kx0 += part * TC;
   // the job's fields, read from the parameter bank once (an indexed
   // parameter read each time they are used measured as a busy ADU pipe)
   const C *const in1p = a.job[job].in1, *const in2p = a.job[job].in2;

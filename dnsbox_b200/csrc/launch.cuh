@@ -45,15 +45,16 @@ static cudaError_t set_smem(K kernel, size_t bytes) {
 }
 
 template <typename T, int N> int Launcher<T, N>::strided_threads() {
-  return round32(TileCols<T>::v * (N / FftPlan<N>::E));
+  return round32(StridedCols<T, N>::v * (N / FftPlan<N>::E));
 }
 
 template <typename T, int N>
 cudaError_t Launcher<T, N>::strided(const StridedArgs<T> &a, bool inv, int ntiles, cudaStream_t st) {
   using C = typename CT<T>::type;
-  const size_t smem = (size_t)N * TileCols<T>::v * sizeof(C);
+  const size_t smem = (size_t)N * StridedCols<T, N>::v * sizeof(C);
   const int nt = strided_threads();
-  const dim3 nb((unsigned)ntiles * a.njobs, (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
+  const dim3 nb((unsigned)ntiles * a.njobs * (TileCols<T>::v / StridedCols<T, N>::v),
+                (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
   cudaError_t e;
   if (inv) {
     if ((e = set_smem(k_strided<T, N, true>, smem)) != cudaSuccess) return e;

@@ -345,11 +345,12 @@ def test_rhs_nonlinear_512_properties():
     assert float((N32.to(torch.complex128) - N64).abs().norm() / N64.abs().norm()) < 2e-6
 
 
-# ---------------------------------------------------------------- 1024-point axes
+# ---------------------------------------------------------------- 512- and 1024-point axes
 @pytest.mark.parametrize("prec", ["fp64", "fp32", "tc_split"])
-@pytest.mark.parametrize("shape", [(1024, 16, 16), (16, 1024, 16), (16, 16, 1024)])
-def test_axes_of_1024(prec, shape):
-    """Every pass at its largest size on small boxes (one axis of 1024): the
+@pytest.mark.parametrize("shape", [(1024, 16, 16), (16, 1024, 16), (16, 16, 1024), (16, 512, 24), (24, 16, 512)])
+def test_long_axes(prec, shape):
+    """Every pass at its largest sizes on small boxes (one axis of 512 or
+    1024, where the FP32 strided kernel splits a tile over two CTAs): the
     transforms against pocketfft and one right-hand side against the oracle."""
     nx, ny, nz = shape
     from dnsbox_b200.ops import Box
