@@ -129,22 +129,25 @@ __host__ __device__ __forceinline__ int strided_col(const StridedArgs<T> &a, int
   return (a.nyq_tile < 0 && kx == a.kcol.a) ? (a.kcol.n >> 1) : kx;
 }
 
-// Columns per CTA of the SIMT strided kernel: the host's tile width, or (FP32,
-// N >= 512, whose plans give 64 threads per column) half a tile, so that a
-// CTA has 512 threads instead of 1024 and two fit an SM side by side.
+// Columns per CTA of the SIMT strided kernel: the host's tile width, or at
+// N >= 512 (plans of 64 threads per column) half a tile, so that a CTA has
+// 512 (FP32) or 256 (FP64) threads and several CTAs share an SM, each with
+// its own barriers.
 template <typename T, int N> struct StridedCols {
-  static constexpr int v = (sizeof(T) == 4 && N >= 512) ? TileCols<T>::v / 2 : TileCols<T>::v;
+  static constexpr int v = N >= 512 ? TileCols<T>::v / 2 : TileCols<T>::v;
 };
 
 // Resident CTAs of a strided launch to ask the register allocator for: FP32
 // blocks of up to 256 threads whose plans hold at most 16 values a thread
 // are held to 64 registers a thread (the load-latency-bound passes gain more
-// from the extra warps than they lose to the tighter allocation); 0 leaves
-// the choice to the compiler.
+// from the extra warps than they lose to the tighter allocation), 512-thread
+// FP32 blocks to two per SM and the 256-thread FP64 blocks of N = 512 to
+// three (80 registers, a few spills: 24% off the inverse y pass at 512^3);
+// 0 leaves the choice to the compiler.
 template <typename T, int N> struct StridedMinCtas {
   static constexpr int NT = round32(StridedCols<T, N>::v * (N / FftPlan<N>::E));
   static constexpr int v = (sizeof(T) == 4 && NT <= 256 && FftPlan<N>::E <= 16) ? 1024 / NT
-                         : (sizeof(T) == 4 && NT == 512) ? 2 : 0;
+                         : (sizeof(T) == 4 && NT == 512) ? 2 : (sizeof(T) == 8 && N == 512) ? 3 : 0;
 };
 
 // Column origin and other-axis index of tile t of the (possibly pruned) grid.
