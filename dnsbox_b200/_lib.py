@@ -137,6 +137,13 @@ SIGNATURES = {
     "dnsbox_set_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(Schedule)]),
     "dnsbox_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.POINTER(Schedule)]),
     "dnsbox_profile_read": (ctypes.c_int, [_VP, ctypes.POINTER(Profile), ctypes.c_int]),
+    "dnsbox_slab_create": (ctypes.c_int, [ctypes.c_int] * 7 + [ctypes.POINTER(_VP)]),
+    "dnsbox_slab_destroy": (None, [_VP]),
+    "dnsbox_slab_dims": (ctypes.c_int, [_VP] + [ctypes.POINTER(ctypes.c_int)] * 4 + [ctypes.POINTER(ctypes.c_size_t)]),
+    "dnsbox_slab_ftran_local": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "dnsbox_slab_ftran_finish": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "dnsbox_slab_btran_local": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "dnsbox_slab_btran_finish": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
 }
 
 _lib = None

@@ -1,0 +1,143 @@
+"""Slab-decomposed 3D FFT over ranks, one GPU each (``dnsbox_slab_*``).
+
+The reference distributes a box with p3dfft's one-dimensional decomposition
+(variables.f90:131-157, processor grid 1 x nproc): physical fields in slabs of
+nz/P z-planes, spectral fields in slabs of ny/P ky rows, and one MPI all-to-all
+inside every p3dfft_ftran_r2c / p3dfft_btran_c2r (dnsbox.f90:44-46, 229-231).
+``SlabFFT`` is that transform on B200s: the library runs the local passes on
+this rank's GPU and the exchange between them is one all-to-all of P equal
+blocks, NCCL over NVLink through ``torch.distributed``.
+
+Layouts (row-major, innermost last):
+
+* physical slab ``(nz/P, ny, nx)`` real, planes ``[rank nz/P, (rank+1) nz/P)``;
+* spectral slab ``(nz, ny/P, nx/2+1)`` complex, ky rows ``[rank ny/P, ...)``.
+
+Transforms are unnormalised, as ``Box.r2c`` / ``Box.c2r`` and p3dfft's.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from .ops import PRECISION
+
+
+def slab_extents(nx: int, ny: int, nz: int, nranks: int, rank: int) -> dict:
+    """(z, y, x) starts and sizes of a rank's physical and spectral slabs
+    (p3dfft_get_dims, 0-based) and the complex elements of one exchange block."""
+    if nranks < 1 or not 0 <= rank < nranks:
+        raise ValueError(f"rank {rank} of {nranks}")
+    if ny % nranks or nz % nranks:
+        raise ValueError(f"{nranks} ranks do not divide ny = {ny} and nz = {nz}")
+    nzl, nyl, nxh = nz // nranks, ny // nranks, nx // 2 + 1
+    return {"phys_start": (rank * nzl, 0, 0), "phys_size": (nzl, ny, nx),
+            "spec_start": (0, rank * nyl, 0), "spec_size": (nz, nyl, nxh),
+            "block_elems": nzl * nyl * nxh}
+
+
+def all_to_all(send: torch.Tensor, recv: torch.Tensor, group=None) -> None:
+    """Block q of this rank's ``send`` to rank q, arriving as block r of its
+    ``recv`` for sender r (P equal blocks along dim 0).  Without a process
+    group: a copy."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        recv.copy_(send)
+        return
+    s = torch.view_as_real(send) if send.is_complex() else send
+    r = torch.view_as_real(recv) if recv.is_complex() else recv
+    dist.all_to_all_single(r.reshape(-1), s.reshape(-1), group=group)
+
+
+class SlabFFT:
+    """This rank's part of a slab-decomposed (nx, ny, nz) transform.
+
+    ``rank`` / ``nranks`` default to the process group's; ``exchange`` (default
+    :func:`all_to_all` over ``group``) moves the blocks between the local
+    halves.  ``r2c`` / ``c2r`` run local half, exchange, finishing half on
+    torch's current stream."""
+
+    def __init__(self, nx: int, ny: int, nz: int, precision: str = "fp64", group=None, rank=None, nranks=None,
+                 device=None, exchange=None):
+        import torch.distributed as dist
+        dist_on = dist.is_available() and dist.is_initialized()
+        self.rank = int(rank) if rank is not None else (dist.get_rank(group) if dist_on else 0)
+        self.nranks = int(nranks) if nranks is not None else (dist.get_world_size(group) if dist_on else 1)
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.nx, self.ny, self.nz, self.precision = nx, ny, nz, precision
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else int(device))
+        self.rdtype = torch.float64 if precision == "fp64" else torch.float32
+        self.cdtype = torch.complex128 if precision == "fp64" else torch.complex64
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.dnsbox_slab_create(nx, ny, nz, self.nranks, self.rank, PRECISION[precision],
+                                                self.device.index, ctypes.byref(h)))
+        self._h = h
+        ps, pz, ss, sz = ((ctypes.c_int * 3)() for _ in range(4))
+        blk = ctypes.c_size_t()
+        _lib.check(self._lib.dnsbox_slab_dims(self._h, ps, pz, ss, sz, ctypes.byref(blk)))
+        self.phys_start, self.phys_size = tuple(ps), tuple(pz)
+        self.spec_start, self.spec_size = tuple(ss), tuple(sz)
+        self.block_elems = blk.value
+        self.send = torch.empty((self.nranks, self.block_elems), dtype=self.cdtype, device=self.device)
+        self.recv = torch.empty_like(self.send)
+        self._group = group
+        self._exchange = exchange if exchange is not None else (lambda s, r: all_to_all(s, r, group))
+
+    # -- the halves (the exchange between them is the caller's in these) --
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _check(self, t: torch.Tensor, shape, dtype, what: str):
+        if t.device != self.device or t.dtype != dtype or tuple(t.shape) != tuple(shape) or not t.is_contiguous():
+            raise ValueError(f"{what}: expected contiguous {dtype} {tuple(shape)} on {self.device}, "
+                             f"got {t.dtype} {tuple(t.shape)} on {t.device}")
+
+    def forward_local(self, phys: torch.Tensor) -> None:
+        self._check(phys, self.phys_size, self.rdtype, "physical slab")
+        _lib.check(self._lib.dnsbox_slab_ftran_local(self._h, ctypes.c_void_p(phys.data_ptr()),
+                                                     ctypes.c_void_p(self.send.data_ptr()), self._stream()))
+
+    def forward_finish(self, spec: torch.Tensor) -> None:
+        self._check(spec, self.spec_size, self.cdtype, "spectral slab")
+        _lib.check(self._lib.dnsbox_slab_ftran_finish(self._h, ctypes.c_void_p(self.recv.data_ptr()),
+                                                      ctypes.c_void_p(spec.data_ptr()), self._stream()))
+
+    def backward_local(self, spec: torch.Tensor) -> None:
+        self._check(spec, self.spec_size, self.cdtype, "spectral slab")
+        _lib.check(self._lib.dnsbox_slab_btran_local(self._h, ctypes.c_void_p(spec.data_ptr()),
+                                                     ctypes.c_void_p(self.send.data_ptr()), self._stream()))
+
+    def backward_finish(self, phys: torch.Tensor) -> None:
+        self._check(phys, self.phys_size, self.rdtype, "physical slab")
+        _lib.check(self._lib.dnsbox_slab_btran_finish(self._h, ctypes.c_void_p(self.recv.data_ptr()),
+                                                      ctypes.c_void_p(phys.data_ptr()), self._stream()))
+
+    # -- whole transforms (p3dfft_ftran_r2c / p3dfft_btran_c2r) --
+    def r2c(self, phys: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        spec = out if out is not None else torch.empty(self.spec_size, dtype=self.cdtype, device=self.device)
+        self.forward_local(phys)
+        self._exchange(self.send, self.recv)
+        self.forward_finish(spec)
+        return spec
+
+    def c2r(self, spec: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        phys = out if out is not None else torch.empty(self.phys_size, dtype=self.rdtype, device=self.device)
+        self.backward_local(spec)
+        self._exchange(self.send, self.recv)
+        self.backward_finish(phys)
+        return phys
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.dnsbox_slab_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

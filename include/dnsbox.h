@@ -188,6 +188,38 @@ int dnsbox_c2r(dnsbox_ctx *ctx, const void *spec_dev, void *phys_dev);
 int dnsbox_c2r_noalloc(int nx, int ny, int nz, int precision, const void *spec_dev, void *phys_dev,
                        void *cuda_stream);
 
+/* ---- slab-decomposed 3D FFT over ranks --------------------------------- */
+/* p3dfft's one-dimensional decomposition (variables.f90:131-157, processor
+ * grid 1 x nranks; p3dfft_ftran_r2c / p3dfft_btran_c2r, dnsbox.f90:44-46,
+ * 229-231), one GPU per rank.  Physical slab: (nz/P, ny, nx) reals, z-planes
+ * [rank nz/P, (rank+1) nz/P); spectral slab: (nz, ny/P, nx/2+1) complex, ky
+ * rows [rank ny/P, (rank+1) ny/P); P = nranks must divide ny and nz.  Each
+ * transform is a local half, an all-to-all of P equal blocks that the CALLER
+ * runs (block q of every rank's send buffer to rank q, arriving as block r of
+ * its recv buffer for sender r; NCCL through torch.distributed in the Python
+ * binding), and a finishing half; the library does no communication.  send /
+ * recv: P * block_elems complex elements of the precision, device memory.
+ * Transforms are unnormalised (as dnsbox_r2c / dnsbox_c2r).  Work runs on
+ * `stream` (NULL: the default stream) on the slab's device.
+ * Replaces p3dfft_setup / p3dfft_get_dims / p3dfft_ftran_r2c /
+ * p3dfft_btran_c2r of the reference's distributed runs. */
+typedef struct dnsbox_slab dnsbox_slab;
+int dnsbox_slab_create(int nx, int ny, int nz, int nranks, int rank, int precision, int device,
+                       dnsbox_slab **out);
+void dnsbox_slab_destroy(dnsbox_slab *slab);
+/* (z, y, x)-ordered starts and sizes of this rank's physical and spectral
+ * slabs (0-based), and the complex elements of one exchange block */
+int dnsbox_slab_dims(const dnsbox_slab *slab, int phys_start[3], int phys_size[3], int spec_start[3],
+                     int spec_size[3], size_t *block_elems);
+/* forward: x R2C and y FFT of the physical slab, packed by destination rank */
+int dnsbox_slab_ftran_local(dnsbox_slab *slab, const void *phys_dev, void *send_dev, void *cuda_stream);
+/* forward: z FFT of the received blocks into the spectral slab */
+int dnsbox_slab_ftran_finish(dnsbox_slab *slab, const void *recv_dev, void *spec_dev, void *cuda_stream);
+/* inverse: z FFT of the spectral slab into the send buffer (block q: planes of rank q) */
+int dnsbox_slab_btran_local(dnsbox_slab *slab, const void *spec_dev, void *send_dev, void *cuda_stream);
+/* inverse: unpack the received ky rows, y FFT and x C2R into the physical slab */
+int dnsbox_slab_btran_finish(dnsbox_slab *slab, const void *recv_dev, void *phys_dev, void *cuda_stream);
+
 /* ---- initial conditions on the device ---------------------------------- */
 /* state_init_rand, state.f90:211-285 (Yoffe 2012, s. 2.2.5): a random physical
  * field, R2C, state_dealias, state_project, state_spectrum (in the context's
