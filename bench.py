@@ -417,6 +417,48 @@ def ensemble_rate(steps=300, rank=0, world=1, dist_on=False):
             "graph": "one CUDA-graph replay per ensemble step and rank (batched size groups)"}
 
 
+def slab_fft_rate(n=1024, reps=5, rank=0, world=1, dist_on=False):
+    """The slab-decomposed transform (p3dfft's 1 x P grid of the reference's
+    distributed runs, variables.f90:131-157): an n^3 FP32 R2C + C2R pair of a
+    random field over the ranks, each rank its z-slab, the NCCL all-to-all
+    between the local halves under torchrun (strong scaling: the grid is
+    fixed; one rank exchanges by a copy).  Pairs per second on the slowest
+    rank's CUDA-event time, and the worst rank's round-trip error."""
+    from dnsbox_b200.slab import SlabFFT
+    s = SlabFFT(n, n, n, precision="fp32")
+    gen = torch.Generator(device="cuda").manual_seed(rank)
+    phys = torch.randn(s.phys_size, generator=gen, device="cuda")
+    spec = torch.empty(s.spec_size, dtype=s.cdtype, device="cuda")
+    back = torch.empty_like(phys)
+    s.r2c(phys, spec)
+    s.c2r(spec, back)
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        s.r2c(phys, spec)
+        s.c2r(spec, back)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    err = float((back / float(n) ** 3 - phys).norm() / phys.norm())
+    if dist_on:
+        ms = max_over_ranks(ms)
+        err = max_over_ranks(err)
+    s.close()
+    del phys, spec, back
+    torch.cuda.empty_cache()
+    if rank != 0:
+        return None
+    return {"value": 1e3 / ms, "unit": "R2C+C2R pairs/s", "grid": n, "precision": "fp32", "n_ranks": world,
+            "ms_per_pair": ms, "roundtrip_rel_l2": err, "scaling": "strong: the grid is split over the ranks",
+            "exchange": "NCCL all-to-all (torch.distributed)" if world > 1 else "device copy (one rank)"}
+
+
 def read_traffic(prec, n, pruned):
     """DRAM bytes per launch from a committed ncu summary, if one exists
     (columns: pass precision n pruned bytes)."""
@@ -473,6 +515,7 @@ def run_ours(args, rank, world, dist_on):
         torch.cuda.empty_cache()
     # the ensemble shards over the ranks (every rank takes part)
     ens_sharded = ensemble_rate(rank=rank, world=world, dist_on=dist_on) if world > 1 and not args.no_extra else None
+    slab_sharded = slab_fft_rate(rank=rank, world=world, dist_on=dist_on) if world > 1 and not args.no_extra else None
     if rank != 0:
         return
     main = args.precisions[0]
@@ -546,13 +589,14 @@ def run_ours(args, rank, world, dist_on):
                        for k, f in rr["pass_fields"].items() if prr["launches"][k]},
             "pruned": rr["pruned"]}
     if ens_sharded:
-        line["extra"] = {"ensemble_96": ens_sharded}
+        line["extra"] = {"ensemble_96": ens_sharded, "slab_fft_1024": slab_sharded}
     if world == 1 and not args.no_extra:
         line["extra"] = extra_sizes(args)
         line["extra"]["tc_split_1024"] = tc_1024_rate(args)
         line["extra"]["adjoint_descent_64"] = adjoint_rate()
         line["extra"]["periodic_orbit_grad_96"] = orbit_rate()
         line["extra"]["ensemble_96"] = ensemble_rate()
+        line["extra"]["slab_fft_1024"] = slab_fft_rate()
     if world == 1 and not args.no_cpu_baseline:
         from oracle import dnsbox_oracle as O
         rate, done, el = cpu_reference_rate(n, 3, budget_s=args.cpu_budget, warmup=0)
