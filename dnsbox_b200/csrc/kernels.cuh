@@ -132,10 +132,12 @@ __host__ __device__ __forceinline__ int strided_col(const StridedArgs<T> &a, int
 // Columns per CTA of the SIMT strided kernel: the host's tile width, or at
 // N >= 512 (plans of 64 threads per column) half a tile, so that a CTA has
 // 512 (FP32) or 256 (FP64) threads and several CTAs share an SM, each with
-// its own barriers; in FP32 also at N = 256 (128-thread CTAs, eight per SM:
-// 5% off the inverse y pass at 256^3; the FP64 kernel at 256 keeps its tile).
+// its own barriers; in FP32 at every size (at 256: 128-thread CTAs, eight per
+// SM, 5% off the inverse y pass at 256^3; at 96 the pruned 34-column grid
+// wastes 6 columns instead of 14, 3% off the 96^3 strided passes; the FP64
+// kernel below 512 keeps its tile).
 template <typename T, int N> struct StridedCols {
-  static constexpr int v = (N >= 512 || (sizeof(T) == 4 && N == 256)) ? TileCols<T>::v / 2 : TileCols<T>::v;
+  static constexpr int v = (N >= 512 || sizeof(T) == 4) ? TileCols<T>::v / 2 : TileCols<T>::v;
 };
 
 // Resident CTAs of a strided launch to ask the register allocator for: FP32
