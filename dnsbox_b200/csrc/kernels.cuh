@@ -374,8 +374,9 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
   }
   __syncthreads();
   // (omega x u) * s at every point; written back as (px_a,py_a) (pz_a,pz_b)
-  // (px_b,py_b) in columns 6j, 6j+1, 6j+2
-  double m0 = 0, m1 = 0, m2 = 0;
+  // (px_b,py_b) in columns 6j, 6j+1, 6j+2; the CFL maxima are taken in T
+  // (exact) and widened for the block reduction
+  T m0 = 0, m1 = 0, m2 = 0;
   for (int it = threadIdx.x; it < N * (B / 2); it += NT) {
     const int n = it % N, j = it / N;
     C *r = s + n * LD + 6 * j;
@@ -388,9 +389,9 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
       px[h] = (oy[h] * ww[h] - oz[h] * vv[h]) * sc;
       py[h] = (oz[h] * uu[h] - ox[h] * ww[h]) * sc;
       pz[h] = (ox[h] * vv[h] - oy[h] * uu[h]) * sc;
-      m0 = fmax(m0, fabs((double)uu[h]));
-      m1 = fmax(m1, fabs((double)vv[h]));
-      m2 = fmax(m2, fabs((double)ww[h]));
+      m0 = fmax(m0, fabs(uu[h]));
+      m1 = fmax(m1, fabs(vv[h]));
+      m2 = fmax(m2, fabs(ww[h]));
     }
     r[0] = mkc<C>(px[0], py[0]);
     r[1] = mkc<C>(pz[0], pz[1]);
@@ -447,9 +448,9 @@ __global__ void __launch_bounds__(round32(3 * XlineB<T, N>::v *(N / FftPlan<N>::
   m2 = warp_max(m2);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (lane == 0) {
-    red[wid] = m0;
-    red[32 + wid] = m1;
-    red[64 + wid] = m2;
+    red[wid] = (double)m0;
+    red[32 + wid] = (double)m1;
+    red[64 + wid] = (double)m2;
   }
   __syncthreads();
   if (wid == 0) {
