@@ -49,6 +49,11 @@ template <bool INV, typename C> __device__ __forceinline__ C mul_i(C a) {
   return INV ? mkc<C>(-a.y, a.x) : mkc<C>(a.y, -a.x);
 }
 
+// Integrating factor exp(x) in the state's precision (x formed in FP64).
+template <typename T> __device__ __forceinline__ T if_exp(double x);
+template <> __device__ __forceinline__ double if_exp<double>(double x) { return exp(x); }
+template <> __device__ __forceinline__ float if_exp<float>(double x) { return expf((float)x); }
+
 // Wavenumber of an index along a full axis of length n (variables.f90:242-262):
 // 0..n/2-1 -> itself, n/2 (Nyquist) -> 0, n/2+1..n-1 -> index - n.
 __host__ __device__ __forceinline__ double k_full(int idx, int n, double alpha) {

@@ -1082,26 +1082,29 @@ __global__ void __launch_bounds__(256, FinishMinB<T, MODE>::v)
       if (cut) {
         Nc[0] = Nc[1] = Nc[2] = mkc<C>(0, 0);
       } else {
-        // phat = -(i k . n) / (-(k.k))  (rhs.f90:101-106)
-        const double knre = kxr * (double)nn[h][0].x + kyr * (double)nn[h][1].x + kzr * (double)nn[h][2].x;
-        const double knim = kxr * (double)nn[h][0].y + kyr * (double)nn[h][1].y + kzr * (double)nn[h][2].y;
-        const double pre = -knim / k2, pim = knre / k2;
-        const double kr[3] = {kxr, kyr, kzr};
+        // phat = -(i k . n) / (-(k.k))  (rhs.f90:101-106), in T: the masks
+        // above and below are decided in FP64 (the same kept set in every
+        // precision), the pointwise arithmetic in the state's precision
+        const T kr[3] = {T(kxr), T(kyr), T(kzr)}, k2t = T(k2);
+        const T knre = kr[0] * nn[h][0].x + kr[1] * nn[h][1].x + kr[2] * nn[h][2].x;
+        const T knim = kr[0] * nn[h][0].y + kr[1] * nn[h][1].y + kr[2] * nn[h][2].y;
+        const T pre = -knim / k2t, pim = knre / k2t;
         const bool forced = a.bandlim && sqrt(k2) <= a.kcut;
+        const T fct = T(fc);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          double re = -(double)nn[h][c].x + kr[c] * pim;
-          double im = -(double)nn[h][c].y - kr[c] * pre;
+          T re = -nn[h][c].x + kr[c] * pim;
+          T im = -nn[h][c].y - kr[c] * pre;
           if (forced) {
-            re += fc * (double)uu[h][c].x;
-            im += fc * (double)uu[h][c].y;
+            re += fct * uu[h][c].x;
+            im += fct * uu[h][c].y;
           }
           if (a.force) {
             const C q = a.force[c * a.nh + idx];
-            re += (double)q.x;
-            im += (double)q.y;
+            re += q.x;
+            im += q.y;
           }
-          Nc[c] = mkc<C>(T(re), T(im));
+          Nc[c] = mkc<C>(re, im);
         }
       }
       if (MODE == FIN_RHS) {
@@ -1109,7 +1112,7 @@ __global__ void __launch_bounds__(256, FinishMinB<T, MODE>::v)
         for (int c = 0; c < 3; ++c) a.out[c * a.nh + idx] = Nc[c];
         continue;
       }
-      const T IF = T(exp((a.Q - nu * k2) * dt));
+      const T IF = if_exp<T>((a.Q - nu * k2) * dt);
       const T tdt = T(dt);
       if (MODE == FIN_PRED) {
 #pragma unroll
@@ -1131,7 +1134,7 @@ __global__ void __launch_bounds__(256, FinishMinB<T, MODE>::v)
         }
       } else {  // FIN_AB2
         const T e1c1 = T(c1) * IF;
-        const T e2c2 = T(c2 * exp((a.Q - nu * k2) * tau2));
+        const T e2c2 = T(c2) * if_exp<T>((a.Q - nu * k2) * tau2);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const C u = uu[h][c], o = no[h][c];
