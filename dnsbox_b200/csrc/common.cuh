@@ -49,10 +49,11 @@ template <bool INV, typename C> __device__ __forceinline__ C mul_i(C a) {
   return INV ? mkc<C>(-a.y, a.x) : mkc<C>(a.y, -a.x);
 }
 
-// Integrating factor exp(x) in the state's precision (x formed in FP64).
-template <typename T> __device__ __forceinline__ T if_exp(double x);
-template <> __device__ __forceinline__ double if_exp<double>(double x) { return exp(x); }
-template <> __device__ __forceinline__ float if_exp<float>(double x) { return expf((float)x); }
+// Integrating factor exp(x), evaluated in FP64 and rounded once to the
+// state's precision: it multiplies the whole state every step, so its error
+// goes straight into the velocity (single-precision expf, up to 2 ulp, moved
+// the 512^3 FP32 run's velocity error against FP64 from 0.7e-6 to 1.6e-6).
+template <typename T> __device__ __forceinline__ T if_exp(double x) { return T(exp(x)); }
 
 // Wavenumber of an index along a full axis of length n (variables.f90:242-262):
 // 0..n/2-1 -> itself, n/2 (Nyquist) -> 0, n/2+1..n-1 -> index - n.
