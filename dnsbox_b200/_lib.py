@@ -144,6 +144,10 @@ SIGNATURES = {
     "dnsbox_slab_ftran_finish": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "dnsbox_slab_btran_local": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "dnsbox_slab_btran_finish": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "dnsbox_slab_rhs_setup": (ctypes.c_int, [_VP, _VP]),
+    "dnsbox_slab_rhs_begin": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "dnsbox_slab_rhs_middle": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "dnsbox_slab_rhs_finish": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
 }
 
 _lib = None

@@ -1001,6 +1001,9 @@ template <typename T> struct FinishArgs {
   // between components and between boxes; 0: the state's (nxh, nh, bstride)
   int n3_pitch;
   long long n3_nh, n3_bstride;
+  // a ky slab of a box split over ranks: row ky of this launch is ky0 + ky of
+  // an axis of ny_k rows (0, 0: the box's own rows)
+  int ky0, ny_k;
 };
 
 // Spectral finish after the forward z transform (the second half of one
@@ -1053,7 +1056,7 @@ __global__ void __launch_bounds__(256, FinishMinB<T, MODE>::v)
     }
     tau2 = dt + tn - tm;
   }
-  const double kyr = k_full(ky, a.ny, a.ay);
+  const double kyr = k_full(a.ky0 + ky, a.ny_k ? a.ny_k : a.ny, a.ay);
   const double kzr = k_full(kz, a.nz, a.az);
   const bool need_u = a.bandlim || MODE != FIN_RHS;
   double esum = 0.0, dsum = 0.0;

@@ -34,6 +34,23 @@
 //   spectral slab  (nz, ny/P, nx/2+1), ky rows [rank ny/P, (rank+1) ny/P)
 //   send / recv    P blocks of nz/P * ny/P * (nx/2+1), block q for rank q
 // Transforms are unnormalised, as p3dfft's and dnsbox_r2c / dnsbox_c2r.
+//
+// rhs_nonlinear over the slabs (rhs.f90:18-135, rhs_Eband :137-168), the
+// single-box right-hand side's passes with the exchanges between them:
+//   rhs_begin:  band-energy partial of the local ky rows; pass A (inverse z
+//               of u, v, w, -dz v, dz u) into five send buffers, whose block
+//               q is planes [q nz/P, (q+1) nz/P) as the z FFT writes them;
+//   (five all-to-alls; the band energy summed over the ranks)
+//   rhs_middle: the received ky rows unpacked into whole planes; pass B
+//               (inverse y, the curl assembled by two-term jobs), pass C (the
+//               fused x pass: C2R, (omega x u) / N^3, CFL maxima, R2C) and
+//               pass D (forward y) on the local planes; N packed by
+//               destination into three send buffers;
+//   (three all-to-alls; the CFL maxima reduced by max)
+//   rhs_finish: pass E1 (forward z) of the received ky-slab and the finish's
+//               right-hand-side mode (2/3 mask, projection, band forcing with
+//               the global band energy) with the rank's ky offset.
+// Unpruned passes throughout.
 #include <vector>
 
 #include "internal.cuh"
@@ -45,6 +62,13 @@ struct dnsbox_slab {
   void *A = nullptr, *B = nullptr;   // scratch, nzl * ny * nxh complex each
   void *tw[3] = {nullptr, nullptr, nullptr};   // exp(-2 pi i j / n), n = nx, ny, nz
   size_t cbytes;
+  // right-hand side (dnsbox_slab_rhs_setup)
+  bool rhs = false;
+  dnsbox_params p;
+  void *W = nullptr, *V = nullptr;   // 6 fields of nzl * ny * nxh each
+  int *band = nullptr;               // band modes of the local ky rows (offset lo, hi, kx)
+  int nband = 0;
+  dnsbox::StepState *st = nullptr;   // band energy, CFL maxima
 };
 
 namespace {
@@ -71,6 +95,10 @@ void slab_free(dnsbox_slab *s) {
   if (!s) return;
   cudaFree(s->A);
   cudaFree(s->B);
+  cudaFree(s->W);
+  cudaFree(s->V);
+  cudaFree(s->band);
+  cudaFree(s->st);
   for (void *t : s->tw) cudaFree(t);
   delete s;
 }
@@ -258,4 +286,248 @@ extern "C" int dnsbox_slab_btran_finish(dnsbox_slab *s, const void *recv, void *
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   return s->precision == DNSBOX_FP64 ? btran_finish<double>(s, recv, phys, st)
                                      : btran_finish<float>(s, recv, phys, st);
+}
+
+// ------------------------------------------------------------ right-hand side
+namespace {
+
+size_t slab_field(const dnsbox_slab *s) { return (size_t)s->nzl * s->ny * s->nxh; }
+
+template <typename T> const char *fld(const void *base, const dnsbox_slab *s, int f) {
+  return reinterpret_cast<const char *>(base) + (size_t)f * slab_field(s) * s->cbytes;
+}
+template <typename T> char *fld(void *base, const dnsbox_slab *s, int f) {
+  return reinterpret_cast<char *>(base) + (size_t)f * slab_field(s) * s->cbytes;
+}
+
+// strided arguments of a pass on the ky-slab (z rows) or on the planes (y rows)
+template <typename T> StridedArgs<T> slab_pass(const dnsbox_slab *s, bool zslab_rows) {
+  StridedArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  a.ncols = s->nxh;
+  a.nx = s->nx;
+  a.alpha_x = s->p.alpha_x;
+  if (zslab_rows) {   // (nz, nyl, nxh): rows kz, one tile row per local ky
+    a.tw = reinterpret_cast<const typename CT<T>::type *>(s->tw[2]);
+    a.rowstride = (long long)s->nyl * s->nxh;
+    a.otherstride = s->nxh;
+    a.alpha_row = s->p.alpha_z;
+  } else {            // (nzl, ny, nxh): rows ky, one tile row per local plane
+    a.tw = reinterpret_cast<const typename CT<T>::type *>(s->tw[1]);
+    a.rowstride = s->nxh;
+    a.otherstride = (long long)s->ny * s->nxh;
+    a.alpha_row = s->p.alpha_y;
+  }
+  return a;
+}
+
+template <typename T> int slab_run(const dnsbox_slab *s, int n, bool inv, const StridedArgs<T> &a, int nother,
+                                   cudaStream_t st) {
+  const int ntx = (s->nxh + TileCols<T>::v - 1) / TileCols<T>::v;
+  cudaError_t e = Ops<T>::strided(n, a, inv, ntx * nother, st);
+  if (e != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "slab right-hand side pass: %s", cudaGetErrorString(e));
+  return DNSBOX_OK;
+}
+
+template <typename T>
+int rhs_begin(dnsbox_slab *s, const void *uh, double *eband, void *send5, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  const double sc = 1.0 / ((double)s->nx * s->ny * s->nz);
+  const size_t F = slab_field(s);   // = nz * nyl * nxh, the ky-slab's field
+  k_eband<C><<<1, 256, 0, st>>>(reinterpret_cast<const C *>(uh), (long long)F, s->band, s->nband, s->nx, s->st,
+                                sc * sc, 1, 0);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(eband, &s->st->eband, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  // pass A: state -> send buffers (rhs.f90:39-65: the spectral curl as multipliers)
+  StridedArgs<T> a = slab_pass<T>(s, true);
+  a.njobs = 5;
+  const char *u = reinterpret_cast<const char *>(uh);
+  auto comp = [&](int c) { return u + (size_t)c * F * s->cbytes; };
+  set_job<T>(a, 0, comp(0), fld<T>(send5, s, 0));
+  set_job<T>(a, 1, comp(1), fld<T>(send5, s, 1));
+  set_job<T>(a, 2, comp(2), fld<T>(send5, s, 2));
+  set_job<T>(a, 3, comp(1), fld<T>(send5, s, 3), 0.0, -sc, 1);   // -dz v
+  set_job<T>(a, 4, comp(0), fld<T>(send5, s, 4), 0.0, sc, 1);    //  dz u
+  return slab_run<T>(s, s->nz, true, a, s->nyl, st);
+}
+
+template <typename T>
+int rhs_middle(dnsbox_slab *s, const void *recv5, double *umax, void *send3, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  const double sc = 1.0 / ((double)s->nx * s->ny * s->nz);
+  for (int f = 0; f < 5; ++f) {
+    if (s->nranks > 1) RET(slab_blocks(s, false, fld<T>(recv5, s, f), fld<T>(s->W, s, f), st));
+    else CK(cudaMemcpyAsync(fld<T>(s->W, s, f), fld<T>(recv5, s, f), slab_field(s) * s->cbytes,
+                            cudaMemcpyDeviceToDevice, st));
+  }
+  // pass B: inverse y; omega_x = dy w - dz v, omega_y = dz u - dx w, omega_z = dx v - dy u
+  StridedArgs<T> b = slab_pass<T>(s, false);
+  b.njobs = 6;
+  set_job<T>(b, 0, fld<T>(s->W, s, 0), fld<T>(s->V, s, 0));
+  set_job<T>(b, 1, fld<T>(s->W, s, 1), fld<T>(s->V, s, 1));
+  set_job<T>(b, 2, fld<T>(s->W, s, 2), fld<T>(s->V, s, 2));
+  set_job<T>(b, 3, fld<T>(s->W, s, 2), fld<T>(s->V, s, 3), 0.0, sc, 1, fld<T>(s->W, s, 3));
+  set_job<T>(b, 4, fld<T>(s->W, s, 4), fld<T>(s->V, s, 4), 1.0, 0.0, 0, fld<T>(s->W, s, 2), 0.0, -sc, 0);
+  set_job<T>(b, 5, fld<T>(s->W, s, 0), fld<T>(s->V, s, 5), 0.0, -sc, 1, fld<T>(s->W, s, 1), 0.0, sc, 0);
+  RET(slab_run<T>(s, s->ny, true, b, s->nzl, st));
+  // pass C: the fused x pass on the local planes
+  XlineNLArgs<T> x;
+  memset(&x, 0, sizeof(x));
+  x.U = reinterpret_cast<const C *>(fld<T>(s->V, s, 0));
+  x.V = reinterpret_cast<const C *>(fld<T>(s->V, s, 1));
+  x.W = reinterpret_cast<const C *>(fld<T>(s->V, s, 2));
+  x.OX = reinterpret_cast<const C *>(fld<T>(s->V, s, 3));
+  x.OY = reinterpret_cast<const C *>(fld<T>(s->V, s, 4));
+  x.OZ = reinterpret_cast<const C *>(fld<T>(s->V, s, 5));
+  x.NX = reinterpret_cast<C *>(fld<T>(s->W, s, 0));
+  x.NY = reinterpret_cast<C *>(fld<T>(s->W, s, 1));
+  x.NZ = reinterpret_cast<C *>(fld<T>(s->W, s, 2));
+  x.tw = reinterpret_cast<const C *>(s->tw[0]);
+  x.st = s->st;
+  x.lines_per_box = s->ny * s->nzl;
+  x.nlines = s->ny * s->nzl;
+  x.nxh = s->nxh;
+  x.alpha_x = s->p.alpha_x;
+  x.s = sc;
+  cudaError_t e = Ops<T>::xline_nl(s->nx, x, 0, st);
+  if (e != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "slab x pass: %s", cudaGetErrorString(e));
+  CK(cudaMemcpyAsync(umax, s->st->umax, 3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  // pass D: forward y, then N packed by destination rank
+  StridedArgs<T> d = slab_pass<T>(s, false);
+  d.njobs = 3;
+  for (int f = 0; f < 3; ++f) set_job<T>(d, f, fld<T>(s->W, s, f), fld<T>(s->V, s, f));
+  RET(slab_run<T>(s, s->ny, false, d, s->nzl, st));
+  for (int f = 0; f < 3; ++f) {
+    if (s->nranks > 1) RET(slab_blocks(s, true, fld<T>(s->V, s, f), fld<T>(send3, s, f), st));
+    else CK(cudaMemcpyAsync(fld<T>(send3, s, f), fld<T>(s->V, s, f), slab_field(s) * s->cbytes,
+                            cudaMemcpyDeviceToDevice, st));
+  }
+  return DNSBOX_OK;
+}
+
+template <typename T>
+int rhs_finish(dnsbox_slab *s, const void *recv3, const void *uh, const double *eband, void *out, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  const dnsbox_params &p = s->p;
+  // pass E1: forward z of the received ky-slab
+  StridedArgs<T> z = slab_pass<T>(s, true);
+  z.njobs = 3;
+  for (int f = 0; f < 3; ++f) set_job<T>(z, f, fld<T>(recv3, s, f), fld<T>(s->W, s, f));
+  RET(slab_run<T>(s, s->nz, false, z, s->nyl, st));
+  CK(cudaMemcpyAsync(&s->st->eband, eband, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  // pass E2 in right-hand-side mode (rhs.f90:67-133), rows of the rank's ky slab
+  FinishArgs<T> f;
+  memset(&f, 0, sizeof(f));
+  f.n3 = reinterpret_cast<const C *>(s->W);
+  f.uin = reinterpret_cast<const C *>(uh);
+  f.out = reinterpret_cast<C *>(out);
+  f.st = s->st;
+  f.tw = reinterpret_cast<const C *>(s->tw[2]);
+  f.nh = (long long)slab_field(s);
+  f.nx = s->nx;
+  f.ny = s->nyl;
+  f.nz = s->nz;
+  f.nxh = s->nxh;
+  f.ky0 = s->rank * s->nyl;
+  f.ny_k = s->ny;
+  f.ax = p.alpha_x;
+  f.ay = p.alpha_y;
+  f.az = p.alpha_z;
+  f.nu = p.nu;
+  f.Q = p.Q;
+  f.Pin = p.Pin;
+  f.kcut = p.kCutOff;
+  f.cutx = (s->nx / 2.0) * (2.0 * p.alpha_x / 3.0);   // rhs.f90:74-88
+  f.cuty = (s->ny / 2.0) * (2.0 * p.alpha_y / 3.0);
+  f.cutz = (s->nz / 2.0) * (2.0 * p.alpha_z / 3.0);
+  f.sph2 = pow((s->nx / 2.0) * 0.5 * p.alpha_x, 2);
+  f.bandlim = p.bandlim;
+  f.spherical = p.spherical;
+  f.s = 1.0 / ((double)s->nx * s->ny * s->nz);
+  f.mode = FIN_RHS;
+  f.kx = AxisKeep{0, s->nx, 0};
+  f.ky = AxisKeep{0, s->nyl, 1};
+  f.kz = AxisKeep{0, s->nz, 1};
+  const int nrows = s->nz * s->nyl;
+  k_finish_rows<T, FIN_RHS><<<dim3((unsigned)((nrows + 7) / 8), 1), 256, 0, st>>>(f, nrows);
+  CK(cudaGetLastError());
+  return DNSBOX_OK;
+}
+
+int rhs_begin_check(const dnsbox_slab *s, const void *a, const void *b, const void *c) {
+  if (!s) return set_err(DNSBOX_ERR_ARG, "null slab");
+  if (!s->rhs) return set_err(DNSBOX_ERR_STATE, "dnsbox_slab_rhs_setup has not been called");
+  if (!a || !b || !c) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  CK(cudaSetDevice(s->device));
+  return DNSBOX_OK;
+}
+
+}  // namespace
+
+extern "C" int dnsbox_slab_rhs_setup(dnsbox_slab *s, const dnsbox_params *p) {
+  if (!s || !p) return set_err(DNSBOX_ERR_ARG, "null argument");
+  if (p->nx != s->nx || p->ny != s->ny || p->nz != s->nz)
+    return set_err(DNSBOX_ERR_ARG, "grid %dx%dx%d is not the slab's %dx%dx%d", p->nx, p->ny, p->nz, s->nx, s->ny,
+                   s->nz);
+  if (!(p->nu >= 0.0) || !(p->alpha_x > 0) || !(p->alpha_y > 0) || !(p->alpha_z > 0))
+    return set_err(DNSBOX_ERR_ARG, "invalid physical parameter");
+  CK(cudaSetDevice(s->device));
+  s->p = *p;
+  if (!s->rhs) {
+    const size_t bytes = 6 * slab_field(s) * s->cbytes;
+    CK(cudaMalloc(&s->W, bytes));
+    CK(cudaMalloc(&s->V, bytes));
+    CK(cudaMalloc(&s->st, sizeof(dnsbox::StepState)));
+    CK(cudaMemset(s->st, 0, sizeof(dnsbox::StepState)));
+  }
+  // band modes |k| <= kCutOff among the local ky rows (as dnsbox_create builds them)
+  cudaFree(s->band);
+  s->band = nullptr;
+  s->nband = 0;
+  std::vector<int> band;
+  if (p->bandlim) {
+    const int ky0 = s->rank * s->nyl;
+    for (int kz = 0; kz < s->nz; ++kz)
+      for (int yl = 0; yl < s->nyl; ++yl)
+        for (int kx = 0; kx < s->nxh; ++kx) {
+          const double a = k_half(kx, s->nx, p->alpha_x), b = k_full(ky0 + yl, s->ny, p->alpha_y),
+                       c = k_full(kz, s->nz, p->alpha_z);
+          if (sqrt(a * a + b * b + c * c) > p->kCutOff) continue;
+          const long long off = ((long long)kz * s->nyl + yl) * s->nxh + kx;
+          band.push_back((int)(off & 0xffffffffLL));
+          band.push_back((int)(off >> 32));
+          band.push_back(kx);
+        }
+  }
+  s->nband = (int)band.size() / 3;
+  if (s->nband) {
+    CK(cudaMalloc(&s->band, band.size() * sizeof(int)));
+    CK(cudaMemcpy(s->band, band.data(), band.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  s->rhs = true;
+  return DNSBOX_OK;
+}
+
+extern "C" int dnsbox_slab_rhs_begin(dnsbox_slab *s, const void *uh, double *eband_dev, void *send5, void *stream) {
+  RET(rhs_begin_check(s, uh, eband_dev, send5));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  return s->precision == DNSBOX_FP64 ? rhs_begin<double>(s, uh, eband_dev, send5, st)
+                                     : rhs_begin<float>(s, uh, eband_dev, send5, st);
+}
+
+extern "C" int dnsbox_slab_rhs_middle(dnsbox_slab *s, const void *recv5, double *umax_dev, void *send3,
+                                      void *stream) {
+  RET(rhs_begin_check(s, recv5, umax_dev, send3));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  return s->precision == DNSBOX_FP64 ? rhs_middle<double>(s, recv5, umax_dev, send3, st)
+                                     : rhs_middle<float>(s, recv5, umax_dev, send3, st);
+}
+
+extern "C" int dnsbox_slab_rhs_finish(dnsbox_slab *s, const void *recv3, const void *uh, const double *eband_dev,
+                                      void *out, void *stream) {
+  RET(rhs_begin_check(s, recv3, eband_dev, out));
+  if (!uh) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  return s->precision == DNSBOX_FP64 ? rhs_finish<double>(s, recv3, uh, eband_dev, out, st)
+                                     : rhs_finish<float>(s, recv3, uh, eband_dev, out, st);
 }

@@ -14,6 +14,12 @@ Layouts (row-major, innermost last):
 * spectral slab ``(nz, ny/P, nx/2+1)`` complex, ky rows ``[rank ny/P, ...)``.
 
 Transforms are unnormalised, as ``Box.r2c`` / ``Box.c2r`` and p3dfft's.
+
+``SlabFFT.rhs_nonlinear`` is the reference's ``rhs_nonlinear`` (rhs.f90:18-135)
+on a spectral ky-slab state ``(3, nz, ny/P, nx/2+1)``: the single-box passes
+with eight all-to-alls (five fields out of the inverse z pass, three into the
+forward z pass), the band energy summed and the CFL maxima reduced over the
+ranks.
 """
 from __future__ import annotations
 
@@ -36,6 +42,15 @@ def slab_extents(nx: int, ny: int, nz: int, nranks: int, rank: int) -> dict:
     return {"phys_start": (rank * nzl, 0, 0), "phys_size": (nzl, ny, nx),
             "spec_start": (0, rank * nyl, 0), "spec_size": (nz, nyl, nxh),
             "block_elems": nzl * nyl * nxh}
+
+
+def all_reduce(t: torch.Tensor, op: str, group=None) -> None:
+    """Sum ("sum") or maximum ("max") of ``t`` over the ranks, in place
+    (nothing without a process group)."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return
+    dist.all_reduce(t, op=dist.ReduceOp.SUM if op == "sum" else dist.ReduceOp.MAX, group=group)
 
 
 def all_to_all(send: torch.Tensor, recv: torch.Tensor, group=None) -> None:
@@ -130,6 +145,68 @@ class SlabFFT:
         self._exchange(self.send, self.recv)
         self.backward_finish(phys)
         return phys
+
+    # -- rhs_nonlinear over the slabs --
+    def setup_rhs(self, nu: float = 0.0, Q: float = 0.0, kCutOff: float = 2.5, Pin: float = 0.0,
+                  bandlim: bool = False, spherical: bool = False, alpha=(1.0, 1.0, 1.0), reduce=None):
+        """Physics of the right-hand side (as ``Box``); ``reduce(t, op)``
+        (default :func:`all_reduce` over the group) sums the band energy and
+        takes the maximum of the CFL maxima over the ranks."""
+        p = _lib.Params()
+        self._lib.dnsbox_default_params(ctypes.byref(p))
+        p.nx, p.ny, p.nz = self.nx, self.ny, self.nz
+        p.precision = PRECISION[self.precision]
+        p.device = self.device.index
+        p.bandlim, p.spherical = int(bandlim), int(spherical)
+        p.alpha_x, p.alpha_y, p.alpha_z = alpha
+        p.nu, p.Q, p.kCutOff, p.Pin = nu, Q, kCutOff, Pin
+        _lib.check(self._lib.dnsbox_slab_rhs_setup(self._h, ctypes.byref(p)))
+        shape = (self.nranks, self.block_elems)
+        self.send5 = torch.empty((5,) + shape, dtype=self.cdtype, device=self.device)
+        self.recv5 = torch.empty_like(self.send5)
+        self.send3 = torch.empty((3,) + shape, dtype=self.cdtype, device=self.device)
+        self.recv3 = torch.empty_like(self.send3)
+        self.eband = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self.umax = torch.zeros(3, dtype=torch.float64, device=self.device)
+        self._reduce = reduce if reduce is not None else (lambda t, op: all_reduce(t, op, self._group))
+
+    def state_shape(self):
+        """The spectral ky-slab state: (3, nz, ny/P, nx/2+1)."""
+        return (3,) + self.spec_size
+
+    def rhs_begin(self, uh: torch.Tensor) -> None:
+        self._check(uh, self.state_shape(), self.cdtype, "state slab")
+        _lib.check(self._lib.dnsbox_slab_rhs_begin(self._h, ctypes.c_void_p(uh.data_ptr()),
+                                                   ctypes.c_void_p(self.eband.data_ptr()),
+                                                   ctypes.c_void_p(self.send5.data_ptr()), self._stream()))
+
+    def rhs_middle(self) -> None:
+        _lib.check(self._lib.dnsbox_slab_rhs_middle(self._h, ctypes.c_void_p(self.recv5.data_ptr()),
+                                                    ctypes.c_void_p(self.umax.data_ptr()),
+                                                    ctypes.c_void_p(self.send3.data_ptr()), self._stream()))
+
+    def rhs_finish(self, uh: torch.Tensor, out: torch.Tensor) -> None:
+        self._check(out, self.state_shape(), self.cdtype, "output slab")
+        _lib.check(self._lib.dnsbox_slab_rhs_finish(self._h, ctypes.c_void_p(self.recv3.data_ptr()),
+                                                    ctypes.c_void_p(uh.data_ptr()),
+                                                    ctypes.c_void_p(self.eband.data_ptr()),
+                                                    ctypes.c_void_p(out.data_ptr()), self._stream()))
+
+    def rhs_nonlinear(self, uh: torch.Tensor, out: torch.Tensor | None = None):
+        """N(u) of this rank's ky slab; returns (N, band energy, (max|u|, max|v|,
+        max|w|)), the last two over the whole box."""
+        if out is None:
+            out = torch.empty(self.state_shape(), dtype=self.cdtype, device=self.device)
+        self.rhs_begin(uh)
+        for f in range(5):
+            self._exchange(self.send5[f], self.recv5[f])
+        self._reduce(self.eband, "sum")
+        self.rhs_middle()
+        for f in range(3):
+            self._exchange(self.send3[f], self.recv3[f])
+        self._reduce(self.umax, "max")
+        self.rhs_finish(uh, out)
+        return out, float(self.eband.item()), tuple(float(v) for v in self.umax.tolist())
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

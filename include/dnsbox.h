@@ -220,6 +220,30 @@ int dnsbox_slab_btran_local(dnsbox_slab *slab, const void *spec_dev, void *send_
 /* inverse: unpack the received ky rows, y FFT and x C2R into the physical slab */
 int dnsbox_slab_btran_finish(dnsbox_slab *slab, const void *recv_dev, void *phys_dev, void *cuda_stream);
 
+/* rhs_nonlinear over the slabs (rhs.f90:18-135 with rhs_Eband :137-168): the
+ * single-box right-hand side's passes (unpruned) with the exchanges between
+ * them, which the caller runs.  uh / out: the spectral ky-slab state and
+ * nonlinear term, 3 components of nz * ny/P * (nx/2+1) each.
+ *   rhs_begin   band-energy partial (one device double; the caller sums it
+ *               over the ranks) and the inverse z pass into send5 (5 fields,
+ *               each P blocks as for dnsbox_slab_btran_local);
+ *   (one all-to-all per field: 5)
+ *   rhs_middle  inverse y, the fused x pass (CFL maxima max|u_i| of the local
+ *               planes into umax_dev, 3 device doubles; the caller reduces them
+ *               by max) and forward y, packed into send3 (3 fields);
+ *   (one all-to-all per field: 3)
+ *   rhs_finish  forward z and the finish (2/3 mask, projection, band forcing
+ *               with the summed band energy eband_dev) into out.
+ * dnsbox_slab_rhs_setup takes the physics from params (nx, ny, nz must be
+ * the slab's; precision, stepper and the step-control fields are ignored). */
+int dnsbox_slab_rhs_setup(dnsbox_slab *slab, const dnsbox_params *params);
+int dnsbox_slab_rhs_begin(dnsbox_slab *slab, const void *uh_dev, double *eband_dev, void *send5_dev,
+                          void *cuda_stream);
+int dnsbox_slab_rhs_middle(dnsbox_slab *slab, const void *recv5_dev, double *umax_dev, void *send3_dev,
+                           void *cuda_stream);
+int dnsbox_slab_rhs_finish(dnsbox_slab *slab, const void *recv3_dev, const void *uh_dev, const double *eband_dev,
+                           void *out_dev, void *cuda_stream);
+
 /* ---- initial conditions on the device ---------------------------------- */
 /* state_init_rand, state.f90:211-285 (Yoffe 2012, s. 2.2.5): a random physical
  * field, R2C, state_dealias, state_project, state_spectrum (in the context's

@@ -105,3 +105,92 @@ def test_slab_through_nccl_one_rank():
         s.close()
     finally:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- rhs_nonlinear over the slabs
+def _emulate_rhs(slabs, states, outs):
+    """The three halves on every rank with the exchanges and reductions done
+    by copies: five and three per-field all-to-alls, the band energy summed and
+    the CFL maxima reduced over the ranks."""
+    p = len(slabs)
+    for s in slabs:
+        s.rhs_begin(states[s.rank])
+    for f in range(5):
+        for q in range(p):
+            for r in range(p):
+                slabs[q].recv5[f][r].copy_(slabs[r].send5[f][q])
+    eb = sum(s.eband.clone() for s in slabs)
+    for s in slabs:
+        s.eband.copy_(eb)
+        s.rhs_middle()
+    for f in range(3):
+        for q in range(p):
+            for r in range(p):
+                slabs[q].recv3[f][r].copy_(slabs[r].send3[f][q])
+    um = torch.stack([s.umax.clone() for s in slabs]).max(dim=0).values
+    for s in slabs:
+        s.umax.copy_(um)
+        s.rhs_finish(states[s.rank], outs[s.rank])
+    return float(eb.item()), um.cpu().numpy()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 2e-6)])
+@pytest.mark.parametrize("shape,p,bandlim", [((32, 32, 32), 2, True), ((32, 48, 64), 4, True),
+                                             ((24, 48, 48), 3, False), ((64, 32, 16), 8, True)])
+def test_slab_rhs_matches_the_box_and_the_oracle(prec, tol, shape, p, bandlim):
+    from dnsbox_b200.ops import Box
+    from dnsbox_b200.slab import SlabFFT
+    nx, ny, nz = shape
+    kw = dict(nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=bandlim)
+    g = O.Grid(O.Params(nx=nx, ny=ny, nz=nz, **kw))
+    rng = np.random.default_rng(5)
+    uh = O.state_dealias(g, O.state_project(g, O.state_u2uhat(g, rng.standard_normal((3, nz, ny, nx)))))
+    want = O.rhs_nonlinear(g, uh)
+    box = Box(nx=nx, ny=ny, nz=nz, precision=prec, **kw)
+    ub = box.from_numpy(uh)
+    nb, eb_box = box.rhs_nonlinear(ub)
+    umax_box = [float(np.abs(box.c2r(ub[c]).cpu().numpy()).max()) for c in range(3)]
+    slabs = [SlabFFT(nx, ny, nz, precision=prec, rank=r, nranks=p) for r in range(p)]
+    for s in slabs:
+        s.setup_rhs(**kw)
+    nyl = ny // p
+    states = [ub[:, :, r * nyl:(r + 1) * nyl, :].contiguous() for r in range(p)]
+    outs = [torch.full(s.state_shape(), complex("nan"), dtype=s.cdtype, device="cuda") for s in slabs]
+    eb, um = _emulate_rhs(slabs, states, outs)
+    got = torch.cat(outs, dim=2).cpu().numpy()
+    assert rel(got, want) < tol
+    assert rel(got, nb.cpu().numpy()) < tol
+    if bandlim:
+        assert abs(eb - eb_box) <= (1e-12 if prec == "fp64" else 1e-6) * abs(eb_box)
+    # CFL maxima: max |u_i| of the physical velocity, which the unnormalised C2R
+    # of the state gives N^3 times
+    s3 = 1.0 / (nx * ny * nz)
+    assert np.allclose(um, np.array(umax_box) * s3, rtol=1e-12 if prec == "fp64" else 2e-6)
+    for s in slabs:
+        s.close()
+    box.close()
+
+
+def test_slab_rhs_through_nccl_one_rank():
+    import torch.distributed as dist
+    from dnsbox_b200.ops import Box
+    from dnsbox_b200.slab import SlabFFT
+    n = 32
+    kw = dict(nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True)
+    g = O.Grid(O.Params(nx=n, ny=n, nz=n, **kw))
+    uh = O.state_dealias(g, O.state_project(g, O.state_u2uhat(g, np.random.default_rng(8).standard_normal((3, n, n, n)))))
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        s = SlabFFT(n, n, n, precision="fp64")
+        s.setup_rhs(**kw)
+        out, eb, um = s.rhs_nonlinear(torch.from_numpy(uh).cuda())
+        assert rel(out.cpu().numpy(), O.rhs_nonlinear(g, uh)) < 1e-12
+        box = Box(n, **kw)
+        _, eb_box = box.rhs_nonlinear(box.from_numpy(uh))
+        assert abs(eb - eb_box) <= 1e-12 * abs(eb_box)
+        torch.cuda.synchronize()
+        s.close()
+        box.close()
+    finally:
+        dist.destroy_process_group()
