@@ -473,10 +473,12 @@ extern "C" int dnsbox_slab_rhs_setup(dnsbox_slab *s, const dnsbox_params *p) {
     return set_err(DNSBOX_ERR_ARG, "invalid physical parameter");
   CK(cudaSetDevice(s->device));
   s->p = *p;
-  if (!s->rhs) {
-    const size_t bytes = 6 * slab_field(s) * s->cbytes;
-    CK(cudaMalloc(&s->W, bytes));
-    CK(cudaMalloc(&s->V, bytes));
+  // buffers once (a repeated set-up, or one after a failed allocation, keeps
+  // what is there and allocates the rest)
+  const size_t bytes = 6 * slab_field(s) * s->cbytes;
+  if (!s->W) CK(cudaMalloc(&s->W, bytes));
+  if (!s->V) CK(cudaMalloc(&s->V, bytes));
+  if (!s->st) {
     CK(cudaMalloc(&s->st, sizeof(dnsbox::StepState)));
     CK(cudaMemset(s->st, 0, sizeof(dnsbox::StepState)));
   }
