@@ -68,7 +68,7 @@ struct dnsbox_slab {
   void *W = nullptr, *V = nullptr;   // 6 fields of nzl * ny * nxh each
   int *band = nullptr;               // band modes of the local ky rows (offset lo, hi, kx)
   int nband = 0;
-  dnsbox::StepState *st = nullptr;   // band energy, CFL maxima
+  dnsbox::StepState *st = nullptr;   // band energy, CFL maxima, dt of the Heun finishes
 };
 
 namespace {
@@ -406,7 +406,8 @@ int rhs_middle(dnsbox_slab *s, const void *recv5, double *umax, void *send3, cud
 }
 
 template <typename T>
-int rhs_finish(dnsbox_slab *s, const void *recv3, const void *uh, const double *eband, void *out, cudaStream_t st) {
+int rhs_finish(dnsbox_slab *s, const void *recv3, const void *uh, const double *eband, void *out, cudaStream_t st,
+               int mode = FIN_RHS, void *state = nullptr) {
   using C = typename CT<T>::type;
   const dnsbox_params &p = s->p;
   // pass E1: forward z of the received ky-slab
@@ -421,6 +422,7 @@ int rhs_finish(dnsbox_slab *s, const void *recv3, const void *uh, const double *
   f.n3 = reinterpret_cast<const C *>(s->W);
   f.uin = reinterpret_cast<const C *>(uh);
   f.out = reinterpret_cast<C *>(out);
+  f.state = reinterpret_cast<C *>(state);
   f.st = s->st;
   f.tw = reinterpret_cast<const C *>(s->tw[2]);
   f.nh = (long long)slab_field(s);
@@ -444,12 +446,17 @@ int rhs_finish(dnsbox_slab *s, const void *recv3, const void *uh, const double *
   f.bandlim = p.bandlim;
   f.spherical = p.spherical;
   f.s = 1.0 / ((double)s->nx * s->ny * s->nz);
-  f.mode = FIN_RHS;
+  f.mode = mode;
   f.kx = AxisKeep{0, s->nx, 0};
   f.ky = AxisKeep{0, s->nyl, 1};
   f.kz = AxisKeep{0, s->nz, 1};
   const int nrows = s->nz * s->nyl;
-  k_finish_rows<T, FIN_RHS><<<dim3((unsigned)((nrows + 7) / 8), 1), 256, 0, st>>>(f, nrows);
+  const dim3 grid((unsigned)((nrows + 7) / 8), 1);
+  switch (mode) {
+    case FIN_RHS: k_finish_rows<T, FIN_RHS><<<grid, 256, 0, st>>>(f, nrows); break;
+    case FIN_PRED: k_finish_rows<T, FIN_PRED><<<grid, 256, 0, st>>>(f, nrows); break;
+    default: k_finish_rows<T, FIN_CORR><<<grid, 256, 0, st>>>(f, nrows); break;
+  }
   CK(cudaGetLastError());
   return DNSBOX_OK;
 }
@@ -532,4 +539,26 @@ extern "C" int dnsbox_slab_rhs_finish(dnsbox_slab *s, const void *recv3, const v
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   return s->precision == DNSBOX_FP64 ? rhs_finish<double>(s, recv3, uh, eband_dev, out, st)
                                      : rhs_finish<float>(s, recv3, uh, eband_dev, out, st);
+}
+
+// dt of the finishes that follow on the stream (a kernel argument: no host
+// staging to keep alive)
+__global__ void k_slab_set_dt(dnsbox::StepState *st, double dt) { st->dt = dt; }
+
+// IF-Heun over the slabs (dnsboxheun.f90:88-126 with a fixed step): the
+// predictor's finish u* = IF (u + dt N(u)) into `out`, the corrector's
+// u <- (IF u + u*) / 2 + dt/2 N(u*) in place in `state` (uin = u*).
+extern "C" int dnsbox_slab_heun_finish(dnsbox_slab *s, const void *recv3, const void *uin_dev,
+                                       const double *eband_dev, int corrector, double dt, void *out_dev,
+                                       void *cuda_stream) {
+  RET(rhs_begin_check(s, recv3, eband_dev, out_dev));
+  if (!uin_dev) return set_err(DNSBOX_ERR_ARG, "null pointer");
+  if (!(dt > 0.0) || !isfinite(dt)) return set_err(DNSBOX_ERR_ARG, "dt must be positive and finite");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(cuda_stream);
+  k_slab_set_dt<<<1, 1, 0, st>>>(s->st, dt);
+  CK(cudaGetLastError());
+  const int mode = corrector ? FIN_CORR : FIN_PRED;
+  void *out = corrector ? nullptr : out_dev, *state = corrector ? out_dev : nullptr;
+  return s->precision == DNSBOX_FP64 ? rhs_finish<double>(s, recv3, uin_dev, eband_dev, out, st, mode, state)
+                                     : rhs_finish<float>(s, recv3, uin_dev, eband_dev, out, st, mode, state);
 }

@@ -192,11 +192,7 @@ class SlabFFT:
                                                     ctypes.c_void_p(self.eband.data_ptr()),
                                                     ctypes.c_void_p(out.data_ptr()), self._stream()))
 
-    def rhs_nonlinear(self, uh: torch.Tensor, out: torch.Tensor | None = None):
-        """N(u) of this rank's ky slab; returns (N, band energy, (max|u|, max|v|,
-        max|w|)), the last two over the whole box."""
-        if out is None:
-            out = torch.empty(self.state_shape(), dtype=self.cdtype, device=self.device)
+    def _exchange_rhs(self, uh: torch.Tensor) -> None:
         self.rhs_begin(uh)
         for f in range(5):
             self._exchange(self.send5[f], self.recv5[f])
@@ -205,6 +201,33 @@ class SlabFFT:
         for f in range(3):
             self._exchange(self.send3[f], self.recv3[f])
         self._reduce(self.umax, "max")
+
+    def heun_finish(self, uin: torch.Tensor, out: torch.Tensor, corrector: bool, dt: float) -> None:
+        self._check(out, self.state_shape(), self.cdtype, "state slab")
+        _lib.check(self._lib.dnsbox_slab_heun_finish(self._h, ctypes.c_void_p(self.recv3.data_ptr()),
+                                                     ctypes.c_void_p(uin.data_ptr()),
+                                                     ctypes.c_void_p(self.eband.data_ptr()), int(bool(corrector)),
+                                                     float(dt), ctypes.c_void_p(out.data_ptr()), self._stream()))
+
+    def heun_step(self, uh: torch.Tensor, dt: float, nsteps: int = 1) -> torch.Tensor:
+        """IF-Heun with a fixed step (dnsboxheun.f90:88-126, tStepFix) on this
+        rank's ky slab, in place: u* = IF (u + dt N(u)), then
+        u <- (IF u + u*) / 2 + dt/2 N(u*)."""
+        self._check(uh, self.state_shape(), self.cdtype, "state slab")
+        ustar = torch.empty_like(uh)
+        for _ in range(int(nsteps)):
+            self._exchange_rhs(uh)
+            self.heun_finish(uh, ustar, False, dt)
+            self._exchange_rhs(ustar)
+            self.heun_finish(ustar, uh, True, dt)
+        return uh
+
+    def rhs_nonlinear(self, uh: torch.Tensor, out: torch.Tensor | None = None):
+        """N(u) of this rank's ky slab; returns (N, band energy, (max|u|, max|v|,
+        max|w|)), the last two over the whole box."""
+        if out is None:
+            out = torch.empty(self.state_shape(), dtype=self.cdtype, device=self.device)
+        self._exchange_rhs(uh)
         self.rhs_finish(uh, out)
         return out, float(self.eband.item()), tuple(float(v) for v in self.umax.tolist())
 

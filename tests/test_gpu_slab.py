@@ -194,3 +194,90 @@ def test_slab_rhs_through_nccl_one_rank():
         box.close()
     finally:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- IF-Heun over the slabs
+def _emulate_stage(slabs, states_in, finish):
+    p = len(slabs)
+    for s in slabs:
+        s.rhs_begin(states_in[s.rank])
+    for f in range(5):
+        for q in range(p):
+            for r in range(p):
+                slabs[q].recv5[f][r].copy_(slabs[r].send5[f][q])
+    eb = sum(s.eband.clone() for s in slabs)
+    for s in slabs:
+        s.eband.copy_(eb)
+        s.rhs_middle()
+    for f in range(3):
+        for q in range(p):
+            for r in range(p):
+                slabs[q].recv3[f][r].copy_(slabs[r].send3[f][q])
+    for s in slabs:
+        finish(s)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 2e-6)])
+@pytest.mark.parametrize("shape,p", [((32, 32, 32), 2), ((32, 48, 64), 4)])
+def test_slab_heun_steps_match_the_box(prec, tol, shape, p):
+    """Three fixed-dt IF-Heun steps (dnsboxheun.f90:88-126, tStepFix) on the
+    slabs of P emulated ranks against the single box's dnsbox_step."""
+    from dnsbox_b200.ops import Box
+    from dnsbox_b200.slab import SlabFFT
+    nx, ny, nz = shape
+    dt, nsteps = 4e-3, 3
+    kw = dict(nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True)
+    g = O.Grid(O.Params(nx=nx, ny=ny, nz=nz, **kw))
+    rng = np.random.default_rng(9)
+    uh = O.state_dealias(g, O.state_project(g, O.state_u2uhat(g, 0.05 * rng.standard_normal((3, nz, ny, nx)))))
+    box = Box(nx=nx, ny=ny, nz=nz, precision=prec, tstep_fix=True, dt=dt, **kw)
+    ub = box.from_numpy(uh)
+    box.step(ub, nsteps, diag=False)
+    want = ub.cpu().numpy()
+    slabs = [SlabFFT(nx, ny, nz, precision=prec, rank=r, nranks=p) for r in range(p)]
+    for s in slabs:
+        s.setup_rhs(**kw)
+    nyl = ny // p
+    u0 = torch.from_numpy(uh).to("cuda", slabs[0].cdtype)
+    us = [u0[:, :, r * nyl:(r + 1) * nyl, :].contiguous() for r in range(p)]
+    ustar = [torch.empty_like(u) for u in us]
+    for _ in range(nsteps):
+        _emulate_stage(slabs, us, lambda s: s.heun_finish(us[s.rank], ustar[s.rank], False, dt))
+        _emulate_stage(slabs, ustar, lambda s: s.heun_finish(ustar[s.rank], us[s.rank], True, dt))
+    got = torch.cat(us, dim=2).cpu().numpy()
+    assert rel(got, want) < tol
+    # and the oracle's IF-Heun (FP64 form only: the FP32 state drifts by its rounding)
+    if prec == "fp64":
+        w = uh
+        for _ in range(nsteps):
+            w = O.heun_step(g, w, dt)
+        assert rel(got, w) < 1e-12
+    for s in slabs:
+        s.close()
+    box.close()
+
+
+def test_slab_heun_through_nccl_one_rank():
+    import torch.distributed as dist
+    from dnsbox_b200.ops import Box
+    from dnsbox_b200.slab import SlabFFT
+    n, dt = 32, 4e-3
+    kw = dict(nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True)
+    g = O.Grid(O.Params(nx=n, ny=n, nz=n, **kw))
+    uh = O.state_dealias(g, O.state_project(g, O.state_u2uhat(g, 0.05 * np.random.default_rng(4).standard_normal((3, n, n, n)))))
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        s = SlabFFT(n, n, n, precision="fp64")
+        s.setup_rhs(**kw)
+        u = torch.from_numpy(uh).cuda()
+        s.heun_step(u, dt, 2)
+        box = Box(n, tstep_fix=True, dt=dt, **kw)
+        ub = box.from_numpy(uh)
+        box.step(ub, 2, diag=False)
+        assert rel(u.cpu().numpy(), ub.cpu().numpy()) < 1e-12
+        torch.cuda.synchronize()
+        s.close()
+        box.close()
+    finally:
+        dist.destroy_process_group()
