@@ -24,6 +24,7 @@ ranks.
 from __future__ import annotations
 
 import ctypes
+import math
 
 import torch
 
@@ -167,6 +168,8 @@ class SlabFFT:
         self.send3 = torch.empty((3,) + shape, dtype=self.cdtype, device=self.device)
         self.recv3 = torch.empty_like(self.send3)
         self.eband = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self._alpha = tuple(float(a) for a in alpha)
+        self._cfl_done = False
         self.umax = torch.zeros(3, dtype=torch.float64, device=self.device)
         self._reduce = reduce if reduce is not None else (lambda t, op: all_reduce(t, op, self._group))
 
@@ -209,18 +212,43 @@ class SlabFFT:
                                                      ctypes.c_void_p(self.eband.data_ptr()), int(bool(corrector)),
                                                      float(dt), ctypes.c_void_p(out.data_ptr()), self._stream()))
 
-    def heun_step(self, uh: torch.Tensor, dt: float, nsteps: int = 1) -> torch.Tensor:
-        """IF-Heun with a fixed step (dnsboxheun.f90:88-126, tStepFix) on this
-        rank's ky slab, in place: u* = IF (u + dt N(u)), then
-        u <- (IF u + u*) / 2 + dt/2 N(u*)."""
+    def courant_dt(self, dt: float, courant_min: float, courant_max: float, dt_max: float, first: bool):
+        """set_time_step (dnsboxheun.f90:227-246) on io_Courant (io.f90:664-676)
+        of the reduced CFL maxima, as the single box's device rule: returns the
+        step and its Courant number."""
+        dx = (2.0 * math.pi / self._alpha[0]) / self.nx
+        dy = (2.0 * math.pi / self._alpha[1]) / self.ny
+        dz = (2.0 * math.pi / self._alpha[2]) / self.nz
+        um = self.umax.tolist()
+        c = um[0] * dt / dx + um[1] * dt / dy + um[2] * dt / dz
+        if first or c > courant_max or (c < courant_min and dt < dt_max):
+            nd = ((courant_max + courant_min) / (2.0 * c)) * dt
+            if nd > dt_max:
+                nd = dt_max
+            c = c * nd / dt
+            dt = nd
+        return dt, c
+
+    def heun_step(self, uh: torch.Tensor, dt: float, nsteps: int = 1, courant=None) -> list:
+        """IF-Heun (dnsboxheun.f90:88-126) on this rank's ky slab, in place:
+        u* = IF (u + dt N(u)), then u <- (IF u + u*) / 2 + dt/2 N(u*).  With
+        ``courant = (courant_min, courant_max, dt_max)`` the step is set from
+        the Courant number of each step's initial state (the first step always
+        adjusts it, as the reference's first call does), else ``dt`` is fixed
+        (tStepFix).  Returns the steps used."""
         self._check(uh, self.state_shape(), self.cdtype, "state slab")
         ustar = torch.empty_like(uh)
-        for _ in range(int(nsteps)):
+        used = []
+        for i in range(int(nsteps)):
             self._exchange_rhs(uh)
+            if courant is not None:
+                dt, _ = self.courant_dt(dt, *courant, first=(i == 0 and not self._cfl_done))
+                self._cfl_done = True
             self.heun_finish(uh, ustar, False, dt)
             self._exchange_rhs(ustar)
             self.heun_finish(ustar, uh, True, dt)
-        return uh
+            used.append(dt)
+        return used
 
     def rhs_nonlinear(self, uh: torch.Tensor, out: torch.Tensor | None = None):
         """N(u) of this rank's ky slab; returns (N, band energy, (max|u|, max|v|,

@@ -281,3 +281,47 @@ def test_slab_heun_through_nccl_one_rank():
         box.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 2e-6)])
+def test_slab_heun_with_courant_control_matches_the_box(prec, tol):
+    """CFL-controlled IF-Heun over P = 2 emulated ranks: the step set from the
+    reduced CFL maxima of each step's initial state (set_time_step on
+    io_Courant) matches the single box's device rule, steps and state."""
+    from dnsbox_b200.ops import Box
+    from dnsbox_b200.slab import SlabFFT
+    nx = ny = nz = 32
+    p, dt0, nsteps, cfl = 2, 4e-3, 3, (0.4, 0.6, 0.01)
+    kw = dict(nu=0.01, kCutOff=2.5, Pin=0.1, bandlim=True)
+    g = O.Grid(O.Params(nx=nx, ny=ny, nz=nz, **kw))
+    rng = np.random.default_rng(12)
+    uh = O.state_dealias(g, O.state_project(g, O.state_u2uhat(g, 0.05 * rng.standard_normal((3, nz, ny, nx)))))
+    box = Box(nx=nx, ny=ny, nz=nz, precision=prec, dt=dt0, courant_min=cfl[0], courant_max=cfl[1], dt_max=cfl[2],
+              **kw)
+    ub = box.from_numpy(uh)
+    recs = box.step(ub, nsteps)
+    slabs = [SlabFFT(nx, ny, nz, precision=prec, rank=r, nranks=p) for r in range(p)]
+    for s in slabs:
+        s.setup_rhs(**kw)
+    nyl = ny // p
+    u0 = torch.from_numpy(uh).to("cuda", slabs[0].cdtype)
+    us = [u0[:, :, r * nyl:(r + 1) * nyl, :].contiguous() for r in range(p)]
+    ustar = [torch.empty_like(u) for u in us]
+    dt, steps = dt0, []
+    for i in range(nsteps):
+        _emulate_stage(slabs, us, lambda s: None)
+        um = torch.stack([s.umax.clone() for s in slabs]).max(dim=0).values
+        for s in slabs:
+            s.umax.copy_(um)
+        dt, _ = slabs[0].courant_dt(dt, *cfl, first=(i == 0))
+        steps.append(dt)
+        for s in slabs:
+            s.heun_finish(us[s.rank], ustar[s.rank], False, dt)
+        _emulate_stage(slabs, ustar, lambda s: s.heun_finish(ustar[s.rank], us[s.rank], True, dt))
+    want_steps = [r["dt"] for r in recs]
+    assert np.allclose(steps, want_steps, rtol=1e-13 if prec == "fp64" else 1e-6), (steps, want_steps)
+    got = torch.cat(us, dim=2).cpu().numpy()
+    assert rel(got, ub.cpu().numpy()) < tol
+    for s in slabs:
+        s.close()
+    box.close()
