@@ -148,7 +148,7 @@ SIGNATURES = {
     "dnsbox_slab_rhs_begin": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "dnsbox_slab_rhs_middle": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "dnsbox_slab_rhs_finish": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
-    "dnsbox_slab_heun_finish": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_int, ctypes.c_double, _VP, _VP]),
+    "dnsbox_slab_heun_finish": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_int, ctypes.c_double, _VP, _VP, _VP]),
 }
 
 _lib = None

@@ -69,6 +69,7 @@ struct dnsbox_slab {
   int *band = nullptr;               // band modes of the local ky rows (offset lo, hi, kx)
   int nband = 0;
   dnsbox::StepState *st = nullptr;   // band energy, CFL maxima, dt of the Heun finishes
+  double *rows = nullptr;            // (E, D) sums of the corrector finish's rows, nz * nyl pairs
 };
 
 namespace {
@@ -99,6 +100,7 @@ void slab_free(dnsbox_slab *s) {
   cudaFree(s->V);
   cudaFree(s->band);
   cudaFree(s->st);
+  cudaFree(s->rows);
   for (void *t : s->tw) cudaFree(t);
   delete s;
 }
@@ -407,7 +409,7 @@ int rhs_middle(dnsbox_slab *s, const void *recv5, double *umax, void *send3, cud
 
 template <typename T>
 int rhs_finish(dnsbox_slab *s, const void *recv3, const void *uh, const double *eband, void *out, cudaStream_t st,
-               int mode = FIN_RHS, void *state = nullptr) {
+               int mode = FIN_RHS, void *state = nullptr, double *rows = nullptr) {
   using C = typename CT<T>::type;
   const dnsbox_params &p = s->p;
   // pass E1: forward z of the received ky-slab
@@ -423,6 +425,7 @@ int rhs_finish(dnsbox_slab *s, const void *recv3, const void *uh, const double *
   f.uin = reinterpret_cast<const C *>(uh);
   f.out = reinterpret_cast<C *>(out);
   f.state = reinterpret_cast<C *>(state);
+  f.partials = rows;
   f.st = s->st;
   f.tw = reinterpret_cast<const C *>(s->tw[2]);
   f.nh = (long long)slab_field(s);
@@ -489,6 +492,7 @@ extern "C" int dnsbox_slab_rhs_setup(dnsbox_slab *s, const dnsbox_params *p) {
     CK(cudaMalloc(&s->st, sizeof(dnsbox::StepState)));
     CK(cudaMemset(s->st, 0, sizeof(dnsbox::StepState)));
   }
+  if (!s->rows) CK(cudaMalloc(&s->rows, 2 * (size_t)s->nz * s->nyl * sizeof(double)));
   // band modes |k| <= kCutOff among the local ky rows (as dnsbox_create builds them)
   cudaFree(s->band);
   s->band = nullptr;
@@ -545,12 +549,31 @@ extern "C" int dnsbox_slab_rhs_finish(dnsbox_slab *s, const void *recv3, const v
 // staging to keep alive)
 __global__ void k_slab_set_dt(dnsbox::StepState *st, double dt) { st->dt = dt; }
 
-// IF-Heun over the slabs (dnsboxheun.f90:88-126 with a fixed step): the
-// predictor's finish u* = IF (u + dt N(u)) into `out`, the corrector's
-// u <- (IF u + u*) / 2 + dt/2 N(u*) in place in `state` (uin = u*).
+// The rank's (E, D) sums: the corrector finish's row pairs added in a fixed
+// order (one block), unscaled, for the caller's sum over the ranks.
+__global__ void k_slab_row_sums(const double *rows, int n, double *ed) {
+  __shared__ double red[2 * 32];
+  double e = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    e += rows[2 * i];
+    d += rows[2 * i + 1];
+  }
+  double v[2] = {e, d};
+  dnsbox::block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    ed[0] = v[0];
+    ed[1] = v[1];
+  }
+}
+
+// IF-Heun over the slabs (dnsboxheun.f90:88-126): the predictor's finish
+// u* = IF (u + dt N(u)) into `out`, the corrector's u <- (IF u + u*) / 2 +
+// dt/2 N(u*) in place in `state` (uin = u*), with the rank's unscaled (E, D)
+// sums of the new state into ed_dev (state_kinetic / state_dissipation in
+// Parseval form: E = s^2 sum, D = nu s^2 sum after the sum over the ranks).
 extern "C" int dnsbox_slab_heun_finish(dnsbox_slab *s, const void *recv3, const void *uin_dev,
                                        const double *eband_dev, int corrector, double dt, void *out_dev,
-                                       void *cuda_stream) {
+                                       double *ed_dev, void *cuda_stream) {
   RET(rhs_begin_check(s, recv3, eband_dev, out_dev));
   if (!uin_dev) return set_err(DNSBOX_ERR_ARG, "null pointer");
   if (!(dt > 0.0) || !isfinite(dt)) return set_err(DNSBOX_ERR_ARG, "dt must be positive and finite");
@@ -559,6 +582,12 @@ extern "C" int dnsbox_slab_heun_finish(dnsbox_slab *s, const void *recv3, const 
   CK(cudaGetLastError());
   const int mode = corrector ? FIN_CORR : FIN_PRED;
   void *out = corrector ? nullptr : out_dev, *state = corrector ? out_dev : nullptr;
-  return s->precision == DNSBOX_FP64 ? rhs_finish<double>(s, recv3, uin_dev, eband_dev, out, st, mode, state)
-                                     : rhs_finish<float>(s, recv3, uin_dev, eband_dev, out, st, mode, state);
+  double *rows = corrector && ed_dev ? s->rows : nullptr;
+  RET(s->precision == DNSBOX_FP64 ? rhs_finish<double>(s, recv3, uin_dev, eband_dev, out, st, mode, state, rows)
+                                  : rhs_finish<float>(s, recv3, uin_dev, eband_dev, out, st, mode, state, rows));
+  if (rows) {
+    k_slab_row_sums<<<1, 256, 0, st>>>(rows, s->nz * s->nyl, ed_dev);
+    CK(cudaGetLastError());
+  }
+  return DNSBOX_OK;
 }

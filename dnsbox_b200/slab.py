@@ -168,8 +168,11 @@ class SlabFFT:
         self.send3 = torch.empty((3,) + shape, dtype=self.cdtype, device=self.device)
         self.recv3 = torch.empty_like(self.send3)
         self.eband = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self.ed = torch.zeros(2, dtype=torch.float64, device=self.device)
         self._alpha = tuple(float(a) for a in alpha)
+        self._phys = dict(nu=float(nu), Q=float(Q), Pin=float(Pin), bandlim=bool(bandlim))
         self._cfl_done = False
+        self.t = 0.0
         self.umax = torch.zeros(3, dtype=torch.float64, device=self.device)
         self._reduce = reduce if reduce is not None else (lambda t, op: all_reduce(t, op, self._group))
 
@@ -206,21 +209,40 @@ class SlabFFT:
         self._reduce(self.umax, "max")
 
     def heun_finish(self, uin: torch.Tensor, out: torch.Tensor, corrector: bool, dt: float) -> None:
+        """The predictor's (u* into out) or the corrector's (out = u, in place)
+        finish; the corrector leaves this rank's (E, D) sums in ``self.ed``."""
         self._check(out, self.state_shape(), self.cdtype, "state slab")
+        ed = ctypes.c_void_p(self.ed.data_ptr()) if corrector else None
         _lib.check(self._lib.dnsbox_slab_heun_finish(self._h, ctypes.c_void_p(self.recv3.data_ptr()),
                                                      ctypes.c_void_p(uin.data_ptr()),
                                                      ctypes.c_void_p(self.eband.data_ptr()), int(bool(corrector)),
-                                                     float(dt), ctypes.c_void_p(out.data_ptr()), self._stream()))
+                                                     float(dt), ctypes.c_void_p(out.data_ptr()), ed, self._stream()))
+
+    def step_record(self, dt: float, courant: float) -> dict:
+        """The step record (the Ekin.dat quantities, io.f90:651-658) from the
+        corrector's (E, D) sums once they are summed over the ranks."""
+        s2 = (1.0 / (self.nx * self.ny * self.nz)) ** 2
+        e, d = self.ed.tolist()
+        ph = self._phys
+        ekin = e * s2
+        return {"t": self.t, "dt": dt, "ekin": ekin, "dissipation": ph["nu"] * d * s2,
+                "production_literal": 2.0 * ph["Q"] * ekin,
+                "injected_power": (ph["Pin"] if ph["bandlim"] else 0.0) + 2.0 * ph["Q"] * ekin,
+                "courant": courant, "umax": tuple(self.umax.tolist()), "eband": float(self.eband.item())}
+
+    def courant_number(self, dt: float) -> float:
+        """io_Courant (io.f90:664-676) of the reduced CFL maxima."""
+        dx = (2.0 * math.pi / self._alpha[0]) / self.nx
+        dy = (2.0 * math.pi / self._alpha[1]) / self.ny
+        dz = (2.0 * math.pi / self._alpha[2]) / self.nz
+        um = self.umax.tolist()
+        return um[0] * dt / dx + um[1] * dt / dy + um[2] * dt / dz
 
     def courant_dt(self, dt: float, courant_min: float, courant_max: float, dt_max: float, first: bool):
         """set_time_step (dnsboxheun.f90:227-246) on io_Courant (io.f90:664-676)
         of the reduced CFL maxima, as the single box's device rule: returns the
         step and its Courant number."""
-        dx = (2.0 * math.pi / self._alpha[0]) / self.nx
-        dy = (2.0 * math.pi / self._alpha[1]) / self.ny
-        dz = (2.0 * math.pi / self._alpha[2]) / self.nz
-        um = self.umax.tolist()
-        c = um[0] * dt / dx + um[1] * dt / dy + um[2] * dt / dz
+        c = self.courant_number(dt)
         if first or c > courant_max or (c < courant_min and dt < dt_max):
             nd = ((courant_max + courant_min) / (2.0 * c)) * dt
             if nd > dt_max:
@@ -235,20 +257,28 @@ class SlabFFT:
         ``courant = (courant_min, courant_max, dt_max)`` the step is set from
         the Courant number of each step's initial state (the first step always
         adjusts it, as the reference's first call does), else ``dt`` is fixed
-        (tStepFix).  Returns the steps used."""
+        (tStepFix).  Returns the step records (t after the step, dt, Ekin,
+        dissipation, production, Courant number, CFL maxima, band energy)."""
         self._check(uh, self.state_shape(), self.cdtype, "state slab")
         ustar = torch.empty_like(uh)
-        used = []
+        recs = []
         for i in range(int(nsteps)):
             self._exchange_rhs(uh)
+            eband, umax = float(self.eband.item()), tuple(self.umax.tolist())
             if courant is not None:
-                dt, _ = self.courant_dt(dt, *courant, first=(i == 0 and not self._cfl_done))
+                dt, c = self.courant_dt(dt, *courant, first=(i == 0 and not self._cfl_done))
                 self._cfl_done = True
+            else:
+                c = self.courant_number(dt)
             self.heun_finish(uh, ustar, False, dt)
             self._exchange_rhs(ustar)
             self.heun_finish(ustar, uh, True, dt)
-            used.append(dt)
-        return used
+            self._reduce(self.ed, "sum")
+            self.t += dt
+            rec = self.step_record(dt, c)
+            rec.update(eband=eband, umax=umax)   # of the step's initial state, as the single box's records
+            recs.append(rec)
+        return recs
 
     def rhs_nonlinear(self, uh: torch.Tensor, out: torch.Tensor | None = None):
         """N(u) of this rank's ky slab; returns (N, band energy, (max|u|, max|v|,

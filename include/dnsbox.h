@@ -243,13 +243,16 @@ int dnsbox_slab_rhs_middle(dnsbox_slab *slab, const void *recv5_dev, double *uma
                            void *cuda_stream);
 int dnsbox_slab_rhs_finish(dnsbox_slab *slab, const void *recv3_dev, const void *uh_dev, const double *eband_dev,
                            void *out_dev, void *cuda_stream);
-/* IF-Heun over the slabs with a fixed step (dnsboxheun.f90:88-126, tStepFix):
- * after rhs_begin / rhs_middle and the exchanges, the finish of the
- * predictor (corrector = 0: out_dev <- u* = IF (u + dt N(u)), uin_dev = u)
- * or of the corrector (corrector = 1: out_dev = u, updated in place to
- * (IF u + u*) / 2 + dt/2 N(u*), uin_dev = u*) replaces rhs_finish. */
+/* IF-Heun over the slabs (dnsboxheun.f90:88-126; the caller picks dt, e.g.
+ * by set_time_step on the reduced CFL maxima): after rhs_begin / rhs_middle
+ * and the exchanges, the finish of the predictor (corrector = 0: out_dev <-
+ * u* = IF (u + dt N(u)), uin_dev = u) or of the corrector (corrector = 1:
+ * out_dev = u, updated in place to (IF u + u*) / 2 + dt/2 N(u*), uin_dev =
+ * u*) replaces rhs_finish.  ed_dev (corrector, or NULL): 2 device doubles,
+ * the rank's unscaled (E, D) sums of the new state; summed over the ranks,
+ * Ekin = s^2 E and the dissipation nu s^2 D with s = 1/(nx ny nz). */
 int dnsbox_slab_heun_finish(dnsbox_slab *slab, const void *recv3_dev, const void *uin_dev, const double *eband_dev,
-                            int corrector, double dt, void *out_dev, void *cuda_stream);
+                            int corrector, double dt, void *out_dev, double *ed_dev, void *cuda_stream);
 
 /* ---- initial conditions on the device ---------------------------------- */
 /* state_init_rand, state.f90:211-285 (Yoffe 2012, s. 2.2.5): a random physical

@@ -271,11 +271,15 @@ def test_slab_heun_through_nccl_one_rank():
         s = SlabFFT(n, n, n, precision="fp64")
         s.setup_rhs(**kw)
         u = torch.from_numpy(uh).cuda()
-        s.heun_step(u, dt, 2)
+        recs = s.heun_step(u, dt, 2)
         box = Box(n, tstep_fix=True, dt=dt, **kw)
         ub = box.from_numpy(uh)
-        box.step(ub, 2, diag=False)
+        want = box.step(ub, 2)
         assert rel(u.cpu().numpy(), ub.cpu().numpy()) < 1e-12
+        for r, w in zip(recs, want):   # the step records, as the single box's
+            for k in ("t", "dt", "ekin", "dissipation", "injected_power", "courant", "eband"):
+                assert abs(r[k] - w[k]) <= 1e-12 * abs(w[k]), (k, r[k], w[k])
+            assert np.allclose(r["umax"], w["umax"], rtol=1e-12)
         torch.cuda.synchronize()
         s.close()
         box.close()
@@ -307,7 +311,8 @@ def test_slab_heun_with_courant_control_matches_the_box(prec, tol):
     u0 = torch.from_numpy(uh).to("cuda", slabs[0].cdtype)
     us = [u0[:, :, r * nyl:(r + 1) * nyl, :].contiguous() for r in range(p)]
     ustar = [torch.empty_like(u) for u in us]
-    dt, steps = dt0, []
+    dt, steps, ekin, diss = dt0, [], [], []
+    s2 = (1.0 / (nx * ny * nz)) ** 2
     for i in range(nsteps):
         _emulate_stage(slabs, us, lambda s: None)
         um = torch.stack([s.umax.clone() for s in slabs]).max(dim=0).values
@@ -318,8 +323,14 @@ def test_slab_heun_with_courant_control_matches_the_box(prec, tol):
         for s in slabs:
             s.heun_finish(us[s.rank], ustar[s.rank], False, dt)
         _emulate_stage(slabs, ustar, lambda s: s.heun_finish(ustar[s.rank], us[s.rank], True, dt))
+        ed = sum(s.ed.clone() for s in slabs).tolist()      # the sum over the ranks
+        ekin.append(ed[0] * s2)
+        diss.append(kw["nu"] * ed[1] * s2)
     want_steps = [r["dt"] for r in recs]
     assert np.allclose(steps, want_steps, rtol=1e-13 if prec == "fp64" else 1e-6), (steps, want_steps)
+    r_tol = 1e-12 if prec == "fp64" else 2e-6
+    assert np.allclose(ekin, [r["ekin"] for r in recs], rtol=r_tol)
+    assert np.allclose(diss, [r["dissipation"] for r in recs], rtol=r_tol)
     got = torch.cat(us, dim=2).cpu().numpy()
     assert rel(got, ub.cpu().numpy()) < tol
     for s in slabs:
