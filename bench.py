@@ -459,6 +459,53 @@ def slab_fft_rate(n=1024, reps=5, rank=0, world=1, dist_on=False):
             "exchange": "NCCL all-to-all (torch.distributed)" if world > 1 else "device copy (one rank)"}
 
 
+def slab_heun_rate(n=512, steps=4, rank=0, world=1, dist_on=False):
+    """One box split over the ranks (p3dfft's slabs): IF-Heun steps of the
+    n^3 forced workload in FP32 on the rank's ky slab, the right-hand side's
+    eight per-field all-to-alls and the band-energy / CFL-maxima / (E, D)
+    reductions over NCCL under torchrun (strong scaling: the box is fixed;
+    one rank exchanges by copies).  Fixed dt; steps per second on the slowest
+    rank's CUDA-event time."""
+    from dnsbox_b200 import ic
+    from dnsbox_b200.ops import Box
+    from dnsbox_b200.slab import SlabFFT
+    s = SlabFFT(n, n, n, precision="fp32")
+    kw = dict(nu=8e-4, kCutOff=WORKLOAD["kCutOff"], Pin=WORKLOAD["Pin"], bandlim=True)
+    s.setup_rhs(**kw)
+    # every rank draws the whole field from the same seed and keeps its ky rows
+    b = Box(n, precision="fp32", **kw)
+    box_uh = ic.random_field_gpu(b, seed=0, k0=WORKLOAD["k0"])
+    b.close()
+    nyl = n // world
+    u = box_uh[:, :, rank * nyl:(rank + 1) * nyl, :].contiguous()
+    del box_uh
+    torch.cuda.empty_cache()
+    dt = 1e-3
+    s.heun_step(u, dt, 1)
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    recs = s.heun_step(u, dt, steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if dist_on:
+        ms = max_over_ranks(ms)
+    s.close()
+    del u
+    torch.cuda.empty_cache()
+    if rank != 0:
+        return None
+    return {"value": 1e3 / ms, "unit": "steps/s", "grid": n, "precision": "fp32", "n_ranks": world,
+            "ms_per_step": ms, "dt": dt, "ekin_last": recs[-1]["ekin"],
+            "scaling": "strong: one box split over the ranks (z-slabs / ky-slabs)",
+            "exchange": "NCCL all-to-all and all-reduce (torch.distributed)" if world > 1 else "device copies (one rank)"}
+
+
 def read_traffic(prec, n, pruned):
     """DRAM bytes per launch from a committed ncu summary, if one exists
     (columns: pass precision n pruned bytes)."""
@@ -516,6 +563,7 @@ def run_ours(args, rank, world, dist_on):
     # the ensemble shards over the ranks (every rank takes part)
     ens_sharded = ensemble_rate(rank=rank, world=world, dist_on=dist_on) if world > 1 and not args.no_extra else None
     slab_sharded = slab_fft_rate(rank=rank, world=world, dist_on=dist_on) if world > 1 and not args.no_extra else None
+    slab_step = slab_heun_rate(rank=rank, world=world, dist_on=dist_on) if world > 1 and not args.no_extra else None
     if rank != 0:
         return
     main = args.precisions[0]
@@ -589,7 +637,7 @@ def run_ours(args, rank, world, dist_on):
                        for k, f in rr["pass_fields"].items() if prr["launches"][k]},
             "pruned": rr["pruned"]}
     if ens_sharded:
-        line["extra"] = {"ensemble_96": ens_sharded, "slab_fft_1024": slab_sharded}
+        line["extra"] = {"ensemble_96": ens_sharded, "slab_fft_1024": slab_sharded, "slab_heun_512": slab_step}
     if world == 1 and not args.no_extra:
         line["extra"] = extra_sizes(args)
         line["extra"]["tc_split_1024"] = tc_1024_rate(args)
@@ -597,6 +645,7 @@ def run_ours(args, rank, world, dist_on):
         line["extra"]["periodic_orbit_grad_96"] = orbit_rate()
         line["extra"]["ensemble_96"] = ensemble_rate()
         line["extra"]["slab_fft_1024"] = slab_fft_rate()
+        line["extra"]["slab_heun_512"] = slab_heun_rate()
     if world == 1 and not args.no_cpu_baseline:
         from oracle import dnsbox_oracle as O
         rate, done, el = cpu_reference_rate(n, 3, budget_s=args.cpu_budget, warmup=0)
