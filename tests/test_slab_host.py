@@ -1,6 +1,6 @@
 """Host side of the slab-decomposed transform (dnsbox_b200/slab.py): the
 partition of p3dfft's 1 x P processor grid (variables.f90:131-157), the
-all-to-all of equal blocks on gloo ranks (world size 2 and 3), and a NumPy
+all-to-all of equal blocks and the sum and max all-reduces on gloo ranks (world size 2 and 3), and a NumPy
 model of the decomposition's block layout, which the CUDA halves follow: the
 received blocks of a forward transform, in rank order, are the local ky rows
 of every z-plane.  No GPU is touched."""
@@ -14,7 +14,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from dnsbox_b200.slab import all_to_all, slab_extents
+from dnsbox_b200.slab import all_reduce, all_to_all, slab_extents
 
 
 def test_extents_tile_the_grid():
@@ -94,6 +94,12 @@ def _worker(rank, world, port, q):
         recv = torch.full_like(send, complex("nan"))
         all_to_all(send, recv)
         ok = all(torch.equal(recv[s], torch.arange(blk) + 1j * (100 * s + rank)) for s in range(world))
+        # the band-energy / (E, D) sums and the CFL maxima of the slab stepper
+        e = torch.tensor([1.0 + rank], dtype=torch.float64)
+        all_reduce(e, "sum")
+        m = torch.tensor([float(rank), 10.0 - rank, 0.5], dtype=torch.float64)
+        all_reduce(m, "max")
+        ok = ok and e.item() == sum(1.0 + r for r in range(world)) and m.tolist() == [world - 1.0, 10.0, 0.5]
         dist.barrier()
         q.put((rank, ok))
     finally:
