@@ -357,20 +357,21 @@ template <typename T>
 int rhs_middle(dnsbox_slab *s, const void *recv5, double *umax, void *send3, cudaStream_t st) {
   using C = typename CT<T>::type;
   const double sc = 1.0 / ((double)s->nx * s->ny * s->nz);
-  for (int f = 0; f < 5; ++f) {
-    if (s->nranks > 1) RET(slab_blocks(s, false, fld<T>(recv5, s, f), fld<T>(s->W, s, f), st));
-    else CK(cudaMemcpyAsync(fld<T>(s->W, s, f), fld<T>(recv5, s, f), slab_field(s) * s->cbytes,
-                            cudaMemcpyDeviceToDevice, st));
+  // the received ky rows as whole planes (one rank: the buffers are the planes)
+  const void *in = recv5;
+  if (s->nranks > 1) {
+    for (int f = 0; f < 5; ++f) RET(slab_blocks(s, false, fld<T>(recv5, s, f), fld<T>(s->W, s, f), st));
+    in = s->W;
   }
   // pass B: inverse y; omega_x = dy w - dz v, omega_y = dz u - dx w, omega_z = dx v - dy u
   StridedArgs<T> b = slab_pass<T>(s, false);
   b.njobs = 6;
-  set_job<T>(b, 0, fld<T>(s->W, s, 0), fld<T>(s->V, s, 0));
-  set_job<T>(b, 1, fld<T>(s->W, s, 1), fld<T>(s->V, s, 1));
-  set_job<T>(b, 2, fld<T>(s->W, s, 2), fld<T>(s->V, s, 2));
-  set_job<T>(b, 3, fld<T>(s->W, s, 2), fld<T>(s->V, s, 3), 0.0, sc, 1, fld<T>(s->W, s, 3));
-  set_job<T>(b, 4, fld<T>(s->W, s, 4), fld<T>(s->V, s, 4), 1.0, 0.0, 0, fld<T>(s->W, s, 2), 0.0, -sc, 0);
-  set_job<T>(b, 5, fld<T>(s->W, s, 0), fld<T>(s->V, s, 5), 0.0, -sc, 1, fld<T>(s->W, s, 1), 0.0, sc, 0);
+  set_job<T>(b, 0, fld<T>(in, s, 0), fld<T>(s->V, s, 0));
+  set_job<T>(b, 1, fld<T>(in, s, 1), fld<T>(s->V, s, 1));
+  set_job<T>(b, 2, fld<T>(in, s, 2), fld<T>(s->V, s, 2));
+  set_job<T>(b, 3, fld<T>(in, s, 2), fld<T>(s->V, s, 3), 0.0, sc, 1, fld<T>(in, s, 3));
+  set_job<T>(b, 4, fld<T>(in, s, 4), fld<T>(s->V, s, 4), 1.0, 0.0, 0, fld<T>(in, s, 2), 0.0, -sc, 0);
+  set_job<T>(b, 5, fld<T>(in, s, 0), fld<T>(s->V, s, 5), 0.0, -sc, 1, fld<T>(in, s, 1), 0.0, sc, 0);
   RET(slab_run<T>(s, s->ny, true, b, s->nzl, st));
   // pass C: the fused x pass on the local planes
   XlineNLArgs<T> x;
@@ -394,16 +395,15 @@ int rhs_middle(dnsbox_slab *s, const void *recv5, double *umax, void *send3, cud
   cudaError_t e = Ops<T>::xline_nl(s->nx, x, 0, st);
   if (e != cudaSuccess) return set_err(DNSBOX_ERR_CUDA, "slab x pass: %s", cudaGetErrorString(e));
   CK(cudaMemcpyAsync(umax, s->st->umax, 3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  // pass D: forward y, then N packed by destination rank
+  // pass D: forward y, then N packed by destination rank (one rank: straight
+  // into the send buffers)
+  void *dout = s->nranks > 1 ? s->V : send3;
   StridedArgs<T> d = slab_pass<T>(s, false);
   d.njobs = 3;
-  for (int f = 0; f < 3; ++f) set_job<T>(d, f, fld<T>(s->W, s, f), fld<T>(s->V, s, f));
+  for (int f = 0; f < 3; ++f) set_job<T>(d, f, fld<T>(s->W, s, f), fld<T>(dout, s, f));
   RET(slab_run<T>(s, s->ny, false, d, s->nzl, st));
-  for (int f = 0; f < 3; ++f) {
-    if (s->nranks > 1) RET(slab_blocks(s, true, fld<T>(s->V, s, f), fld<T>(send3, s, f), st));
-    else CK(cudaMemcpyAsync(fld<T>(send3, s, f), fld<T>(s->V, s, f), slab_field(s) * s->cbytes,
-                            cudaMemcpyDeviceToDevice, st));
-  }
+  if (s->nranks > 1)
+    for (int f = 0; f < 3; ++f) RET(slab_blocks(s, true, fld<T>(s->V, s, f), fld<T>(send3, s, f), st));
   return DNSBOX_OK;
 }
 
